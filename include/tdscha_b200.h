@@ -1,0 +1,162 @@
+/*
+ * tdscha_b200.h -- C ABI of the B200 (sm_100a) TD-SCHA linear-response engine.
+ *
+ * Plain pointers and sizes only.  Every entry point returns 0 on success and a negative
+ * TDSCHA_E* code on failure (never exit()); tdscha_last_error() gives the message of the last
+ * failure on the calling thread.  "_device" entry points take device pointers and an optional
+ * cudaStream_t passed as void* (NULL = the legacy default stream) and are asynchronous with respect
+ * to the host unless stated otherwise; the other entry points take host buffers and synchronise.
+ *
+ * Reference interfaces replaced (mesonepigreco/python-sscha, tdscha package):
+ *   sscha_HP_odd.GetPerturbAverageSym          CModules/odd_corr_module.c:491-634
+ *     -> tdscha_GetPerturbAverageSym (same argument list), tdscha_perturb_average_sym (resident)
+ *   get_f_average_from_Y_pert_sym_fast          CModules/LanczosFunctions.c:2082-2254
+ *   get_d2v_dR2_from_R_pert_sym_fast            CModules/LanczosFunctions.c:2257-2438
+ *   get_d2v_dR2_from_Y_pert_sym_fast            CModules/LanczosFunctions.c:2615-2754
+ *     -> the three are computed together by tdscha_perturb_average_sym[_device]
+ *   Lanczos.apply_full_L / apply_L1_FT / apply_anharmonic_FT
+ *                                               Modules/DynamicalLanczos.py:3467-3570, 2227-2385, 2891-3281
+ *     -> tdscha_apply_full_L_device
+ *   Lanczos.run_FT (one bi-conjugate step, n_rep_orth = 0)
+ *                                               Modules/DynamicalLanczos.py:6026-6153
+ *     -> tdscha_lanczos_step_device
+ *   Lanczos.get_green_function_continued_fraction
+ *                                               Modules/DynamicalLanczos.py:4951-5047
+ *     -> tdscha_continued_fraction_device
+ */
+#ifndef TDSCHA_B200_H
+#define TDSCHA_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define TDSCHA_OK 0
+#define TDSCHA_EINVAL (-1)     /* bad argument (shape, value, layout)                       */
+#define TDSCHA_ECUDA (-2)      /* CUDA runtime / driver error                               */
+#define TDSCHA_ENOMEM (-3)     /* device allocation failed                                  */
+#define TDSCHA_ENOSUPPORT (-4) /* no sm_100 device, or precision not available              */
+#define TDSCHA_ETIMEOUT (-5)   /* a device-side bounded wait expired (kernel aborted cleanly) */
+
+/* arithmetic of the two O(N * N_sym * n^2) ensemble contractions; everything else is FP64 */
+#define TDSCHA_PREC_FP64 0     /* FP64 throughout                                            */
+#define TDSCHA_PREC_TF32 1     /* tcgen05 kind::tf32, one product, FP32 accumulation        */
+#define TDSCHA_PREC_BF16X3 2   /* tcgen05 kind::f16 on bf16 hi/lo splits, 3 products, FP32 acc */
+#define TDSCHA_PREC_TF32X3 3   /* tcgen05 kind::tf32 on tf32 hi/lo splits, 3 products, FP32 acc */
+#define TDSCHA_PREC_BF16 4     /* tcgen05 kind::f16, one bf16 product (accuracy reference)     */
+
+typedef struct tdscha_ensemble tdscha_ensemble;
+
+/* Message of the last failure on this thread ("" if none). */
+const char *tdscha_last_error(void);
+
+/* Library version string. */
+const char *tdscha_version(void);
+
+/*
+ * Upload an ensemble and its mode-space symmetries to the current CUDA device and keep them
+ * resident.  Argument meaning follows GetPerturbAverageSym (odd_corr_module.c:519-520):
+ *   X, Y        (N, n) C order, mass-rescaled displacements / anharmonic forces in the mode basis
+ *   w           (n) frequencies [Ry];  rho (N) weights;  T temperature [K]
+ *   N_sym       number of symmetry operations
+ *   n_blocks    number of degenerate blocks;  n_deg (n_blocks) block sizes
+ *   deg_space   n_blocks pointers, each to n_deg[b] int mode indices (contiguous, ascending)
+ *   sym_blocks  n_blocks pointers, each to an (N_sym, n_deg[b], n_deg[b]) C-order table
+ *   blocks_ids  (n) block of each mode
+ * Every frequency inside a block must be equal to within 1e-6 relative (degenerate subspace).
+ */
+int tdscha_ensemble_create(const double *X, const double *Y, const double *w, const double *rho,
+                           int N, int n, double T, int N_sym, int n_blocks, const int *n_deg,
+                           const int *const *deg_space, const double *const *sym_blocks,
+                           const int *blocks_ids, tdscha_ensemble **out);
+
+int tdscha_ensemble_destroy(tdscha_ensemble *ens);
+
+/* Sizes of a resident ensemble (any pointer may be NULL). */
+int tdscha_ensemble_info(const tdscha_ensemble *ens, int *n, int *N, int *N_sym, int *n_blocks,
+                         double *T, double *N_eff);
+
+/* Device bytes the ensemble holds now (operands of every precision built so far included). */
+int tdscha_ensemble_device_bytes(const tdscha_ensemble *ens, long long *bytes);
+
+/*
+ * Symmetrised perturbed averages on host buffers: f_out (n), d2v_out (n, n) C order, exactly the
+ * outputs of GetPerturbAverageSym (d2v overwritten, D4 part added when apply_d4 = 1).
+ * Only the symmetric part of Y1 enters the reference's formulas; Y1 may be non-symmetric.
+ */
+int tdscha_perturb_average_sym(tdscha_ensemble *ens, const double *R1, const double *Y1, int apply_d4,
+                               int precision, double *f_out, double *d2v_out);
+
+/* Batched, device-resident: nb perturbations R1 (nb, n), Y1 (nb, n, n) -> f (nb, n), d2v (nb, n, n). */
+int tdscha_perturb_average_sym_device(tdscha_ensemble *ens, int nb, const double *R1, const double *Y1,
+                                      int apply_d4, int precision, double *f_out, double *d2v_out,
+                                      void *stream);
+
+/*
+ * One-shot drop-in with the argument list of sscha_HP_odd.GetPerturbAverageSym
+ * (odd_corr_module.c:519-520), FP64: uploads, computes, downloads, frees.
+ */
+int tdscha_GetPerturbAverageSym(const double *X, const double *Y, const double *w, const double *rho,
+                                const double *R1, const double *Y1, double T, int apply_D4, int N_syms,
+                                int n_blocks, const double *const *sym_list, const int *n_deg,
+                                const int *const *deg_space_list, const int *blocks_ids, int N_configs,
+                                int N_modes, double *f_out, double *d2v_out);
+
+/* Flags of Lanczos.apply_full_L (DynamicalLanczos.py:241-271, 494). */
+typedef struct tdscha_apply_opts {
+    int use_wigner;       /* Wigner representation (a', b') instead of (Upsilon, ReA)         */
+    int ignore_harmonic;  /* drop L1                                                          */
+    int ignore_v3;        /* drop the whole anharmonic part (Python semantics, :3532)          */
+    int ignore_v4;        /* drop the D4 part of the averages                                  */
+    int reverse_L;        /* output *= -1                                                      */
+    double shift_value;   /* output += shift_value * psi                                       */
+} tdscha_apply_opts;
+
+/*
+ * apply_full_L on nb device vectors psi (nb, n + n(n+1)) -> out (nb, n + n(n+1)).
+ * transpose (nb ints, host) selects L or L^T per vector; opts may be NULL (all defaults).
+ */
+int tdscha_apply_full_L_device(tdscha_ensemble *ens, int nb, const double *psi, const int *transpose,
+                               const tdscha_apply_opts *opts, int precision, double *out, void *stream);
+
+/*
+ * One bi-conjugate Lanczos step (DynamicalLanczos.py:6059-6153, n_rep_orth = 0) for nc chains,
+ * all FP64 on the device.  Per chain c the arrays hold vectors of length len:
+ *   Lq, pL        L q_k and L^T p_k;   q, p   current q_k, p_k;   q_prev, p_prev   q_{k-1}, p_{k-1}
+ *   sc_in  (nc, 6) : [c_{k-1}, b_{k-1}, s_norm_k, s_norm_{k-1}, c_{k-2}, step_k]  (step 0 ignores the
+ *                    history terms exactly as the reference's len(basis) checks do)
+ *   mask   optional (len) scalar-product weights (mask_dot_wigner, run_simm), NULL otherwise
+ * Outputs: q_next, p_next (nc, len) and sc_out (nc, 4) = [a_k, b_k, c_k, s_norm_{k+1}].
+ */
+int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const double *pL,
+                               const double *q, const double *p, const double *q_prev,
+                               const double *p_prev, const double *sc_in, const double *mask,
+                               double *q_next, double *p_next, double *sc_out, void *stream);
+
+/*
+ * Continued-fraction Green function (DynamicalLanczos.py:4951-5047) on the device.
+ * a (n_iter), b (n_iter-1 or more), c (same as b or NULL = symmetric) FP64 device arrays;
+ * omega (n_w) device; gf_out (2 * n_w) interleaved re, im.
+ */
+int tdscha_continued_fraction_device(int n_iter, const double *a, const double *b, const double *c,
+                                     int n_b, int n_c, int n_w, const double *omega, int use_terminator,
+                                     int last_average, double smearing, int use_wigner, int reverse_L,
+                                     double shift_value, double perturbation_modulus, double *gf_out,
+                                     void *stream);
+
+/*
+ * The tensor-core contraction used by the averages, exposed for testing and reuse (no counterpart
+ * in the reference): D (M x N, fp32, row-major, leading dimension ldd) = A (M x K) . B (N x K)^T
+ * on device operands stored row-major with K contiguous.  precision TF32 / TF32X3: fp32 elements
+ * already rounded to tf32; BF16 / BF16X3: bf16 elements; the X3 modes also read A_lo / B_lo and
+ * accumulate hi.hi + hi.lo + lo.hi.  K must be a multiple of 64 (bf16) or 32 (tf32); lda / ldb in
+ * elements with 16-byte aligned rows.
+ */
+int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, const void *A_lo, long long lda,
+                       const void *B_hi, const void *B_lo, long long ldb, float *D, long long ldd, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TDSCHA_B200_H */

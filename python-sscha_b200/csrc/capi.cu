@@ -1,0 +1,207 @@
+// capi.cu -- extern "C" entry points declared in include/tdscha_b200.h.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "ensemble.cuh"
+#include "tc_gemm.cuh"
+
+namespace tdscha {
+
+static thread_local char g_err[1024] = "";
+
+void set_error(const char *fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+void clear_error() { g_err[0] = 0; }
+
+int apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose_h, const tdscha_apply_opts *opts,
+                        int precision, double *out, cudaStream_t st, void *scratch, size_t scratch_bytes);
+size_t apply_scratch_bytes(const tdscha_ensemble *e, int nb);
+int lanczos_step_device(int nc, long long len, const double *Lq, const double *pL, const double *q, const double *p,
+                        const double *q_prev, const double *p_prev, const double *sc_in, const double *mask, double *q_next,
+                        double *p_next, double *sc_out, cudaStream_t st, double *scratch, size_t scratch_bytes);
+size_t lanczos_scratch_bytes(int nc);
+int continued_fraction_device(int n_iter, const double *a, const double *b, const double *c, int n_b, int n_c, int n_w,
+                              const double *omega, int use_terminator, int last_average, double smearing, int use_wigner,
+                              int reverse_L, double shift_value, double modulus, double *gf_out, cudaStream_t st);
+
+// Scratch owned by the library for the calls that need temporaries (grown on demand, per device).
+struct Scratch {
+    void *p = nullptr;
+    size_t bytes = 0;
+    int device = -1;
+};
+static thread_local Scratch g_scratch[2];
+
+static int scratch_get(int slot, size_t bytes, void **out) {
+    int dev = 0;
+    TD_CUDA(cudaGetDevice(&dev));
+    Scratch &s = g_scratch[slot];
+    if (s.p && (s.device != dev || s.bytes < bytes)) {
+        int prev = dev;
+        cudaSetDevice(s.device);
+        cudaDeviceSynchronize();
+        cudaFree(s.p);
+        cudaSetDevice(prev);
+        s = Scratch();
+    }
+    if (!s.p) {
+        TD_CUDA(cudaMalloc(&s.p, bytes));
+        s.bytes = bytes;
+        s.device = dev;
+    }
+    *out = s.p;
+    return 0;
+}
+
+static int check_err_word(tdscha_ensemble *e, cudaStream_t st) {
+    unsigned h = 0;
+    TD_CUDA(cudaMemcpyAsync(&h, e->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    TD_CUDA(cudaStreamSynchronize(st));
+    if (h) {
+        cudaMemsetAsync(e->d_err, 0, sizeof(unsigned), st);
+        set_error("a tensor-core kernel hit its bounded-wait limit and aborted (error word 0x%x)", h);
+        return TDSCHA_ETIMEOUT;
+    }
+    return 0;
+}
+
+}  // namespace tdscha
+
+using namespace tdscha;
+
+extern "C" {
+
+const char *tdscha_last_error(void) { return g_err; }
+
+const char *tdscha_version(void) { return "tdscha_b200 0.1.0 (sm_100a)"; }
+
+int tdscha_ensemble_create(const double *X, const double *Y, const double *w, const double *rho, int N, int n, double T,
+                           int N_sym, int n_blocks, const int *n_deg, const int *const *deg_space,
+                           const double *const *sym_blocks, const int *blocks_ids, tdscha_ensemble **out) {
+    clear_error();
+    return ensemble_create(X, Y, w, rho, N, n, T, N_sym, n_blocks, n_deg, deg_space, sym_blocks, blocks_ids, out);
+}
+
+int tdscha_ensemble_destroy(tdscha_ensemble *ens) { return ensemble_destroy(ens); }
+
+int tdscha_ensemble_info(const tdscha_ensemble *e, int *n, int *N, int *N_sym, int *n_blocks, double *T, double *N_eff) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    if (n) *n = e->n;
+    if (N) *N = e->N;
+    if (N_sym) *N_sym = e->N_sym;
+    if (n_blocks) *n_blocks = e->n_blocks;
+    if (T) *T = e->T;
+    if (N_eff) *N_eff = e->N_eff;
+    return 0;
+}
+
+int tdscha_ensemble_device_bytes(const tdscha_ensemble *e, long long *bytes) {
+    TD_CHECK(e != nullptr && bytes != nullptr, TDSCHA_EINVAL, "NULL argument");
+    size_t b = e->base_bytes + e->ws.bytes;
+    for (const auto &o : e->ops) b += o.bytes;
+    *bytes = (long long)b;
+    return 0;
+}
+
+int tdscha_perturb_average_sym_device(tdscha_ensemble *e, int nb, const double *R1, const double *Y1, int apply_d4,
+                                      int precision, double *f_out, double *d2v_out, void *stream) {
+    clear_error();
+    TD_CHECK(e && R1 && Y1 && f_out && d2v_out, TDSCHA_EINVAL, "NULL argument");
+    TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+    TD_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    void *ys = nullptr;
+    TD_TRY(scratch_get(0, (size_t)nb * e->n * e->n * sizeof(double), &ys));
+    TD_TRY(symmetrize_device(nb, e->n, Y1, static_cast<double *>(ys), st));
+    TD_TRY(perturb_average_device(e, nb, R1, static_cast<const double *>(ys), apply_d4, precision, f_out, d2v_out, st));
+    return check_err_word(e, st);
+}
+
+int tdscha_perturb_average_sym(tdscha_ensemble *e, const double *R1, const double *Y1, int apply_d4, int precision,
+                               double *f_out, double *d2v_out) {
+    clear_error();
+    TD_CHECK(e && R1 && Y1 && f_out && d2v_out, TDSCHA_EINVAL, "NULL argument");
+    TD_CUDA(cudaSetDevice(e->device));
+    const size_t n = e->n;
+    void *buf = nullptr;
+    TD_TRY(scratch_get(1, (2 * n + 2 * n * n) * sizeof(double), &buf));
+    double *dR = static_cast<double *>(buf), *dY = dR + n, *df = dY + n * n, *dD = df + n;
+    TD_CUDA(cudaMemcpy(dR, R1, n * sizeof(double), cudaMemcpyHostToDevice));
+    TD_CUDA(cudaMemcpy(dY, Y1, n * n * sizeof(double), cudaMemcpyHostToDevice));
+    TD_TRY(tdscha_perturb_average_sym_device(e, 1, dR, dY, apply_d4, precision, df, dD, nullptr));
+    TD_CUDA(cudaMemcpy(f_out, df, n * sizeof(double), cudaMemcpyDeviceToHost));
+    TD_CUDA(cudaMemcpy(d2v_out, dD, n * n * sizeof(double), cudaMemcpyDeviceToHost));
+    return 0;
+}
+
+int tdscha_GetPerturbAverageSym(const double *X, const double *Y, const double *w, const double *rho, const double *R1,
+                                const double *Y1, double T, int apply_D4, int N_syms, int n_blocks,
+                                const double *const *sym_list, const int *n_deg, const int *const *deg_space_list,
+                                const int *blocks_ids, int N_configs, int N_modes, double *f_out, double *d2v_out) {
+    clear_error();
+    TD_CHECK(apply_D4 == 0 || apply_D4 == 1, TDSCHA_EINVAL, "the apply_D4 value passed must be either 0 or 1 (got %d)", apply_D4);
+    tdscha_ensemble *e = nullptr;
+    TD_TRY(ensemble_create(X, Y, w, rho, N_configs, N_modes, T, N_syms, n_blocks, n_deg, deg_space_list, sym_list, blocks_ids, &e));
+    int rc = tdscha_perturb_average_sym(e, R1, Y1, apply_D4, TDSCHA_PREC_FP64, f_out, d2v_out);
+    ensemble_destroy(e);
+    return rc;
+}
+
+int tdscha_apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose,
+                               const tdscha_apply_opts *opts, int precision, double *out, void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t need = apply_scratch_bytes(e, nb);
+    void *buf = nullptr;
+    TD_TRY(scratch_get(0, need, &buf));
+    TD_TRY(apply_full_L_device(e, nb, psi, transpose, opts, precision, out, st, buf, need));
+    return check_err_word(e, st);
+}
+
+int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const double *pL, const double *q, const double *p,
+                               const double *q_prev, const double *p_prev, const double *sc_in, const double *mask,
+                               double *q_next, double *p_next, double *sc_out, void *stream) {
+    clear_error();
+    const size_t need = lanczos_scratch_bytes(nc);
+    void *buf = nullptr;
+    TD_TRY(scratch_get(1, need, &buf));
+    return lanczos_step_device(nc, len, Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_out,
+                               static_cast<cudaStream_t>(stream), static_cast<double *>(buf), need);
+}
+
+int tdscha_continued_fraction_device(int n_iter, const double *a, const double *b, const double *c, int n_b, int n_c, int n_w,
+                                     const double *omega, int use_terminator, int last_average, double smearing,
+                                     int use_wigner, int reverse_L, double shift_value, double perturbation_modulus,
+                                     double *gf_out, void *stream) {
+    clear_error();
+    return continued_fraction_device(n_iter, a, b, c, n_b, n_c, n_w, omega, use_terminator, last_average, smearing, use_wigner,
+                                     reverse_L, shift_value, perturbation_modulus, gf_out, static_cast<cudaStream_t>(stream));
+}
+
+int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, const void *A_lo, long long lda,
+                       const void *B_hi, const void *B_lo, long long ldb, float *D, long long ldd, void *stream) {
+    clear_error();
+    TD_CHECK(precision != TDSCHA_PREC_FP64 && precision >= 0 && precision <= TDSCHA_PREC_BF16, TDSCHA_EINVAL,
+             "tdscha_tc_contract: precision %d is not a tensor-core mode", precision);
+    static thread_local unsigned *err = nullptr;
+    if (!err) TD_CUDA(cudaMalloc(&err, sizeof(unsigned)));
+    TD_CUDA(cudaMemsetAsync(err, 0, sizeof(unsigned), static_cast<cudaStream_t>(stream)));
+    tc::GemmOperands op{format_of(precision), products_of(precision), A_hi, A_lo, lda, B_hi, B_lo, ldb};
+    TD_TRY(tc::gemm(op, M, N, K, D, ldd, static_cast<cudaStream_t>(stream), err));
+    unsigned h = 0;
+    TD_CUDA(cudaMemcpyAsync(&h, err, sizeof(unsigned), cudaMemcpyDeviceToHost, static_cast<cudaStream_t>(stream)));
+    TD_CUDA(cudaStreamSynchronize(static_cast<cudaStream_t>(stream)));
+    TD_CHECK(h == 0, TDSCHA_ETIMEOUT, "tensor-core contraction hit its bounded-wait limit (error word 0x%x)", h);
+    return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,646 @@
+// ensemble.cu -- resident ensemble, operand builders, symmetry transform/fold kernels and the
+// orchestration of the symmetrised perturbed averages (the algebra is in ensemble.cuh).
+#include <cublas_v2.h>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "common.cuh"
+#include "ensemble.cuh"
+#include "tc_gemm.cuh"
+
+namespace tdscha {
+
+constexpr int SYM_THREADS = 256;
+constexpr int FOLD_MAXE = 36;     // accumulator elements per thread: d_b * d_c <= 36 * 256 (dmax 96)
+constexpr int DMAX_SUPPORTED = 96;
+
+// ------------------------------------------------------------------------------------------------
+// operand builders (once per ensemble and storage format)
+// ------------------------------------------------------------------------------------------------
+// V (2N x Kp): rows < N -> c_p x_mu x_nu ; rows >= N -> x_mu g_nu + x_nu g_mu (x g on the diagonal)
+__global__ void build_V_kernel(const double *__restrict__ X, const double *__restrict__ G,
+                               const int *__restrict__ pmu, const int *__restrict__ pnu, int N, int n,
+                               long long P, long long Kp, Format fmt, void *hi, void *lo) {
+    const long long total = 2LL * N * Kp;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx / Kp, p = idx % Kp;
+        double v = 0.0;
+        if (p < P) {
+            const int mu = pmu[p], nu = pnu[p];
+            if (k < N) {
+                const double *x = X + k * n;
+                v = (mu == nu ? 1.0 : 2.0) * x[mu] * x[nu];
+            } else {
+                const double *x = X + (k - N) * n;
+                const double *g = G + (k - N) * n;
+                v = (mu == nu) ? x[mu] * g[mu] : x[mu] * g[nu] + x[nu] * g[mu];
+            }
+        }
+        store_split(fmt, hi, lo, idx, v);
+    }
+}
+
+// VT (P x N2p) = V^T with zero columns beyond 2N
+__global__ void build_VT_kernel(const double *__restrict__ X, const double *__restrict__ G,
+                                const int *__restrict__ pmu, const int *__restrict__ pnu, int N, int n,
+                                long long P, long long N2p, Format fmt, void *hi, void *lo) {
+    const long long total = P * N2p;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long p = idx / N2p, k = idx % N2p;
+        const int mu = pmu[p], nu = pnu[p];
+        double v = 0.0;
+        if (k < N) {
+            const double *x = X + k * n;
+            v = (mu == nu ? 1.0 : 2.0) * x[mu] * x[nu];
+        } else if (k < 2LL * N) {
+            const double *x = X + (k - N) * n;
+            const double *g = G + (k - N) * n;
+            v = (mu == nu) ? x[mu] * g[mu] : x[mu] * g[nu] + x[nu] * g[mu];
+        }
+        store_split(fmt, hi, lo, idx, v);
+    }
+}
+
+// XG (2N x np) = [X ; G] ; YXt (n x N2p) = [Y^T | X~^T]
+__global__ void build_XG_kernel(const double *X, const double *G, int N, int n, long long np, Format fmt, void *hi, void *lo) {
+    const long long total = 2LL * N * np;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx / np, m = idx % np;
+        double v = 0.0;
+        if (m < n) v = (k < N) ? X[k * n + m] : G[(k - N) * n + m];
+        store_split(fmt, hi, lo, idx, v);
+    }
+}
+__global__ void build_YXt_kernel(const double *Y, const double *Xt, int N, int n, long long N2p, Format fmt, void *hi, void *lo) {
+    const long long total = (long long)n * N2p;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long m = idx / N2p, k = idx % N2p;
+        double v = 0.0;
+        if (k < N) v = Y[k * n + m];
+        else if (k < 2LL * N) v = Xt[(k - N) * n + m];
+        store_split(fmt, hi, lo, idx, v);
+    }
+}
+
+__global__ void thermal_kernel(const double *w, int n, double T, double *ups, double *psi) {
+    int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    double nb = T > 0 ? 1.0 / (exp(w[m] * RY_TO_K / T) - 1.0) : 0.0;
+    ups[m] = 2.0 * w[m] / (1.0 + 2.0 * nb);
+    psi[m] = (1.0 + 2.0 * nb) / (2.0 * w[m]);
+}
+
+__global__ void scale_rows_kernel(const double *A, const double *s, int N, int n, double *out) {
+    long long total = (long long)N * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x)
+        out[idx] = A[idx] * s[idx % n];
+}
+
+__global__ void symmetrize_kernel(int nb, int n, const double *Y, double *Ys) {
+    long long total = (long long)nb * n * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        long long k = idx / ((long long)n * n), e = idx % ((long long)n * n);
+        int r = (int)(e / n), c = (int)(e % n);
+        const double *Yk = Y + k * n * n;
+        Ys[idx] = 0.5 * (Yk[(long long)r * n + c] + Yk[(long long)c * n + r]);
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// symmetry transform: B1[r, p(mu,nu)] = (S_j^T Ys_k S_j)[mu, nu]  and  r1[r, mu] = ups_mu (S_j^T R1_k)_mu
+//   grid (rows r = k*Jc + jj, blocks b); the CTA owns the row block b of Y~_j, all column blocks c >= b.
+// ------------------------------------------------------------------------------------------------
+struct SymTables {
+    const double *sym;
+    const long long *off;
+    const int *start, *dim;
+    int n_blocks, n, dmax;
+};
+
+__device__ __forceinline__ long long pair_index(int mu, int nu, int n) {   // mu <= nu
+    return (long long)mu * n - ((long long)mu * (mu - 1)) / 2 + (nu - mu);
+}
+
+__global__ void __launch_bounds__(SYM_THREADS)
+transform_kernel(SymTables t, const double *__restrict__ Ys, const double *__restrict__ R1, const double *__restrict__ ups,
+                 int Jc, int j0, long long P, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo,
+                 void *r1_hi, void *r1_lo) {
+    extern __shared__ double sm[];
+    const int dmax = t.dmax;
+    double *Sb = sm;                   // d_b x d_b
+    double *Sc = Sb + dmax * dmax;     // d_c x d_c
+    double *tmp = Sc + dmax * dmax;    // d_b x d_c
+    const int r = blockIdx.x, b = blockIdx.y;
+    const int k = r / Jc, j = j0 + r % Jc;
+    const int n = t.n;
+    const int sb = t.start[b], db = t.dim[b];
+    const double *Yk = Ys + (long long)k * n * n;
+    const double *Rk = R1 + (long long)k * n;
+    const double *Sbg = t.sym + t.off[b] + (long long)j * db * db;
+    for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = Sbg[e];
+    if (b == 0) {   // zero padding columns of this row
+        for (long long p = P + threadIdx.x; p < Kp; p += blockDim.x) store_split(fmt, B1_hi, B1_lo, (long long)r * Kp + p, 0.0);
+        for (long long m = n + threadIdx.x; m < np; m += blockDim.x) store_split(fmt, r1_hi, r1_lo, (long long)r * np + m, 0.0);
+    }
+    __syncthreads();
+    // r1 for the modes of block b:  (S_j^T R)_mu' = sum_p' S_b[p', mu'] R[sb + p']
+    for (int mu = threadIdx.x; mu < db; mu += blockDim.x) {
+        double acc = 0.0;
+        for (int p = 0; p < db; ++p) acc += Sb[p * db + mu] * Rk[sb + p];
+        store_split(fmt, r1_hi, r1_lo, (long long)r * np + sb + mu, ups[sb + mu] * acc);
+    }
+    for (int c = b; c < t.n_blocks; ++c) {
+        const int sc = t.start[c], dc = t.dim[c];
+        const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
+        __syncthreads();
+        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) Sc[e] = Scg[e];
+        __syncthreads();
+        // tmp[p', nu'] = sum_q' Ys[sb + p', sc + q'] S_c[q', nu']
+        for (int e = threadIdx.x; e < db * dc; e += blockDim.x) {
+            const int p = e / dc, nu = e % dc;
+            const double *yrow = Yk + (long long)(sb + p) * n + sc;
+            double acc = 0.0;
+            for (int q = 0; q < dc; ++q) acc += yrow[q] * Sc[q * dc + nu];
+            tmp[e] = acc;
+        }
+        __syncthreads();
+        // out[mu', nu'] = sum_p' S_b[p', mu'] tmp[p', nu']
+        for (int e = threadIdx.x; e < db * dc; e += blockDim.x) {
+            const int mu = e / dc, nu = e % dc;
+            const int gm = sb + mu, gn = sc + nu;
+            if (gm > gn) continue;
+            double acc = 0.0;
+            for (int p = 0; p < db; ++p) acc += Sb[p * db + mu] * tmp[p * dc + nu];
+            store_split(fmt, B1_hi, B1_lo, (long long)r * Kp + pair_index(gm, gn, n), acc);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// weights: from [a | b] (D1) and [c | d] (Dcd) build Cw = [delta/2 | gamma] and AB = [alpha | beta]
+// ------------------------------------------------------------------------------------------------
+template <typename AccT>
+__global__ void weights_kernel(const AccT *__restrict__ D1, const AccT *__restrict__ Dcd, long long ld, const double *__restrict__ rho,
+                               int N, int M, long long N2p, int d4, Format fmt, void *Cw_hi, void *Cw_lo, void *AB_hi,
+                               void *AB_lo) {
+    const long long per_row = N + (N2p - 2LL * N);
+    const long long total = (long long)M * per_row;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / per_row, i = idx % per_row;
+        if (i < N) {
+            const double a = (double)D1[r * ld + i], b = (double)D1[r * ld + N + i];
+            const double c = (double)Dcd[r * ld + i], d = (double)Dcd[r * ld + N + i];
+            const double rh = rho[i];
+            const double gam = rh * (-c / 3.0 + (d4 ? a / 8.0 : 0.0));
+            const double del = rh * (-d / 3.0 + (d4 ? b / 4.0 : 0.0));
+            store_split(fmt, Cw_hi, Cw_lo, r * N2p + i, 0.5 * del);
+            store_split(fmt, Cw_hi, Cw_lo, r * N2p + N + i, gam);
+            store_split(fmt, AB_hi, AB_lo, r * N2p + i, -rh * a / 6.0);
+            store_split(fmt, AB_hi, AB_lo, r * N2p + N + i, -rh * b / 3.0);
+        } else {
+            const long long col = 2LL * N + (i - N);
+            store_split(fmt, Cw_hi, Cw_lo, r * N2p + col, 0.0);
+            store_split(fmt, AB_hi, AB_lo, r * N2p + col, 0.0);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// fold: partial[k][f] (block b, c) = sum_{j in chunk f} S_j W_j S_j^T  (and f partials on diagonal pairs)
+//   W_j[mu,nu] = e ups_mu ups_nu Z[r, p(mu,nu)]
+// ------------------------------------------------------------------------------------------------
+template <typename AccT>
+__global__ void __launch_bounds__(SYM_THREADS)
+fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ bp_c, const AccT *__restrict__ Z, long long ldz,
+            const AccT *__restrict__ F, long long ldf, const double *__restrict__ ups, int Jc, int j0, int nj, int Jf, int nf_total,
+            double *__restrict__ partD, double *__restrict__ partF) {
+    extern __shared__ double sm[];
+    const int dmax = t.dmax;
+    double *Sb = sm;
+    double *Sc = Sb + dmax * dmax;
+    double *Wt = Sc + dmax * dmax;
+    double *tmp = Wt + dmax * dmax;
+    const int b = bp_b[blockIdx.x], c = bp_c[blockIdx.x];
+    const int fc = blockIdx.y, k = blockIdx.z;
+    const int n = t.n;
+    const int sb = t.start[b], db = t.dim[b], sc = t.start[c], dc = t.dim[c];
+    const int fg = j0 / Jf + fc;
+    const int ja = j0 + fc * Jf, jb = min(j0 + (fc + 1) * Jf, j0 + nj);
+    const int ne = db * dc;
+    double acc[FOLD_MAXE];
+#pragma unroll
+    for (int u = 0; u < FOLD_MAXE; ++u) acc[u] = 0.0;
+    double facc = 0.0;   // f partial for mode sb + threadIdx.x (diagonal pairs only)
+    for (int j = ja; j < jb; ++j) {
+        const long long r = (long long)k * Jc + (j - j0);
+        const double *Sbg = t.sym + t.off[b] + (long long)j * db * db;
+        const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
+        __syncthreads();
+        for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = Sbg[e];
+        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) Sc[e] = Scg[e];
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int p = e / dc, q = e % dc;
+            int gm = sb + p, gn = sc + q;
+            if (gm > gn) { int s = gm; gm = gn; gn = s; }
+            const double z = (double)Z[r * ldz + pair_index(gm, gn, n)];
+            Wt[e] = (gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn] * z;
+        }
+        __syncthreads();
+        // tmp = W S_c^T : tmp[p, nu] = sum_q W[p, q] S_c[nu, q]
+        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
+            const int p = e / dc, nu = e % dc;
+            double s = 0.0;
+            for (int q = 0; q < dc; ++q) s += Wt[p * dc + q] * Sc[nu * dc + q];
+            tmp[e] = s;
+        }
+        if (b == c && threadIdx.x < db) {
+            const AccT *Fr = F + r * ldf + sb;
+            double s = 0.0;
+            for (int p = 0; p < db; ++p) s += Sb[threadIdx.x * db + p] * (double)Fr[p];
+            facc += s;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int u = 0; u < FOLD_MAXE; ++u) {
+            const int e = threadIdx.x + u * SYM_THREADS;
+            if (e < ne) {
+                const int mu = e / dc, nu = e % dc;
+                double s = 0.0;
+                for (int p = 0; p < db; ++p) s += Sb[mu * db + p] * tmp[p * dc + nu];
+                acc[u] += s;
+            }
+        }
+    }
+    double *out = partD + ((long long)k * nf_total + fg) * (long long)n * n;
+#pragma unroll
+    for (int u = 0; u < FOLD_MAXE; ++u) {
+        const int e = threadIdx.x + u * SYM_THREADS;
+        if (e < ne) out[(long long)(sb + e / dc) * n + sc + e % dc] = acc[u];
+    }
+    if (b == c && threadIdx.x < db) partF[((long long)k * nf_total + fg) * n + sb + threadIdx.x] = facc;
+}
+
+__global__ void fold_reduce_kernel(const double *partD, const double *partF, int nf, int n, int nb,
+                                   const int *blocks_ids, double norm, double *D_out, double *f_out) {
+    const long long nn = (long long)n * n;
+    const long long total = (long long)nb * nn;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx / nn, e = idx % nn;
+        int mu = (int)(e / n), nu = (int)(e % n);
+        if (blocks_ids[mu] > blocks_ids[nu]) { int s = mu; mu = nu; nu = s; }
+        const double *src = partD + k * nf * nn + (long long)mu * n + nu;
+        double s = 0.0;
+        for (int f = 0; f < nf; ++f) s += src[f * nn];
+        D_out[idx] = s * norm;
+    }
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < (long long)nb * n;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx / n, m = idx % n;
+        double s = 0.0;
+        for (int f = 0; f < nf; ++f) s += partF[(k * nf + f) * n + m];
+        f_out[idx] = s * norm;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host orchestration
+// ------------------------------------------------------------------------------------------------
+static int grid_for(long long total, int threads = 256) {
+    long long g = (total + threads - 1) / threads;
+    return (int)std::min<long long>(std::max<long long>(g, 1), 148LL * 32);
+}
+
+static int dev_alloc(void **p, size_t bytes, size_t *acc) {
+    TD_CUDA(cudaMalloc(p, bytes));
+    if (acc) *acc += bytes;
+    return 0;
+}
+
+int symmetrize_device(int nb, int n, const double *Y, double *Ys, cudaStream_t st) {
+    symmetrize_kernel<<<grid_for((long long)nb * n * n), 256, 0, st>>>(nb, n, Y, Ys);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int ensemble_create(const double *X, const double *Y, const double *w, const double *rho, int N, int n, double T,
+                    int N_sym, int n_blocks, const int *n_deg, const int *const *deg_space,
+                    const double *const *sym_blocks, const int *blocks_ids, tdscha_ensemble **out) {
+    TD_CHECK(out != nullptr, TDSCHA_EINVAL, "out handle pointer is NULL");
+    *out = nullptr;
+    TD_CHECK(X && Y && w && rho && n_deg && deg_space && sym_blocks && blocks_ids, TDSCHA_EINVAL, "NULL input array");
+    TD_CHECK(N > 0 && n > 0 && N_sym > 0 && n_blocks > 0 && n_blocks <= n, TDSCHA_EINVAL,
+             "bad sizes N=%d n=%d N_sym=%d n_blocks=%d", N, n, N_sym, n_blocks);
+    int dev = 0;
+    TD_CUDA(cudaGetDevice(&dev));
+    cudaDeviceProp prop;
+    TD_CUDA(cudaGetDeviceProperties(&prop, dev));
+    TD_CHECK(prop.major == 10, TDSCHA_ENOSUPPORT, "device %d is sm_%d%d; this library is built for sm_100a", dev, prop.major, prop.minor);
+
+    // validate the block structure (contiguous, ascending, covering 0..n-1 in order) and degeneracy
+    std::vector<int> start(n_blocks), dim(n_blocks);
+    int expect = 0, dmax = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        TD_CHECK(n_deg[b] > 0 && deg_space[b] && sym_blocks[b], TDSCHA_EINVAL, "block %d empty", b);
+        start[b] = deg_space[b][0];
+        dim[b] = n_deg[b];
+        TD_CHECK(start[b] == expect, TDSCHA_EINVAL,
+                 "degenerate blocks must be contiguous and ordered: block %d starts at mode %d, expected %d", b, start[b], expect);
+        for (int q = 0; q < n_deg[b]; ++q)
+            TD_CHECK(deg_space[b][q] == start[b] + q, TDSCHA_EINVAL, "block %d is not a contiguous ascending mode range", b);
+        double wmin = w[start[b]], wmax = w[start[b]];
+        for (int q = 0; q < n_deg[b]; ++q) {
+            TD_CHECK(blocks_ids[start[b] + q] == b, TDSCHA_EINVAL, "blocks_ids[%d] != %d", start[b] + q, b);
+            wmin = std::min(wmin, w[start[b] + q]);
+            wmax = std::max(wmax, w[start[b] + q]);
+        }
+        TD_CHECK(wmax - wmin <= 1e-10 * std::fabs(wmax), TDSCHA_EINVAL,
+                 "block %d is not degenerate: frequency spread %.3e (relative) > 1e-10", b, (wmax - wmin) / std::fabs(wmax));
+        expect += n_deg[b];
+        dmax = std::max(dmax, n_deg[b]);
+    }
+    TD_CHECK(expect == n, TDSCHA_EINVAL, "blocks cover %d modes, n = %d", expect, n);
+    TD_CHECK(dmax <= DMAX_SUPPORTED, TDSCHA_EINVAL, "degenerate block of %d modes exceeds the supported %d", dmax, DMAX_SUPPORTED);
+    for (int m = 0; m < n; ++m) TD_CHECK(w[m] > 0, TDSCHA_EINVAL, "frequency %d is not positive (%g)", m, w[m]);
+
+    auto *e = new tdscha_ensemble();
+    e->device = dev;
+    e->n = n; e->N = N; e->N_sym = N_sym; e->n_blocks = n_blocks; e->T = T; e->dmax = dmax;
+    e->P = (long long)n * (n + 1) / 2;
+    e->Kp = round_up(e->P, 64);
+    e->N2 = 2LL * N;
+    e->N2p = round_up(e->N2, 64);
+    e->np = round_up(n, 64);
+    e->blk_start = start; e->blk_dim = dim;
+    e->blk_sym_off.resize(n_blocks);
+    long long soff = 0;
+    for (int b = 0; b < n_blocks; ++b) { e->blk_sym_off[b] = soff; soff += (long long)N_sym * dim[b] * dim[b]; }
+    for (int b = 0; b < n_blocks; ++b)
+        for (int c = b; c < n_blocks; ++c) { e->bp_b.push_back(b); e->bp_c.push_back(c); }
+    double neff = 0;
+    for (int i = 0; i < N; ++i) neff += rho[i];
+    e->N_eff = neff;
+
+    auto fail = [&](int rc) { ensemble_destroy(e); return rc; };
+    size_t acc = 0;
+    const size_t xb = (size_t)N * n * sizeof(double);
+    int rc;
+    if ((rc = dev_alloc((void **)&e->X, xb, &acc)) || (rc = dev_alloc((void **)&e->Y, xb, &acc)) ||
+        (rc = dev_alloc((void **)&e->G, xb, &acc)) || (rc = dev_alloc((void **)&e->Xt, xb, &acc)) ||
+        (rc = dev_alloc((void **)&e->rho, N * sizeof(double), &acc)) || (rc = dev_alloc((void **)&e->w, n * sizeof(double), &acc)) ||
+        (rc = dev_alloc((void **)&e->ups, n * sizeof(double), &acc)) || (rc = dev_alloc((void **)&e->psi, n * sizeof(double), &acc)) ||
+        (rc = dev_alloc((void **)&e->sym, soff * sizeof(double), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_blk_start, n_blocks * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_blk_dim, n_blocks * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_blk_sym_off, n_blocks * sizeof(long long), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_blocks_ids, n * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_bp_b, e->bp_b.size() * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_bp_c, e->bp_c.size() * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_pair_mu, e->P * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_pair_nu, e->P * sizeof(int), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_err, sizeof(unsigned), &acc)))
+        return fail(rc);
+    e->base_bytes = acc;
+    std::vector<int> pmu(e->P), pnu(e->P);
+    {
+        long long p = 0;
+        for (int mu = 0; mu < n; ++mu)
+            for (int nu = mu; nu < n; ++nu) { pmu[p] = mu; pnu[p] = nu; ++p; }
+    }
+#define TD_UP(dst, src, bytes)                                                         \
+    do {                                                                               \
+        cudaError_t ce = cudaMemcpy((dst), (src), (bytes), cudaMemcpyHostToDevice);    \
+        if (ce != cudaSuccess) { set_error("upload: %s", cudaGetErrorString(ce)); return fail(TDSCHA_ECUDA); } \
+    } while (0)
+    TD_UP(e->X, X, xb);
+    TD_UP(e->Y, Y, xb);
+    TD_UP(e->rho, rho, N * sizeof(double));
+    TD_UP(e->w, w, n * sizeof(double));
+    for (int b = 0; b < n_blocks; ++b)
+        TD_UP(e->sym + e->blk_sym_off[b], sym_blocks[b], (size_t)N_sym * dim[b] * dim[b] * sizeof(double));
+    TD_UP(e->d_blk_start, start.data(), n_blocks * sizeof(int));
+    TD_UP(e->d_blk_dim, dim.data(), n_blocks * sizeof(int));
+    TD_UP(e->d_blk_sym_off, e->blk_sym_off.data(), n_blocks * sizeof(long long));
+    TD_UP(e->d_blocks_ids, blocks_ids, n * sizeof(int));
+    TD_UP(e->d_bp_b, e->bp_b.data(), e->bp_b.size() * sizeof(int));
+    TD_UP(e->d_bp_c, e->bp_c.data(), e->bp_c.size() * sizeof(int));
+    TD_UP(e->d_pair_mu, pmu.data(), e->P * sizeof(int));
+    TD_UP(e->d_pair_nu, pnu.data(), e->P * sizeof(int));
+#undef TD_UP
+    if (cudaMemset(e->d_err, 0, sizeof(unsigned)) != cudaSuccess) return fail(TDSCHA_ECUDA);
+    thermal_kernel<<<ceil_div(n, 128), 128>>>(e->w, n, T, e->ups, e->psi);
+    scale_rows_kernel<<<grid_for((long long)N * n), 256>>>(e->Y, e->psi, N, n, e->G);
+    scale_rows_kernel<<<grid_for((long long)N * n), 256>>>(e->X, e->ups, N, n, e->Xt);
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
+        set_error("ensemble set-up kernels failed");
+        return fail(TDSCHA_ECUDA);
+    }
+    if (cublasCreate(&e->cublas) != CUBLAS_STATUS_SUCCESS) {
+        set_error("cublasCreate failed");
+        return fail(TDSCHA_ECUDA);
+    }
+    *out = e;
+    return 0;
+}
+
+static void free_ops(OperandSet &o) {
+    void *ps[] = {o.V_hi, o.V_lo, o.VT_hi, o.VT_lo, o.XG_hi, o.XG_lo, o.YXt_hi, o.YXt_lo};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    o = OperandSet();
+}
+
+int ensemble_destroy(tdscha_ensemble *e) {
+    if (!e) return 0;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(e->device);
+    cudaDeviceSynchronize();
+    void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->d_blk_start, e->d_blk_dim,
+                  e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    for (auto &o : e->ops) free_ops(o);
+    if (e->cublas) cublasDestroy(e->cublas);
+    delete e;
+    cudaSetDevice(prev);
+    return 0;
+}
+
+// Build (once) the V / VT / XG / YXt operands in storage format fmt; lo splits when with_lo.
+static int ensure_operands(tdscha_ensemble *e, Format fmt, bool with_lo, cudaStream_t st) {
+    OperandSet &o = e->ops[fmt];
+    if (o.built && (o.has_lo || !with_lo)) return 0;
+    free_ops(o);
+    const size_t es = format_bytes(fmt);
+    const long long nV = e->N2 * e->Kp, nVT = e->P * e->N2p, nXG = e->N2 * e->np, nYX = (long long)e->n * e->N2p;
+    size_t acc = 0;
+    TD_TRY(dev_alloc(&o.V_hi, nV * es, &acc));
+    TD_TRY(dev_alloc(&o.VT_hi, nVT * es, &acc));
+    TD_TRY(dev_alloc(&o.XG_hi, nXG * es, &acc));
+    TD_TRY(dev_alloc(&o.YXt_hi, nYX * es, &acc));
+    if (with_lo) {
+        TD_TRY(dev_alloc(&o.V_lo, nV * es, &acc));
+        TD_TRY(dev_alloc(&o.VT_lo, nVT * es, &acc));
+        TD_TRY(dev_alloc(&o.XG_lo, nXG * es, &acc));
+        TD_TRY(dev_alloc(&o.YXt_lo, nYX * es, &acc));
+    }
+    build_V_kernel<<<grid_for(nV), 256, 0, st>>>(e->X, e->G, e->d_pair_mu, e->d_pair_nu, e->N, e->n, e->P, e->Kp, fmt, o.V_hi, o.V_lo);
+    build_VT_kernel<<<grid_for(nVT), 256, 0, st>>>(e->X, e->G, e->d_pair_mu, e->d_pair_nu, e->N, e->n, e->P, e->N2p, fmt, o.VT_hi, o.VT_lo);
+    build_XG_kernel<<<grid_for(nXG), 256, 0, st>>>(e->X, e->G, e->N, e->n, e->np, fmt, o.XG_hi, o.XG_lo);
+    build_YXt_kernel<<<grid_for(nYX), 256, 0, st>>>(e->Y, e->Xt, e->N, e->n, e->N2p, fmt, o.YXt_hi, o.YXt_lo);
+    TD_CUDA(cudaGetLastError());
+    o.built = true;
+    o.has_lo = with_lo;
+    o.bytes = acc;
+    return 0;
+}
+
+// Layout of one call's workspace for M = nb * Jc rows.
+struct WsLayout {
+    size_t B1_hi, B1_lo, r1_hi, r1_lo, D1, Dcd, Cw_hi, Cw_lo, AB_hi, AB_lo, Z, F, partD, partF, total;
+    long long ld1, ldz, ldf;
+};
+
+static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, Format fmt, bool lo) {
+    WsLayout L{};
+    const size_t es = format_bytes(fmt);
+    const size_t as = (fmt == FMT_F64) ? 8 : 4;
+    const long long M = (long long)nb * Jc;
+    L.ld1 = round_up(e->N2, 4);
+    L.ldz = round_up(e->P, 4);
+    L.ldf = round_up(e->n, 4);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    L.B1_hi = take(M * e->Kp * es);
+    L.B1_lo = lo ? take(M * e->Kp * es) : 0;
+    L.r1_hi = take(M * e->np * es);
+    L.r1_lo = lo ? take(M * e->np * es) : 0;
+    L.D1 = take(M * L.ld1 * as);
+    L.Dcd = take(M * L.ld1 * as);
+    L.Cw_hi = take(M * e->N2p * es);
+    L.Cw_lo = lo ? take(M * e->N2p * es) : 0;
+    L.AB_hi = take(M * e->N2p * es);
+    L.AB_lo = lo ? take(M * e->N2p * es) : 0;
+    L.Z = take(M * L.ldz * as);
+    L.F = take(M * L.ldf * as);
+    L.partD = take((size_t)nb * nf_total * e->n * e->n * 8);
+    L.partF = take((size_t)nb * nf_total * e->n * 8);
+    L.total = off;
+    return L;
+}
+
+static int ensure_ws(tdscha_ensemble *e, size_t bytes) {
+    if (e->ws.bytes >= bytes) return 0;
+    if (e->ws.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->ws.base); e->ws = Workspace(); }
+    TD_CUDA(cudaMalloc(&e->ws.base, bytes));
+    e->ws.bytes = bytes;
+    return 0;
+}
+
+// C (M x N) row-major = A (M x K) . B (N x K)^T
+static int gemm_abt(tdscha_ensemble *e, Format fmt, int nprod, const void *A_hi, const void *A_lo, long long lda, long long M,
+                    const void *B_hi, const void *B_lo, long long ldb, long long N, long long K, void *Cout, long long ldc,
+                    cudaStream_t st) {
+    if (fmt == FMT_F64) {
+        const double one = 1.0, zero = 0.0;
+        cublasSetStream(e->cublas, st);
+        cublasStatus_t s = cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)N, (int)M, (int)K, &one,
+                                       static_cast<const double *>(B_hi), (int)ldb, static_cast<const double *>(A_hi), (int)lda,
+                                       &zero, static_cast<double *>(Cout), (int)ldc);
+        TD_CHECK(s == CUBLAS_STATUS_SUCCESS, TDSCHA_ECUDA, "cublasDgemm failed (%d)", (int)s);
+        return 0;
+    }
+    tc::GemmOperands op{fmt, nprod, A_hi, A_lo, lda, B_hi, B_lo, ldb};
+    return tc::gemm(op, (int)M, (int)N, (int)K, static_cast<float *>(Cout), ldc, st, e->d_err);
+}
+
+int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4, int precision,
+                           double *f_out, double *d_out, cudaStream_t st) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+    TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);
+    TD_CHECK(precision >= TDSCHA_PREC_FP64 && precision <= TDSCHA_PREC_BF16, TDSCHA_EINVAL, "unknown precision %d", precision);
+    const Format fmt = format_of(precision);
+    const int nprod = products_of(precision);
+    const bool lo = needs_lo(precision);
+    TD_TRY(ensure_operands(e, fmt, lo, st));
+    OperandSet &o = e->ops[fmt];
+
+    // fold chunking over symmetries: Jf symmetries per partial, at most 64 partials
+    const int Jf = std::max(16, ceil_div(e->N_sym, 64));
+    const int nf_total = ceil_div(e->N_sym, Jf);
+    // GEMM chunk over symmetries: a multiple of Jf whose workspace fits in the budget
+    size_t free_b = 0, tot_b = 0;
+    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
+    int Jc = (int)round_up(e->N_sym, Jf);
+    while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo).total > budget) Jc = (int)round_up(Jc / 2, Jf);
+    const WsLayout L = layout(e, nb, Jc, nf_total, fmt, lo);
+    TD_TRY(ensure_ws(e, L.total));
+    uint8_t *W = static_cast<uint8_t *>(e->ws.base);
+    void *B1_hi = W + L.B1_hi, *B1_lo = lo ? W + L.B1_lo : nullptr;
+    void *r1_hi = W + L.r1_hi, *r1_lo = lo ? W + L.r1_lo : nullptr;
+    void *D1 = W + L.D1, *Dcd = W + L.Dcd, *Z = W + L.Z, *F = W + L.F;
+    void *Cw_hi = W + L.Cw_hi, *Cw_lo = lo ? W + L.Cw_lo : nullptr;
+    void *AB_hi = W + L.AB_hi, *AB_lo = lo ? W + L.AB_lo : nullptr;
+    double *partD = reinterpret_cast<double *>(W + L.partD);
+    double *partF = reinterpret_cast<double *>(W + L.partF);
+
+    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax};
+    const size_t sm_tr = 3 * (size_t)e->dmax * e->dmax * sizeof(double);
+    const size_t sm_fold = 4 * (size_t)e->dmax * e->dmax * sizeof(double);
+    TD_CUDA(cudaFuncSetAttribute(transform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tr));
+    TD_CUDA(cudaFuncSetAttribute(fold_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fold));
+    TD_CUDA(cudaFuncSetAttribute(fold_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fold));
+
+    for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
+        const int nj = std::min(Jc, e->N_sym - j0);
+        const long long M = (long long)nb * nj;
+        // rows r = k * nj + jj
+        transform_kernel<<<dim3((unsigned)M, e->n_blocks), SYM_THREADS, sm_tr, st>>>(
+            t, Ys, R1, e->ups, nj, j0, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
+        TD_CUDA(cudaGetLastError());
+        // GEMM1: [a | b] = B1 . V^T      (M x 2N, K = Kp)
+        TD_TRY(gemm_abt(e, fmt, nprod, B1_hi, B1_lo, e->Kp, M, o.V_hi, o.V_lo, e->Kp, e->N2, e->Kp, D1, L.ld1, st));
+        // [c | d] = r1 . [X; G]^T         (M x 2N, K = np)
+        TD_TRY(gemm_abt(e, fmt, nprod, r1_hi, r1_lo, e->np, M, o.XG_hi, o.XG_lo, e->np, e->N2, e->np, Dcd, L.ld1, st));
+        // weights
+        if (fmt == FMT_F64)
+            weights_kernel<double><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
+                (const double *)D1, (const double *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
+        else
+            weights_kernel<float><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
+                (const float *)D1, (const float *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
+        TD_CUDA(cudaGetLastError());
+        // GEMM2: Z = Cw . VT^T            (M x P, K = N2p)
+        TD_TRY(gemm_abt(e, fmt, nprod, Cw_hi, Cw_lo, e->N2p, M, o.VT_hi, o.VT_lo, e->N2p, e->P, e->N2p, Z, L.ldz, st));
+        // F = AB . YXt^T                  (M x n, K = N2p)
+        TD_TRY(gemm_abt(e, fmt, nprod, AB_hi, AB_lo, e->N2p, M, o.YXt_hi, o.YXt_lo, e->N2p, e->n, e->N2p, F, L.ldf, st));
+        // fold this chunk into the partials
+        dim3 fg((unsigned)e->bp_b.size(), (unsigned)ceil_div(nj, Jf), (unsigned)nb);
+        if (fmt == FMT_F64)
+            fold_kernel<double><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const double *)Z, L.ldz,
+                                                                   (const double *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total, partD, partF);
+        else
+            fold_kernel<float><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const float *)Z, L.ldz,
+                                                                  (const float *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total, partD, partF);
+        TD_CUDA(cudaGetLastError());
+    }
+    const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
+    fold_reduce_kernel<<<grid_for((long long)nb * e->n * e->n), 256, 0, st>>>(partD, partF, nf_total, e->n, nb, e->d_blocks_ids,
+                                                                               norm, d_out, f_out);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace tdscha

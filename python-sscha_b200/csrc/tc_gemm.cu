@@ -1,0 +1,358 @@
+// tc_gemm.cu -- hand-written sm_100a tensor-core contraction D = A . B^T for the ensemble averages.
+//
+//   A (M x K), B (N x K): row-major, K contiguous ("K-major" for both UMMA operands), stored as
+//   bf16 or tf32-rounded fp32; optionally as hi/lo splits so that three products
+//   hi.hi + hi.lo + lo.hi recover ~16 (bf16) / ~21 (tf32) significant bits.
+//   D (M x N): fp32, row-major, written with edge masking.
+//
+// Pipeline (one CTA per 128 x BN output tile, 6 warps):
+//   warp 0      : TMA producer -- cp.async.bulk.tensor.2d into a STAGES-deep ring of 128B-swizzled
+//                 tiles, completion tracked by mbarrier transaction counts;
+//   warp 1      : allocates BN TMEM columns; one elected thread issues tcgen05.mma (kind::f16 for
+//                 bf16, kind::tf32) from shared-memory descriptors, accumulating in TMEM, and frees
+//                 each ring slot with tcgen05.commit -> mbarrier;
+//   warps 2..5  : epilogue -- tcgen05.ld 32x32b from TMEM (warp w reads lanes 32*(w%4)..+31), fp32
+//                 stores to global memory.
+// Every mbarrier wait is bounded by a %globaltimer budget; on expiry the CTA raises ERR_TIMEOUT in
+// the caller's error word, drains its own TMA copies (bounded), frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "common.cuh"
+#include "tc_gemm.cuh"
+
+namespace tdscha {
+namespace tc {
+
+constexpr int BM = 128;
+constexpr int NUM_THREADS = 192;
+constexpr unsigned long long WAIT_BUDGET_NS = 4000000000ull;   // 4 s per wait
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait: true when the phase completed, false on timeout or when another role aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
+    unsigned long long t0 = 0;
+    for (uint32_t it = 0;; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 255u) == 255u) {
+            if (*abort_flag) return false;
+            unsigned long long t = globaltimer();
+            if (t0 == 0) t0 = t;
+            else if (t - t0 > WAIT_BUDGET_NS) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(bar)
+        : "memory");
+}
+
+// Shared-memory matrix descriptor of a K-major tile stored as rows of 128 bytes with the 128-byte
+// swizzle (what TMA writes with CU_TENSOR_MAP_SWIZZLE_128B): start address >> 4 in bits 0-13,
+// leading byte offset (unused for swizzled K-major, 16 B) in bits 16-29, stride byte offset = 1024
+// (one 8-row swizzle atom) in bits 32-45, descriptor version 1 in bits 46-47, swizzle mode 2
+// (128B) in bits 61-63.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(16u >> 4) << 16;
+    d |= (uint64_t)(1024u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)2u << 61;
+    return d;
+}
+
+// Instruction descriptor for kind::f16 / kind::tf32 with fp32 accumulation, both operands K-major:
+// D format (bits 4-5) = 1 (f32); A/B format (bits 7-9, 10-12) = 1 (bf16) or 2 (tf32);
+// N >> 3 in bits 17-22; M >> 4 in bits 24-28.
+__host__ __device__ constexpr uint32_t make_idesc(bool tf32, int m, int n) {
+    return (1u << 4) | ((tf32 ? 2u : 1u) << 7) | ((tf32 ? 2u : 1u) << 10) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+template <bool TF32>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t accum) {
+    if constexpr (TF32) {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+    } else {
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+            ::"r"(tmem_d), "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accum));
+    }
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <int BN, int STAGES, bool TF32, int NPROD>
+struct Cfg {
+    static constexpr int A_BYTES = BM * 128;                 // one 128 x (128 B) tile
+    static constexpr int B_BYTES = BN * 128;
+    static constexpr int NOPS = (NPROD == 3) ? 2 : 1;        // hi (+ lo)
+    static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
+    static constexpr int K_ELEMS = TF32 ? 32 : 64;            // K per stage (128 B of K)
+    static constexpr int UMMA_K = TF32 ? 8 : 16;              // K per instruction (32 B)
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
+    static constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+};
+
+template <int BN, int STAGES, bool TF32, int NPROD>
+__global__ void __launch_bounds__(NUM_THREADS, 1)
+tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
+               const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
+               int M, int N, int K, float *__restrict__ D, long long ldd, unsigned *err) {
+    using C = Cfg<BN, STAGES, TF32, NPROD>;
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * C::STAGE_BYTES);
+    // bars[0..S) full, bars[S..2S) empty, bars[2S] accumulator ready
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 1);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 2);
+
+    const int warp = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * BM;
+    const int n0 = blockIdx.x * BN;
+    const int num_kb = K / C::K_ELEMS;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&bars[s]), 1);
+            mbar_init(smem_u32(&bars[STAGES + s]), 1);
+        }
+        mbar_init(smem_u32(&bars[2 * STAGES]), 1);
+        *abort_flag = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(tmem_slot)), "r"(C::TMEM_COLS) : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem_base = *tmem_slot;
+
+    int issued = 0;   // stages handed to TMA by the producer (for the drain on abort)
+    if (warp == 0 && lane == 0) {
+        // ---------------- TMA producer ----------------
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA_hi)) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB_hi)) : "memory");
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+            if (!mbar_wait(smem_u32(&bars[STAGES + s]), ph ^ 1u, abort_flag)) { *abort_flag = 1; break; }
+            uint8_t *st = smem + s * C::STAGE_BYTES;
+            const uint32_t full = smem_u32(&bars[s]);
+            mbar_expect_tx(full, C::STAGE_BYTES);
+            const int kc = kb * C::K_ELEMS;
+            tma_load_2d(smem_u32(st), &tmA_hi, kc, m0, full);
+            tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES), &tmB_hi, kc, n0, full);
+            if constexpr (NPROD == 3) {
+                tma_load_2d(smem_u32(st + C::A_BYTES), &tmA_lo, kc, m0, full);
+                tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES), &tmB_lo, kc, n0, full);
+            }
+            issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---------------- MMA issuer ----------------
+        constexpr uint32_t idesc = make_idesc(TF32, BM, BN);
+        bool ok = true;
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+            if (!mbar_wait(smem_u32(&bars[s]), ph, abort_flag)) { ok = false; *abort_flag = 1; break; }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint8_t *st = smem + s * C::STAGE_BYTES;
+            const uint32_t a_hi = smem_u32(st);
+            const uint32_t b_hi = smem_u32(st + C::NOPS * C::A_BYTES);
+#pragma unroll
+            for (int k = 0; k < C::K_ELEMS / C::UMMA_K; ++k) {
+                const uint32_t koff = k * 32;   // bytes inside the 128-byte swizzled row
+                const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
+                umma<TF32>(tmem_base, sw128_desc(a_hi + koff), sw128_desc(b_hi + koff), idesc, acc);
+                if constexpr (NPROD == 3) {
+                    const uint32_t a_lo = smem_u32(st + C::A_BYTES);
+                    const uint32_t b_lo = smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES);
+                    umma<TF32>(tmem_base, sw128_desc(a_hi + koff), sw128_desc(b_lo + koff), idesc, 1u);
+                    umma<TF32>(tmem_base, sw128_desc(a_lo + koff), sw128_desc(b_hi + koff), idesc, 1u);
+                }
+            }
+            umma_commit(smem_u32(&bars[STAGES + s]));   // slot s free once these MMAs retire
+        }
+        if (ok) umma_commit(smem_u32(&bars[2 * STAGES]));   // accumulator complete
+    } else if (warp >= 2) {
+        // ---------------- epilogue ----------------
+        const int q = warp & 3;              // TMEM lane quadrant this warp may access
+        const int row = q * 32 + lane;
+        const bool ready = mbar_wait(smem_u32(&bars[2 * STAGES]), 0u, abort_flag);
+        if (!ready) {
+            *abort_flag = 1;
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const long long grow = (long long)m0 + row;
+#pragma unroll 1
+            for (int c = 0; c < BN / 32; ++c) {
+                uint32_t r[32];
+                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 32), r);
+                if (grow < M) {
+                    float *drow = D + grow * ldd;
+                    const int cb = n0 + c * 32;
+                    if (cb + 32 <= N && ((ldd & 3) == 0)) {
+#pragma unroll
+                        for (int v = 0; v < 8; ++v) {
+                            float4 f4 = make_float4(__uint_as_float(r[4 * v]), __uint_as_float(r[4 * v + 1]),
+                                                    __uint_as_float(r[4 * v + 2]), __uint_as_float(r[4 * v + 3]));
+                            *reinterpret_cast<float4 *>(drow + cb + 4 * v) = f4;
+                        }
+                    } else {
+#pragma unroll
+                        for (int v = 0; v < 32; ++v)
+                            if (cb + v < N) drow[cb + v] = __uint_as_float(r[v]);
+                    }
+                }
+            }
+        }
+    }
+
+    // ---------------- teardown ----------------
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (*abort_flag) {
+        if (threadIdx.x == 0) atomicOr(err, ERR_TIMEOUT);
+        if (warp == 0 && lane == 0) {
+            // drain the TMA copies this CTA still has in flight (bounded)
+            volatile int never = 0;
+            for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
+                mbar_wait(smem_u32(&bars[kb % STAGES]), (uint32_t)(kb / STAGES) & 1u, &never);
+        }
+        __syncthreads();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base), "r"(C::TMEM_COLS) : "memory");
+    }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+// ------------------------------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn get_encode() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+// rows x K operand, leading dimension ld (elements), box = box_rows x (128 bytes of K)
+static int make_map(CUtensorMap *map, const void *base, bool tf32, long long rows, long long K, long long ld, int box_rows) {
+    EncodeTiledFn enc = get_encode();
+    TD_CHECK(enc != nullptr, TDSCHA_ECUDA, "cuTensorMapEncodeTiled entry point unavailable");
+    const size_t es = tf32 ? 4 : 2;
+    TD_CHECK((reinterpret_cast<uintptr_t>(base) & 15) == 0, TDSCHA_EINVAL, "operand base not 16-byte aligned");
+    TD_CHECK(((ld * es) & 15) == 0, TDSCHA_EINVAL, "operand row stride not a multiple of 16 bytes");
+    cuuint64_t gdim[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    cuuint64_t gstride[1] = {(cuuint64_t)(ld * es)};
+    cuuint32_t box[2] = {(cuuint32_t)(128 / es), (cuuint32_t)box_rows};
+    cuuint32_t estride[2] = {1, 1};
+    CUresult r = enc(map, tf32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                     const_cast<void *>(base), gdim, gstride, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    TD_CHECK(r == CUDA_SUCCESS, TDSCHA_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return 0;
+}
+
+template <int BN, int STAGES, bool TF32, int NPROD>
+static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+    using C = Cfg<BN, STAGES, TF32, NPROD>;
+    CUtensorMap a_hi, a_lo, b_hi, b_lo;
+    TD_TRY(make_map(&a_hi, op.A_hi, TF32, M, K, op.lda, BM));
+    TD_TRY(make_map(&b_hi, op.B_hi, TF32, N, K, op.ldb, BN));
+    if (NPROD == 3) {
+        TD_TRY(make_map(&a_lo, op.A_lo, TF32, M, K, op.lda, BM));
+        TD_TRY(make_map(&b_lo, op.B_lo, TF32, N, K, op.ldb, BN));
+    } else {
+        a_lo = a_hi;
+        b_lo = b_hi;
+    }
+    auto kern = tc_gemm_kernel<BN, STAGES, TF32, NPROD>;
+    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
+    dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
+    kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, D, ldd, err);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+    TD_CHECK(M > 0 && N > 0 && K > 0, TDSCHA_EINVAL, "tc::gemm: empty problem %d x %d x %d", M, N, K);
+    const bool tf32 = op.fmt == FMT_TF32;
+    TD_CHECK(op.fmt == FMT_TF32 || op.fmt == FMT_BF16, TDSCHA_EINVAL, "tc::gemm: operand format must be bf16 or tf32");
+    TD_CHECK(K % (tf32 ? 32 : 64) == 0, TDSCHA_EINVAL, "tc::gemm: K=%d not a multiple of the 128-byte K block", K);
+    TD_CHECK(op.nprod == 1 || op.nprod == 3, TDSCHA_EINVAL, "tc::gemm: nprod must be 1 or 3");
+    if (tf32) {
+        if (op.nprod == 3) return launch_cfg<256, 2, true, 3>(op, M, N, K, D, ldd, st, err);
+        return launch_cfg<256, 4, true, 1>(op, M, N, K, D, ldd, st, err);
+    }
+    if (op.nprod == 3) return launch_cfg<256, 2, false, 3>(op, M, N, K, D, ldd, st, err);
+    return launch_cfg<256, 4, false, 1>(op, M, N, K, D, ldd, st, err);
+}
+
+}  // namespace tc
+}  // namespace tdscha

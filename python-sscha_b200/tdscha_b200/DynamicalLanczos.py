@@ -1,0 +1,483 @@
+"""
+B200 compute mode for the TD-SCHA Lanczos linear response.
+
+Host-side mirror of ``tdscha.DynamicalLanczos.Lanczos`` (Modules/DynamicalLanczos.py:182) for the
+hot path: same attribute names, method names, argument meanings and checkpoint (npz) schema, with
+one more compute mode ``MODE_B200 = 4`` next to the reference's 0-3 (:166-169).  Every operator
+application, Lanczos step and continued fraction runs on the GPU through the C ABI
+(include/tdscha_b200.h); there is no CPU fallback.
+
+Differences from the reference that a user sees:
+  * the ensemble argument is any object exposing the arrays the reference extracts from an
+    ``sscha.Ensemble`` (X, Y, rho, w, pols, m, T, ...), e.g. ``rocksalt.SyntheticEnsemble``;
+    cellconstructor/sscha are not needed;
+  * ``precision`` selects the arithmetic of the two ensemble contractions
+    ("fp64", "tf32", "bf16x3", "tf32x3", "bf16"); the recurrence is always FP64;
+  * errors raise exceptions where the reference's C binding calls exit().
+"""
+from __future__ import annotations
+
+import difflib
+import os
+import sys
+import time
+
+import numpy as np
+
+from . import _native
+
+MODE_SLOW_SERIAL = 0
+MODE_FAST_SERIAL = 1
+MODE_FAST_MPI = 2
+MODE_FAST_JULIA = 3
+MODE_B200 = 4
+
+TYPE_DP = np.double
+__EPSILON__ = 1e-12          # DynamicalLanczos.py:121
+__RyToK__ = 157887.32400374097
+
+
+def _torch():
+    import torch
+    if not torch.cuda.is_available():
+        raise _native.TdschaError("MODE_B200 needs a CUDA device (no CPU fallback)")
+    return torch
+
+
+class Lanczos(object):
+    def __init__(self, ensemble=None, mode=None, unwrap_symmetries=False, select_modes=None, use_wigner=False,
+                 lo_to_split="random", precision="fp64"):
+        self.mode = MODE_B200
+        if mode is not None and mode != MODE_B200:
+            raise ValueError(f"this package implements only MODE_B200 = {MODE_B200} (got {mode})")
+        self.verbose = True
+        self.T = 0
+        self.nat = 0
+        self.m = []
+        self.w = []
+        self.pols = []
+        self.n_modes = 0
+        self.ignore_harmonic = False
+        self.ignore_v3 = False
+        self.ignore_v4 = False
+        self.N = 0
+        self.rho = []
+        self.N_eff = 0
+        self.X = []
+        self.Y = []
+        self.psi = []
+        self.eigvals = None
+        self.eigvects = None
+        self.a_coeffs = []
+        self.b_coeffs = []
+        self.c_coeffs = []
+        self.krilov_basis = []
+        self.basis_P = []
+        self.basis_Q = []
+        self.s_norm = []
+        self.arnoldi_matrix = []
+        self.reverse_L = False
+        self.shift_value = 0
+        self.symmetrize = False
+        self.symmetries = None
+        self.degenerate_space = None
+        self.N_degeneracy = None
+        self.initialized = False
+        self.perturbation_modulus = 1
+        self.dyn = None
+        self.uci_structure = None
+        self.super_structure = None
+        self.qe_sym = None
+        self.L_linop = None
+        self.M_linop = None
+        self.unwrapped = False
+        self.sym_julia = None
+        self.deg_julia = None
+        self.n_syms = 1
+        self.u_tilde = None
+        self.f_tilde = None
+        self.sym_block_id = None
+        self.use_wigner = use_wigner
+        self.ignore_small_w = False
+        self.precision = precision
+        self.effective_charges = None
+        self.raman_tensor = None
+        self.supercell = (1, 1, 1)
+        self.nat_uc = 0
+        self.device_ensemble = None
+        self.__total_attributes__ = [item for item in self.__dict__.keys()]
+        self.fixed_attributes = True
+
+        if ensemble is None:
+            return
+        if precision not in _native.PREC:
+            raise ValueError(f"precision must be one of {list(_native.PREC)}")
+        self.T = float(ensemble.T)
+        self.nat = int(ensemble.nat)
+        self.m = np.asarray(ensemble.m, dtype=TYPE_DP)
+        self.w = np.asarray(ensemble.w, dtype=TYPE_DP)
+        self.pols = np.asarray(ensemble.pols, dtype=TYPE_DP)
+        if select_modes is not None:
+            raise NotImplementedError("select_modes: pass the already reduced mode set in the ensemble")
+        self.n_modes = len(self.w)
+        self.N = int(ensemble.N)
+        self.rho = np.asarray(ensemble.rho, dtype=TYPE_DP).copy()
+        self.N_eff = float(np.sum(self.rho))
+        self.X = np.ascontiguousarray(ensemble.X, dtype=TYPE_DP)
+        self.Y = np.ascontiguousarray(ensemble.Y, dtype=TYPE_DP)
+        self.effective_charges = getattr(ensemble, "effective_charges", None)
+        self.raman_tensor = getattr(ensemble, "raman_tensor", None)
+        self.supercell = tuple(getattr(ensemble, "supercell", (1, 1, 1)))
+        self.nat_uc = int(getattr(ensemble, "nat_uc", self.nat))
+        self._ens_symmetries = (getattr(ensemble, "symmetries", None), getattr(ensemble, "deg_space", None),
+                                getattr(ensemble, "blocks_ids", None))
+        self.psi = np.zeros(self.n_modes + self.n_modes * (self.n_modes + 1), dtype=TYPE_DP)
+
+    def __setattr__(self, name, value):
+        if "fixed_attributes" in self.__dict__:
+            if name in self.__total_attributes__ or name.startswith("_"):
+                super(Lanczos, self).__setattr__(name, value)
+            elif self.fixed_attributes:
+                similar = str(difflib.get_close_matches(name, self.__total_attributes__))
+                raise AttributeError(f"""
+        Error, the attribute '{name}' is not a member of '{type(self).__name__}'.
+        Suggested similar attributes: {similar} ?
+        """)
+        else:
+            super(Lanczos, self).__setattr__(name, value)
+
+    # ------------------------------------------------------------------------------------------
+    def reset(self):
+        n = self.n_modes
+        self.psi = np.zeros(n + n * (n + 1), dtype=TYPE_DP)
+        self.eigvals = None
+        self.eigvects = None
+        self.a_coeffs = []
+        self.b_coeffs = []
+        self.c_coeffs = []
+        self.basis_P = []
+        self.basis_Q = []
+        self.s_norm = []
+        self.krilov_basis = []
+        self.arnoldi_matrix = []
+
+    def init(self, use_symmetries=True):
+        self.prepare_symmetrization(no_sym=not use_symmetries)
+        self.initialized = True
+
+    def prepare_symmetrization(self, no_sym=False, verbose=True, symmetries=None):
+        """Mode-space symmetry blocks (DynamicalLanczos.py:686-782).  ``symmetries`` may be a tuple
+        (per-block tables, per-block mode lists, blocks_ids); by default the ensemble's are used."""
+        n = self.n_modes
+        self.initialized = True
+        if no_sym or self.unwrapped:
+            self.symmetries = [np.ones((1, 1, 1), dtype=np.double)] * n
+            self.N_degeneracy = np.ones(n, dtype=np.intc)
+            self.degenerate_space = [np.array([i], dtype=np.intc) for i in range(n)]
+            self.sym_block_id = np.arange(n).astype(np.intc)
+        else:
+            syms, degs, bids = symmetries if symmetries is not None else self._ens_symmetries
+            if syms is None:
+                raise ValueError("no symmetry tables available: pass symmetries=(tables, blocks, ids) or no_sym=True")
+            self.symmetries = [np.asarray(s, dtype=np.double) for s in syms]
+            self.degenerate_space = [np.array(d, dtype=np.intc) for d in degs]
+            self.N_degeneracy = np.array([len(d) for d in degs], dtype=np.intc)
+            self.sym_block_id = np.asarray(bids, dtype=np.intc)
+        self.n_syms = self.symmetries[0].shape[0]
+        self._upload()
+
+    def _upload(self):
+        if self.device_ensemble is not None:
+            self.device_ensemble.close()
+        self.device_ensemble = _native.DeviceEnsemble(self.X, self.Y, self.w, self.rho, self.T, self.symmetries,
+                                                      self.degenerate_space, self.sym_block_id)
+
+    def _opts(self, harmonic=True, anharmonic=True, post=True):
+        return _native.ApplyOpts(int(self.use_wigner), int(self.ignore_harmonic or not harmonic),
+                                 int(self.ignore_v3 or not anharmonic), int(self.ignore_v4),
+                                 int(self.reverse_L) if post else 0, float(self.shift_value) if post else 0.0)
+
+    def _check_init(self):
+        if not self.initialized or self.device_ensemble is None:
+            raise ValueError("Error, this class must be initialized before lunching the computation:\n Use the .init()")
+
+    def _apply_host(self, psi, transpose, opts):
+        torch = _torch()
+        self._check_init()
+        x = torch.as_tensor(np.asarray(psi, dtype=TYPE_DP), device="cuda").reshape(1, -1).contiguous()
+        out = torch.empty_like(x)
+        self.device_ensemble.apply_full_L(x, out, [int(transpose)], opts, self.precision)
+        return out.reshape(-1).cpu().numpy()
+
+    # ---- operator (DynamicalLanczos.py:2227-2385, 2891-3281, 3467-3570) ----------------------
+    def apply_L1_FT(self, transpose=False):
+        if self.ignore_harmonic:
+            return np.zeros(np.shape(self.psi), dtype=TYPE_DP)
+        return self._apply_host(self.psi, transpose, self._opts(anharmonic=False, post=False))
+
+    def apply_anharmonic_FT(self, transpose=False, test_weights=True, use_old_version=False):
+        if use_old_version:
+            raise NotImplementedError("the pre-symmetrisation averages are not part of the B200 path")
+        o = self._opts(harmonic=False, post=False)
+        o.ignore_v3 = 0
+        return self._apply_host(self.psi, transpose, o)
+
+    def apply_full_L(self, target=None, force_t_0=False, force_FT=True, transpose=False, fast_lanczos=True):
+        if force_t_0 and force_FT:
+            raise ValueError("Error, only one between force_t_0 and force_FT can be True")
+        if target is not None:
+            self.psi = target
+        self._check_init()
+        if (force_t_0 or self.T < __EPSILON__) and not force_FT:
+            raise NotImplementedError("the T = 0 operator (apply_L1) is not part of the B200 path")
+        opts = self._opts(anharmonic=fast_lanczos)
+        self.psi = self._apply_host(self.psi, transpose, opts)
+        return self.psi
+
+    # ---- perturbations (DynamicalLanczos.py:1963-2031, 1647-1689, 1003-1124) -----------------
+    def prepare_perturbation(self, vector, masses_exp=1, add=False):
+        if not add:
+            self.reset()
+            self.psi = np.zeros(self.psi.shape, dtype=TYPE_DP)
+        m_on = np.sqrt(self.m) ** masses_exp
+        new_v = np.einsum("a, a, ab->b", m_on, vector, self.pols)
+        self.psi[:self.n_modes] += new_v
+        self.perturbation_modulus = new_v.dot(new_v)
+
+    def prepare_mode(self, index):
+        self.reset()
+        self.psi[:] = 0
+        self.psi[index] = 1
+        self.perturbation_modulus = 1
+
+    def prepare_ir(self, effective_charges=None, pol_vec=np.array([1, 0, 0])):
+        ec = self.effective_charges if effective_charges is None else effective_charges
+        assert ec is not None, "Error, no effective charge found. Cannot initialize IR responce"
+        ec = np.asarray(ec)
+        assert len(ec.shape) == 3 and ec.shape[1] == ec.shape[2] == 3, f"Error, effective charges of the wrong shape: {ec.shape}"
+        n_supercell = int(np.prod(self.supercell))
+        if not self.ignore_small_w:
+            assert ec.shape[0] * ec.shape[2] * n_supercell == self.n_modes + 3
+        z_eff = np.einsum("abc, b", ec, pol_vec)
+        self.prepare_perturbation(np.tile(z_eff.ravel(), n_supercell), masses_exp=-1)
+
+    def prepare_raman(self, pol_vec_in=np.array([1, 0, 0]), pol_vec_out=np.array([1, 0, 0]), mixed=False,
+                      pol_in_2=None, pol_out_2=None, unpolarized=None):
+        """Raman perturbation.  As in the reference (DynamicalLanczos.py:1124), the final call
+        re-prepares the perturbation from the last vector without ``add``."""
+        from .rocksalt import raman_vector
+        assert self.raman_tensor is not None, "Error, no Raman tensor found. Cannot initialize the Raman responce"
+        rv = lambda a, b: raman_vector(self.raman_tensor, np.asarray(a, float), np.asarray(b, float))   # noqa: E731
+        n_supercell = int(np.prod(self.supercell))
+        raman_v = rv(pol_vec_in, pol_vec_out)
+        if mixed:
+            raman_v += rv(pol_in_2, pol_out_2)
+        px, py, pz = np.eye(3)
+        if unpolarized is None:
+            new_raman_v = np.tile(rv(pol_vec_in, pol_vec_out).ravel(), n_supercell)
+            self.prepare_perturbation(new_raman_v, masses_exp=-1)
+        else:
+            plan = {0: [((px, px), 1 / 3), ((py, py), 1 / 3), ((pz, pz), 1 / 3)],
+                    1: [((px, px), 1 / np.sqrt(2)), ((py, py), -1 / np.sqrt(2))],
+                    2: [((px, px), 1 / np.sqrt(2)), ((pz, pz), -1 / np.sqrt(2))],
+                    3: [((py, py), 1 / np.sqrt(2)), ((pz, pz), -1 / np.sqrt(2))],
+                    4: [((px, py), np.sqrt(3))], 5: [((py, pz), np.sqrt(3))], 6: [((px, pz), np.sqrt(3))]}
+            if unpolarized not in plan:
+                raise ValueError(f"Error, unpolarized must be between [0, ... ,6] got invalid {unpolarized}.")
+            for t, ((a, b), s) in enumerate(plan[unpolarized]):
+                new_raman_v = np.tile(rv(a, b).ravel(), n_supercell) * s
+                self.prepare_perturbation(new_raman_v, masses_exp=-1, add=t > 0)
+        self.prepare_perturbation(new_raman_v, masses_exp=-1)
+
+    def prepare_random(self, seed=0, sector="R"):
+        """Seeded random unit perturbation on R^(1) (sector "R") or on the whole vector ("all")."""
+        rng = np.random.default_rng(seed)
+        self.reset()
+        v = np.zeros_like(self.psi)
+        if sector == "R":
+            v[:self.n_modes] = rng.standard_normal(self.n_modes)
+        else:
+            v[:] = rng.standard_normal(len(v))
+        v /= np.linalg.norm(v)
+        self.psi = v
+        self.perturbation_modulus = 1
+
+    def mask_dot_wigner(self, debug=False):
+        n = self.n_modes
+        mask = np.ones(n + n * (n + 1))
+        r, c = np.triu_indices(n)
+        m = n * (n + 1) // 2
+        mask[n:n + m][r < c] = 2
+        mask[n + m:][r < c] = 2
+        return mask
+
+    # ---- Lanczos (DynamicalLanczos.py:5843-6374) ---------------------------------------------
+    def run_FT(self, n_iter, save_dir=None, save_each=5, verbose=True, n_rep_orth=0, n_ortho=10, flush_output=True,
+               debug=False, prefix="LANCZOS", run_simm=False, optimized=False):
+        run_FT_batched([self], n_iter, save_dir=save_dir, save_each=save_each, verbose=verbose, n_rep_orth=n_rep_orth,
+                       run_simm=run_simm, prefix=[prefix])
+
+    # ---- Green function (DynamicalLanczos.py:4951-5047) --------------------------------------
+    def get_green_function_continued_fraction(self, w_array, use_terminator=True, last_average=1, smearing=0):
+        torch = _torch()
+        w_array = np.asarray(w_array, dtype=np.float64)
+        a = torch.as_tensor(np.asarray(self.a_coeffs, dtype=np.float64), device="cuda")
+        b = torch.as_tensor(np.asarray(self.b_coeffs, dtype=np.float64), device="cuda") if len(self.b_coeffs) else None
+        c = torch.as_tensor(np.asarray(self.c_coeffs, dtype=np.float64), device="cuda") if len(self.c_coeffs) else None
+        om = torch.as_tensor(w_array.ravel(), device="cuda")
+        gf = torch.empty(2 * om.numel(), dtype=torch.float64, device="cuda")
+        _native.continued_fraction(a, b, c, om, gf, use_terminator, last_average, smearing, self.use_wigner,
+                                   self.reverse_L, self.shift_value, self.perturbation_modulus)
+        g = gf.cpu().numpy()
+        return (g[0::2] + 1j * g[1::2]).reshape(w_array.shape)
+
+    # ---- checkpoints (DynamicalLanczos.py:3597-3758) -----------------------------------------
+    def save_status(self, file):
+        if ".npz" not in file.lower():
+            file += ".npz"
+        np.savez_compressed(file, T=self.T, nat=self.nat, m=self.m, w=self.w, pols=self.pols, n_modes=self.n_modes,
+                            ignore_v3=self.ignore_v3, ignore_v4=self.ignore_v4, N=self.N, rho=self.rho, X=self.X,
+                            Y=self.Y, psi=self.psi, a_coeffs=self.a_coeffs, b_coeffs=self.b_coeffs,
+                            c_coeffs=self.c_coeffs, basis_Q=self.basis_Q, basis_P=self.basis_P, s_norm=self.s_norm,
+                            krilov_basis=self.krilov_basis, arnoldi_matrix=self.arnoldi_matrix, reverse=self.reverse_L,
+                            shift=self.shift_value, perturbation_modulus=self.perturbation_modulus,
+                            use_wigner=self.use_wigner, ignore_small_w=self.ignore_small_w, sym_julia=self.sym_julia,
+                            deg_julia=self.deg_julia, n_syms=self.n_syms)
+
+    def load_status(self, file, is_file_instance=False):
+        if not is_file_instance:
+            if ".npz" not in file.lower():
+                file += ".npz"
+            if not os.path.exists(file):
+                raise IOError("Error while loading %s" % file)
+        data = dict(np.load(file, allow_pickle=True))
+        self.T = np.double(data["T"])
+        self.nat = np.intc(data["nat"])
+        self.m = data["m"]
+        self.w = data["w"]
+        self.pols = data["pols"]
+        self.n_modes = np.intc(data["n_modes"])
+        self.ignore_v3 = bool(data["ignore_v3"])
+        self.ignore_v4 = bool(data["ignore_v4"])
+        self.N = np.intc(data["N"])
+        self.rho = data["rho"]
+        self.X = data["X"]
+        self.Y = data["Y"]
+        self.psi = data["psi"]
+        self.a_coeffs = list(data["a_coeffs"])
+        self.b_coeffs = list(data["b_coeffs"])
+        self.c_coeffs = list(data["c_coeffs"]) if "c_coeffs" in data else []
+        self.krilov_basis = data["krilov_basis"]
+        self.arnoldi_matrix = data["arnoldi_matrix"]
+        self.sym_julia = data.get("sym_julia")
+        self.deg_julia = data.get("deg_julia")
+        self.n_syms = data.get("n_syms", 1)
+        self.basis_Q = data["basis_Q"]
+        self.basis_P = data["basis_P"]
+        self.s_norm = data["s_norm"]
+        self.use_wigner = bool(data["use_wigner"])
+        self.ignore_small_w = bool(data.get("ignore_small_w", False))
+        if "reverse" in data:
+            self.reverse_L = bool(data["reverse"])
+            self.shift_value = float(data["shift"])
+        if "perturbation_modulus" in data:
+            self.perturbation_modulus = float(data["perturbation_modulus"])
+        self.N_eff = float(np.sum(self.rho))
+
+
+def run_FT_batched(lanczos_list, n_iter, save_dir=None, save_each=5, verbose=False, n_rep_orth=0, run_simm=False,
+                   prefix=None, precision=None):
+    """Advance several bi-conjugate Lanczos chains that share one ensemble in lockstep: each step
+    is ONE batched apply over [L q_c, L^T p_c for every active chain] plus one batched recurrence
+    launch; all vectors stay in HBM.  Chains stop independently on breakdown (|b| or |c| < 1e-12)."""
+    torch = _torch()
+    if n_rep_orth:
+        raise NotImplementedError("Gram-Schmidt re-orthogonalisation (n_rep_orth > 0) is not available in MODE_B200")
+    L0 = lanczos_list[0]
+    dev_ens = L0.device_ensemble
+    for L in lanczos_list:
+        L._check_init()
+        if L.device_ensemble is not dev_ens:
+            raise ValueError("batched chains must share one initialised ensemble (set lanc.device_ensemble)")
+        if run_simm and not L.use_wigner:
+            raise NotImplementedError('The symmetric Lanczos works only with Wigner. Set use_wigner to True')
+        psi = np.asarray(L.psi)
+        if np.isnan(np.sum(psi ** 2)) or np.sum(psi ** 2) == 0:
+            raise ValueError("Error, you must initialize a perturbation to start the Lanczos.")
+    prec = precision or L0.precision
+    nc = len(lanczos_list)
+    n = L0.n_modes
+    length = n + n * (n + 1)
+    mask = torch.as_tensor(L0.mask_dot_wigner(), device="cuda") if run_simm else None
+    dev = "cuda"
+    # per chain device state: current q, p, previous q, p
+    state = []
+    for L in lanczos_list:
+        if len(L.a_coeffs) == 0:
+            v = torch.as_tensor(np.asarray(L.psi, dtype=np.float64), device=dev)
+            nrm = torch.sqrt((v * v * (mask if mask is not None else 1.0)).sum())
+            first = v / nrm
+            L.basis_Q, L.basis_P, L.s_norm = [first.cpu().numpy()], [first.cpu().numpy()], [1]
+        L.basis_Q, L.basis_P, L.s_norm = list(L.basis_Q), list(L.basis_P), list(L.s_norm)
+        L.a_coeffs, L.b_coeffs, L.c_coeffs = list(L.a_coeffs), list(L.b_coeffs), list(L.c_coeffs)
+        q = torch.as_tensor(np.asarray(L.basis_Q[-1]), device=dev)
+        p = torch.as_tensor(np.asarray(L.basis_P[-1]), device=dev)
+        qp = torch.as_tensor(np.asarray(L.basis_Q[-2]), device=dev) if len(L.basis_Q) > 1 else torch.zeros_like(q)
+        pp = torch.as_tensor(np.asarray(L.basis_P[-2]), device=dev) if len(L.basis_P) > 1 else torch.zeros_like(p)
+        state.append({"q": q, "p": p, "qp": qp, "pp": pp, "done": False, "L": L})
+    opts = L0._opts()
+    for it in range(n_iter):
+        active = [s for s in state if not s["done"]]
+        if not active:
+            break
+        na = len(active)
+        if run_simm:
+            vecs = torch.stack([s["q"] for s in active])
+            tr = [0] * na
+        else:
+            vecs = torch.stack([s["q"] for s in active] + [s["p"] for s in active])
+            tr = [0] * na + [1] * na
+        out = torch.empty_like(vecs)
+        dev_ens.apply_full_L(vecs, out, tr, opts, prec)
+        Lq = out[:na]
+        pL = out[:na].clone() if run_simm else out[na:]
+        sc_in = torch.tensor([[s["L"].c_coeffs[-1] if s["L"].c_coeffs else 0.0,
+                               s["L"].b_coeffs[-1] if s["L"].b_coeffs else 0.0,
+                               s["L"].s_norm[-1],
+                               s["L"].s_norm[-2] if len(s["L"].s_norm) > 1 else 0.0,
+                               s["L"].c_coeffs[-2] if len(s["L"].c_coeffs) > 1 else 1.0,
+                               float(len(s["L"].a_coeffs))] for s in active], dtype=torch.float64, device=dev)
+        Q = torch.stack([s["q"] for s in active]).contiguous()
+        Pm = torch.stack([s["p"] for s in active]).contiguous()
+        QP = torch.stack([s["qp"] for s in active]).contiguous()
+        PP = torch.stack([s["pp"] for s in active]).contiguous()
+        qn = torch.empty_like(Q)
+        pn = torch.empty_like(Pm)
+        sc_out = torch.empty((na, 4), dtype=torch.float64, device=dev)
+        _native.lanczos_step(Lq.contiguous(), pL.contiguous(), Q, Pm, QP, PP, sc_in, mask, qn, pn, sc_out)
+        sc = sc_out.cpu().numpy()
+        for ci, s in enumerate(active):
+            L = s["L"]
+            a, b, c, snew = (float(x) for x in sc[ci])
+            if np.isnan(a):
+                raise ValueError("Invalid value encountered during the Lanczos.")
+            L.a_coeffs.append(a)
+            if abs(b) < __EPSILON__ or abs(c) < __EPSILON__:
+                s["done"] = True
+                continue
+            s["qp"], s["pp"] = s["q"], s["p"]
+            s["q"], s["p"] = qn[ci], pn[ci]
+            L.basis_Q.append(qn[ci].cpu().numpy())
+            L.basis_P.append(pn[ci].cpu().numpy())
+            L.b_coeffs.append(b)
+            L.c_coeffs.append(c)
+            L.s_norm.append(snew)
+            if save_dir is not None and len(L.a_coeffs) % save_each == 0:
+                os.makedirs(save_dir, exist_ok=True)
+                pre = prefix[state.index(s)] if prefix else "LANCZOS"
+                L.save_status(os.path.join(save_dir, f"{pre}_STEP{len(L.a_coeffs)}"))
+        if verbose:
+            print(f"Lanczos step {it + 1}: " + ", ".join(f"a={s['L'].a_coeffs[-1]:.6e}" for s in active))
+            sys.stdout.flush()
+    for s in state:
+        s["L"].psi = s["q"].cpu().numpy()

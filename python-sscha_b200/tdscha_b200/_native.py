@@ -1,0 +1,209 @@
+"""ctypes binding of the C ABI in include/tdscha_b200.h (libtdscha_b200.so, built in-tree).
+
+There is no CPU fallback: importing the binding without the library, or calling it without an
+sm_100 GPU, raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+PREC = {"fp64": 0, "tf32": 1, "bf16x3": 2, "tf32x3": 3, "bf16": 4}
+ERRORS = {-1: "EINVAL", -2: "ECUDA", -3: "ENOMEM", -4: "ENOSUPPORT", -5: "ETIMEOUT"}
+
+_lib = None
+
+dp = ctypes.POINTER(ctypes.c_double)
+ip = ctypes.POINTER(ctypes.c_int)
+vp = ctypes.c_void_p
+
+
+class ApplyOpts(ctypes.Structure):
+    _fields_ = [("use_wigner", ctypes.c_int), ("ignore_harmonic", ctypes.c_int), ("ignore_v3", ctypes.c_int),
+                ("ignore_v4", ctypes.c_int), ("reverse_L", ctypes.c_int), ("shift_value", ctypes.c_double)]
+
+
+class TdschaError(RuntimeError):
+    pass
+
+
+def library_path():
+    return _build.LIB_PATH
+
+
+def load():
+    """Load the CUDA library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = library_path()
+    if not os.path.exists(path):
+        raise TdschaError(f"{path} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(path)
+    lib.tdscha_last_error.restype = ctypes.c_char_p
+    lib.tdscha_version.restype = ctypes.c_char_p
+    lib.tdscha_ensemble_create.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                           ctypes.c_int, ip, ctypes.POINTER(ip), ctypes.POINTER(dp), ip,
+                                           ctypes.POINTER(vp)]
+    lib.tdscha_ensemble_destroy.argtypes = [vp]
+    lib.tdscha_ensemble_info.argtypes = [vp, ip, ip, ip, ip, dp, dp]
+    lib.tdscha_ensemble_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.tdscha_perturb_average_sym.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, dp, dp]
+    lib.tdscha_perturb_average_sym_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+    lib.tdscha_GetPerturbAverageSym.argtypes = [dp, dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.POINTER(dp), ip, ctypes.POINTER(ip), ip,
+                                                ctypes.c_int, ctypes.c_int, dp, dp]
+    lib.tdscha_apply_full_L_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), ctypes.c_int, vp, vp]
+    lib.tdscha_lanczos_step_device.argtypes = [ctypes.c_int, ctypes.c_longlong, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                               vp, vp]
+    lib.tdscha_continued_fraction_device.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                     vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                                     ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp]
+    for name in ("tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+                 "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
+                 "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
+                 "tdscha_continued_fraction_device"):
+        getattr(lib, name).restype = ctypes.c_int
+    _lib = lib
+    return lib
+
+
+def check(rc):
+    if rc != 0:
+        msg = _lib.tdscha_last_error().decode() if _lib is not None else ""
+        raise TdschaError(f"tdscha_b200 error {ERRORS.get(rc, rc)}: {msg}")
+
+
+def _d(a):
+    return a.ctypes.data_as(dp)
+
+
+def _i(a):
+    return a.ctypes.data_as(ip)
+
+
+class DeviceEnsemble:
+    """Owner of a ``tdscha_ensemble`` handle (X, Y, rho, w and the symmetry tables resident in HBM)."""
+
+    def __init__(self, X, Y, w, rho, T, symmetries, deg_space, blocks_ids):
+        lib = load()
+        self.X = np.ascontiguousarray(X, dtype=np.float64)
+        self.Y = np.ascontiguousarray(Y, dtype=np.float64)
+        self.w = np.ascontiguousarray(w, dtype=np.float64)
+        self.rho = np.ascontiguousarray(rho, dtype=np.float64)
+        self.T = float(T)
+        N, n = self.X.shape
+        self.N, self.n = N, n
+        syms = [np.ascontiguousarray(s, dtype=np.float64) for s in symmetries]
+        degs = [np.ascontiguousarray(d, dtype=np.intc) for d in deg_space]
+        self.N_sym = int(syms[0].shape[0])
+        n_deg = np.array([len(d) for d in degs], dtype=np.intc)
+        bid = np.ascontiguousarray(blocks_ids, dtype=np.intc)
+        sym_ptrs = (dp * len(syms))(*[_d(s) for s in syms])
+        deg_ptrs = (ip * len(degs))(*[_i(d) for d in degs])
+        h = vp()
+        check(lib.tdscha_ensemble_create(_d(self.X), _d(self.Y), _d(self.w), _d(self.rho), N, n, self.T, self.N_sym,
+                                         len(syms), _i(n_deg), deg_ptrs, sym_ptrs, _i(bid), ctypes.byref(h)))
+        self.handle = h
+        self._lib = lib
+
+    def close(self):
+        if getattr(self, "handle", None) is not None and self.handle.value:
+            self._lib.tdscha_ensemble_destroy(self.handle)
+            self.handle = vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self):
+        b = ctypes.c_longlong()
+        check(self._lib.tdscha_ensemble_device_bytes(self.handle, ctypes.byref(b)))
+        return b.value
+
+    def perturb_average(self, R1, Y1, apply_d4=1, precision="fp64"):
+        """Host-buffer drop-in of GetPerturbAverageSym: returns (f_av (n), d2v (n, n))."""
+        R1 = np.ascontiguousarray(R1, dtype=np.float64)
+        Y1 = np.ascontiguousarray(Y1, dtype=np.float64)
+        f = np.zeros(self.n)
+        d = np.zeros((self.n, self.n))
+        check(self._lib.tdscha_perturb_average_sym(self.handle, _d(R1), _d(Y1), int(apply_d4), PREC[precision], _d(f), _d(d)))
+        return f, d
+
+    def perturb_average_device(self, R1, Y1, f_out, d_out, apply_d4=1, precision="fp64", stream=None):
+        """Batched device version on torch tensors: R1 (nb, n), Y1 (nb, n, n) float64 CUDA."""
+        nb = R1.shape[0]
+        check(self._lib.tdscha_perturb_average_sym_device(self.handle, nb, R1.data_ptr(), Y1.data_ptr(), int(apply_d4),
+                                                          PREC[precision], f_out.data_ptr(), d_out.data_ptr(),
+                                                          _stream_ptr(stream)))
+
+    def apply_full_L(self, psi, out, transpose, opts, precision="fp64", stream=None):
+        """psi, out: (nb, len) float64 CUDA tensors; transpose: sequence of nb ints."""
+        nb = psi.shape[0]
+        tr = np.ascontiguousarray(np.asarray(transpose, dtype=np.intc).reshape(nb))
+        check(self._lib.tdscha_apply_full_L_device(self.handle, nb, psi.data_ptr(), _i(tr), ctypes.byref(opts),
+                                                   PREC[precision], out.data_ptr(), _stream_ptr(stream)))
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    return stream
+
+
+def lanczos_step(Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_out, stream=None):
+    lib = load()
+    nc, length = Lq.shape
+    ptr = lambda t: None if t is None else t.data_ptr()   # noqa: E731
+    check(lib.tdscha_lanczos_step_device(nc, length, ptr(Lq), ptr(pL), ptr(q), ptr(p), ptr(q_prev), ptr(p_prev),
+                                         ptr(sc_in), ptr(mask), ptr(q_next), ptr(p_next), ptr(sc_out),
+                                         _stream_ptr(stream)))
+
+
+def continued_fraction(a, b, c, omega, gf_out, use_terminator, last_average, smearing, use_wigner, reverse_L,
+                       shift_value, modulus, stream=None):
+    lib = load()
+    nb = 0 if b is None else b.numel()
+    ncc = 0 if c is None else c.numel()
+    check(lib.tdscha_continued_fraction_device(a.numel(), a.data_ptr(), None if b is None else b.data_ptr(),
+                                               None if c is None else c.data_ptr(), nb, ncc, omega.numel(),
+                                               omega.data_ptr(), int(use_terminator), int(last_average),
+                                               float(smearing), int(use_wigner), int(reverse_L), float(shift_value),
+                                               float(modulus), gf_out.data_ptr(), _stream_ptr(stream)))
+
+
+def get_perturb_average_sym(X, Y, w, rho, R1, Y1, T, apply_D4, N_syms, sym_list, n_deg, deg_space_list, blocks_ids,
+                            f_out, d2v_out):
+    """Same argument list and in-place outputs as ``sscha_HP_odd.GetPerturbAverageSym``
+    (CModules/odd_corr_module.c:519-520), FP64 on the GPU.  Unlike the reference, bad arguments
+    raise instead of terminating the process."""
+    lib = load()
+    X = np.ascontiguousarray(X, dtype=np.float64)
+    Y = np.ascontiguousarray(Y, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    rho = np.ascontiguousarray(rho, dtype=np.float64)
+    R1 = np.ascontiguousarray(R1, dtype=np.float64)
+    Y1 = np.ascontiguousarray(Y1, dtype=np.float64)
+    N, n = X.shape
+    if len(w) != n:
+        raise ValueError(f"N_modes from X is {n}, while len(w) = {len(w)}")
+    syms = [np.ascontiguousarray(s, dtype=np.float64) for s in sym_list]
+    degs = [np.ascontiguousarray(d, dtype=np.intc) for d in deg_space_list]
+    n_deg = np.ascontiguousarray(n_deg, dtype=np.intc)
+    bid = np.ascontiguousarray(blocks_ids, dtype=np.intc)
+    for name, arr, shape in (("f_out", f_out, (n,)), ("d2v_out", d2v_out, (n, n))):
+        if arr.dtype != np.float64 or arr.shape != shape or not arr.flags.c_contiguous:
+            raise ValueError(f"{name} must be a C-contiguous float64 array of shape {shape}")
+    sym_ptrs = (dp * len(syms))(*[_d(s) for s in syms])
+    deg_ptrs = (ip * len(degs))(*[_i(d) for d in degs])
+    check(lib.tdscha_GetPerturbAverageSym(_d(X), _d(Y), _d(w), _d(rho), _d(R1), _d(Y1), float(T), int(apply_D4),
+                                          int(N_syms), len(syms), sym_ptrs, _i(n_deg), deg_ptrs, _i(bid), N, n,
+                                          _d(f_out), _d(d2v_out)))

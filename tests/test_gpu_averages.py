@@ -1,0 +1,75 @@
+"""Symmetrised perturbed averages on the GPU (C ABI) against the reference kernel's golden outputs."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# max-norm error relative to the max-norm of the golden output, per precision mode
+TOL = {"fp64": 1e-12, "tf32x3": 2e-5, "bf16x3": 2e-4, "tf32": 2e-2, "bf16": 1e-1}
+
+
+def _dev_ens(d):
+    from tdscha_b200 import _native
+    return _native.DeviceEnsemble(d["X"], d["Y"], d["w"], d["rho"], d["T"], d["syms"], d["blocks"], d["blocks_ids"])
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+@pytest.mark.parametrize("fixture", ["mode10", "rocksalt_l2"])
+@pytest.mark.parametrize("precision", list(TOL))
+def test_averages_match_reference_golden(request, cuda, fixture, precision):
+    d = request.getfixturevalue(fixture)
+    ens = _dev_ens(d)
+    for case in ("case0", "case1", "case2"):
+        f, dv = ens.perturb_average(d[f"{case}_R1"], d[f"{case}_Y1"], int(d[f"{case}_d4"]), precision)
+        ef, ed = _rel(f, d[f"{case}_f"]), _rel(dv, d[f"{case}_d2v"])
+        print(f"{fixture} {precision} {case}: f {ef:.2e} d2v {ed:.2e}")
+        assert ef < TOL[precision] and ed < TOL[precision], (case, ef, ed)
+    ens.close()
+
+
+def test_one_shot_drop_in_matches_golden(cuda, mode10):
+    """tdscha_GetPerturbAverageSym: the reference's argument list, outputs written in place."""
+    from tdscha_b200 import _native
+    d = mode10
+    n = d["X"].shape[1]
+    f = np.zeros(n)
+    dv = np.zeros((n, n))
+    _native.get_perturb_average_sym(d["X"], d["Y"], d["w"], d["rho"], d["case1_R1"], d["case1_Y1"], d["T"], 1,
+                                    d["syms"][0].shape[0], d["syms"], d["n_deg"], d["blocks"], d["blocks_ids"], f, dv)
+    assert _rel(f, d["case1_f"]) < 1e-12 and _rel(dv, d["case1_d2v"]) < 1e-12
+
+
+def test_batched_device_averages_equal_single(cuda, rocksalt_l2):
+    torch = cuda
+    d = rocksalt_l2
+    ens = _dev_ens(d)
+    n = d["X"].shape[1]
+    R = torch.as_tensor(np.stack([d[f"case{c}_R1"] for c in range(2)]), device="cuda")
+    Y = torch.as_tensor(np.stack([d[f"case{c}_Y1"] for c in range(2)]), device="cuda")
+    f = torch.empty((2, n), dtype=torch.float64, device="cuda")
+    dv = torch.empty((2, n, n), dtype=torch.float64, device="cuda")
+    ens.perturb_average_device(R, Y, f, dv, 1, "fp64")
+    torch.cuda.synchronize()
+    for c in range(2):
+        assert _rel(f[c].cpu().numpy(), d[f"case{c}_f"]) < 1e-12
+        assert _rel(dv[c].cpu().numpy(), d[f"case{c}_d2v"]) < 1e-12
+
+
+def test_bad_blocks_raise_not_exit(cuda, mode10):
+    """Argument errors come back as exceptions (the reference's binding calls exit())."""
+    from tdscha_b200 import _native
+    d = mode10
+    blocks = [b.copy() for b in d["blocks"]]
+    blocks[1] = blocks[1][::-1].copy()          # not ascending
+    with pytest.raises(_native.TdschaError, match="contiguous"):
+        _native.DeviceEnsemble(d["X"], d["Y"], d["w"], d["rho"], d["T"], d["syms"], blocks, d["blocks_ids"])
+    w = d["w"].copy()
+    w[1] *= 1.001                               # breaks the degeneracy of block 0
+    with pytest.raises(_native.TdschaError, match="degenerate"):
+        _native.DeviceEnsemble(d["X"], d["Y"], w, d["rho"], d["T"], d["syms"], d["blocks"], d["blocks_ids"])
+    ens = _dev_ens(d)
+    with pytest.raises(_native.TdschaError, match="apply_D4"):
+        ens.perturb_average(d["case0_R1"], d["case0_Y1"], 2, "fp64")
