@@ -1,0 +1,413 @@
+"""Benchmark of the TD-SCHA Lanczos hot path on B200: apply_full_L throughput (apply_L/s).
+
+Workload (default): rock-salt 4x4x4 supercell (128 atoms, n = 381 modes), N = 10000 configurations
+at T = 300 K, 3072 symmetry operations (O_h x 64), seeded synthetic ensemble; `--chains` bi-conjugate
+Lanczos chains advanced in lockstep, so one step = one batched apply of 2*chains vectors (L q and
+L^T p of every chain) + one batched FP64 recurrence launch.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision bf16x3] [--chains 8]
+  python bench.py --impl reference       # the reference's own C kernel on the host cores
+Under torchrun every rank runs its own chains on its own GPU (weak scaling, no collective on the
+data path); the time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+for _p in (REPO, os.path.join(REPO, "python-sscha_b200")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "apply_L/s at 128 atoms N=1e4: mixed+batched vs FP64 GPU at G(w) rel err <=1e-5"
+RY_TO_CM = 109737.31568160
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="bf16x3")
+    ap.add_argument("--chains", type=int, default=8)
+    ap.add_argument("--L", type=int, default=4)
+    ap.add_argument("--N", type=int, default=10000)
+    ap.add_argument("--T", type=float, default=300.0)
+    ap.add_argument("--accuracy-steps", type=int, default=30)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true")
+    return ap.parse_args()
+
+
+def workload_name(a):
+    nat = 2 * a.L ** 3
+    return (f"rock-salt {a.L}x{a.L}x{a.L} ({nat} atoms, n={3 * nat - 3}), N={a.N}, T={a.T:g} K, "
+            f"O_h x {a.L ** 3} = {48 * a.L ** 3} symmetries, {a.chains} bi-conjugate chains "
+            f"(2 x {a.chains} applies per step)")
+
+
+# ------------------------------------------------------------------------------------------------
+# CPU baseline: the reference's GetPerturbAverageSym (oracle/_ref, compiled from its sources)
+# ------------------------------------------------------------------------------------------------
+_REF_DATA = {}
+
+
+def _ref_worker(i):
+    d = _REF_DATA
+    from oracle import lanczos_oracle as LO
+    t0 = time.perf_counter()
+    LO.perturb_average_sym(d["X"][i:i + 1], d["Y"][i:i + 1], d["w"], d["rho"][i:i + 1], d["R1"], d["Y1"], d["T"], 1,
+                           d["syms"], d["n_deg"], d["degs"], d["bid"], backend="reference")
+    return time.perf_counter() - t0
+
+
+def cpu_reference_timing(system, X, Y, rho, seconds_target=20.0, max_procs=None):
+    """Time the reference kernel on P host processes, one configuration each (the reference's MPI
+    partition: contiguous config slices, LanczosFunctions.c:2123-2136).  Returns (apply/s for the
+    full ensemble, cores, sample description).  The per-(configuration, symmetry) cost is O(n^2)
+    and the same for every pair, so the full apply time is the sample time x (N N_sym) / pairs.
+    Must run before any CUDA context exists in this process (the pool forks)."""
+    import multiprocessing as mp
+    n = system.n_modes
+    rng = np.random.default_rng(7)
+    R1 = rng.standard_normal(n) * 1e-3
+    Y1 = rng.standard_normal((n, n)) * 1e-3
+    Y1 = Y1 + Y1.T
+    procs = max_procs or min(os.cpu_count() or 1, 64)
+    # bounded sample: a slice of the symmetry group keeps one task near seconds_target on big cells
+    per_pair = 6.4e-3 * (n / 381.0) ** 2
+    n_sym_sample = int(min(system.n_syms, max(48, seconds_target / per_pair)))
+    _REF_DATA.update(X=X, Y=Y, w=system.w, rho=rho, R1=R1, Y1=Y1, T=system.T,
+                     syms=[s[:n_sym_sample] for s in system.symmetries],
+                     n_deg=np.array([len(d) for d in system.deg_space], dtype=np.intc), degs=system.deg_space,
+                     bid=system.blocks_ids)
+    ctx = mp.get_context("fork")
+    t0 = time.perf_counter()
+    with ctx.Pool(procs) as pool:
+        per_task = pool.map(_ref_worker, range(procs))
+    wall = time.perf_counter() - t0
+    pairs_sample = procs * n_sym_sample
+    pairs_full = X.shape[0] * system.n_syms
+    t_apply = max(per_task) * pairs_full / pairs_sample
+    sample = (f"reference GetPerturbAverageSym (oracle/_ref, gcc -O2) on {procs} processes x 1 configuration x "
+              f"{n_sym_sample} symmetries ({pairs_sample} pairs, {wall:.1f} s wall); one apply = "
+              f"{pairs_full} pairs, extrapolated linearly in pairs")
+    return 1.0 / t_apply, procs, sample
+
+
+# ------------------------------------------------------------------------------------------------
+def clocks_sampler_start(path):
+    try:
+        f = open(path, "w")
+        p = subprocess.Popen(["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                              "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "200"],
+                             stdout=f, stderr=subprocess.DEVNULL)
+        return p, f
+    except Exception:
+        return None, None
+
+
+def clocks_sampler_stop(p, f, path, device_index):
+    if p is None:
+        return None
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except Exception:
+        p.kill()
+    f.close()
+    sm, smax, reasons = [], None, set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for line in open(path):
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) < 9 or parts[0] != str(device_index):
+            continue
+        try:
+            sm.append(float(parts[1]))
+            smax = float(parts[2])
+        except ValueError:
+            continue
+        for nm, v in zip(names, parts[5:9]):
+            if v.lower() == "active":
+                reasons.add(nm)
+    if not sm:
+        return None
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------------
+def run_reference_arm(a, rank):
+    if rank != 0:
+        return None
+    from tdscha_b200 import rocksalt as RS
+    s = RS.build_system(a.L, T=a.T)
+    X, Y, rho = RS.sample_ensemble(s, a.N, seed=0)
+    vals = []
+    for _ in range(max(1, a.warmup // 3)):      # untimed warm-up (import + page-in)
+        cpu_reference_timing(s, X, Y, rho, seconds_target=2.0, max_procs=min(2, os.cpu_count() or 1))
+    cores = 1
+    sample = ""
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        v, cores, sample = cpu_reference_timing(s, X, Y, rho, seconds_target=8.0)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    v = float(np.mean(vals))
+    line = {"metric": METRIC, "value": v, "unit": "apply_L/s", "n_gpus": a.gpus, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded rock-salt ensemble)",
+            "config": {"workload": workload_name(a), "N": a.N, "n_modes": s.n_modes, "N_sym": s.n_syms},
+            "impl": "reference",
+            "cpu_baseline": {"value": v, "unit": "apply_L/s", "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "apply_L/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "wall_s": wall}
+    return line
+
+
+# ------------------------------------------------------------------------------------------------
+def main():
+    a = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if a.impl == "reference":
+        line = run_reference_arm(a, rank)
+        if line is not None:
+            print(json.dumps(line))
+        return
+
+    from tdscha_b200 import rocksalt as RS
+
+    # CPU baseline first (spawned processes, before any CUDA context): rank 0 at N = 1 only
+    s = RS.build_system(a.L, T=a.T)
+    X, Y, rho = RS.sample_ensemble(s, a.N, seed=0)
+    cpu_base = None
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        try:
+            v, cores, sample = cpu_reference_timing(s, X, Y, rho)
+            cpu_base = {"value": v, "unit": "apply_L/s", "cores": cores, "kind": "reference", "sample": sample}
+        except Exception as ex:   # reference kernel not built on this machine
+            cpu_base = {"value": None, "unit": "apply_L/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {ex}"}
+
+    import torch
+    import torch.distributed as dist
+    from tdscha_b200 import _native
+    from tdscha_b200.DynamicalLanczos import Lanczos, run_FT_batched
+
+    torch.cuda.set_device(local_rank)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+
+    ens = _native.DeviceEnsemble(X, Y, s.w, rho, s.T, s.symmetries, s.deg_space, s.blocks_ids)
+    n = s.n_modes
+    ln = n + n * (n + 1)
+    nc = a.chains
+    nb = 2 * nc
+    opts = _native.ApplyOpts(0, 0, 0, 0, 0, 0.0)
+    gen = torch.Generator(device="cpu").manual_seed(1000 + rank)
+    q0 = torch.randn(nc, ln, generator=gen, dtype=torch.float64)
+    q0 /= q0.norm(dim=1, keepdim=True)
+    dev = f"cuda:{local_rank}"
+    stream = torch.cuda.current_stream()
+
+    state = {}
+
+    def reset_chains():
+        state["q"] = q0.to(dev).contiguous()
+        state["p"] = state["q"].clone()
+        state["qp"] = torch.zeros_like(state["q"])
+        state["pp"] = torch.zeros_like(state["q"])
+        state["sc"] = torch.tensor([[0.0, 0.0, 1.0, 0.0, 1.0, 0.0]] * nc, dtype=torch.float64, device=dev)
+        state["k"] = 0
+
+    vec = torch.empty((nb, ln), dtype=torch.float64, device=dev)
+    out = torch.empty_like(vec)
+    qn = torch.empty((nc, ln), dtype=torch.float64, device=dev)
+    pn = torch.empty_like(qn)
+    sc_out = torch.empty((nc, 4), dtype=torch.float64, device=dev)
+    tr = [0] * nc + [1] * nc
+
+    def step(prec):
+        """One bi-conjugate step of every chain: batched apply of [q; p] + batched recurrence."""
+        vec[:nc].copy_(state["q"])
+        vec[nc:].copy_(state["p"])
+        ens.apply_full_L(vec, out, tr, opts, prec)
+        _native.lanczos_step(out[:nc], out[nc:], state["q"], state["p"], state["qp"], state["pp"], state["sc"], None,
+                             qn, pn, sc_out)
+        # history for the next step (device-side scalar bookkeeping, no host sync)
+        k = state["k"]
+        sc_prev = state["sc"]
+        new = torch.empty_like(sc_prev)
+        new[:, 0] = sc_out[:, 2]                      # c_k
+        new[:, 1] = sc_out[:, 1]                      # b_k
+        new[:, 2] = sc_out[:, 3]                      # s_norm_{k+1}
+        new[:, 3] = sc_prev[:, 2]                     # s_norm_k
+        new[:, 4] = sc_prev[:, 0] if k >= 1 else 1.0  # c_{k-1}
+        new[:, 5] = k + 1
+        state["qp"], state["pp"] = state["q"], state["p"]
+        state["q"], state["p"] = qn.clone(), pn.clone()
+        state["sc"] = new
+        state["k"] = k + 1
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------- device-resident throughput ----------------
+    reset_chains()
+    for _ in range(a.warmup):
+        step(a.precision)
+    ens.read_profile()
+    ens.set_profiling(True)
+    smi_path = os.path.join(REPO, f".bench_clocks_{rank}.csv")
+    sp, sf = clocks_sampler_start(smi_path)
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        step(a.precision)
+    e1.record(stream)
+    barrier()
+    clocks = clocks_sampler_stop(sp, sf, smi_path, local_rank)
+    try:
+        os.remove(smi_path)
+    except OSError:
+        pass
+    ms_total = max_over_ranks(e0.elapsed_time(e1))
+    prof = ens.read_profile()
+    ens.set_profiling(False)
+    applies = nb * a.steps * world
+    value = applies / (ms_total / 1e3)
+    launches = sum(c for _, c in prof.values()) + 3 * a.steps          # + 3 recurrence kernels per step
+
+    # roofline of the dominant contraction ([a | b] projection, K = n(n+1)/2)
+    P = n * (n + 1) // 2
+    ab_ms, ab_launches = prof["gemm_ab"]
+    flops_ab_per_apply = 2.0 * s.n_syms * (2 * a.N) * P                # = 2 N N_sym n(n+1) ~ 2 M n^2
+    flops_per_launch = flops_ab_per_apply * nb * a.steps / max(ab_launches, 1)
+    t_launch = ab_ms / 1e3 / max(ab_launches, 1)
+    peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(REPO, "MEASURED_PEAKS.json")) else {}
+    bf16_peak = peaks.get("bf16_tflops", 1590.0)
+    peak_src = "of measured" if "bf16_tflops" in peaks else "of fallback"
+    nprod = 3 if a.precision.endswith("x3") else 1
+    rate_div = {"bf16": 1.0, "tf32": 2.0}[a.precision[:4]] * nprod
+    achieved = flops_per_launch / t_launch / 1e12
+    roofline = {"kernel": "tc_gemm_kernel ([a|b] = Y~ . V^T projection)", "bound": "tensor",
+                "achieved": achieved, "peak": bf16_peak / rate_div, "unit": "TFLOP/s",
+                "frac": achieved / (bf16_peak / rate_div), "traffic": None,
+                "peak_basis": f"{peak_src} bf16 dense burst {bf16_peak} TFLOP/s / {rate_div:g} "
+                              f"({nprod} product(s){', tf32 at half the bf16 rate' if a.precision.startswith('tf32') else ''})",
+                "algorithmic_flops_per_launch": flops_per_launch, "avg_launch_ms": t_launch * 1e3}
+    total_prof = sum(v for v, _ in prof.values()) or 1.0
+    stage_share = {k: round(v / total_prof, 4) for k, (v, _) in prof.items()}
+
+    # ---------------- end to end through the host-buffer API ----------------
+    host_in = torch.empty((nb, ln), dtype=torch.float64).pin_memory()
+    host_out = torch.empty((nb, ln), dtype=torch.float64).pin_memory()
+    host_in.copy_(vec.cpu())
+    barrier()
+    for _ in range(2):
+        vec.copy_(host_in, non_blocking=True)
+        ens.apply_full_L(vec, out, tr, opts, a.precision)
+        host_out.copy_(out, non_blocking=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(a.steps):
+        vec.copy_(host_in, non_blocking=True)
+        ens.apply_full_L(vec, out, tr, opts, a.precision)
+        host_out.copy_(out, non_blocking=True)
+    e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e = {"value": applies / (e2e_ms / 1e3), "unit": "apply_L/s", "h2d_bytes_per_step": nb * ln * 8,
+           "d2h_bytes_per_step": nb * ln * 8}
+
+    # ---------------- FP64 GPU path (the comparison arm of the metric) ----------------
+    fp64_ms = None
+    if rank == 0:
+        v2 = vec[:2].clone()
+        o2 = torch.empty_like(v2)
+        ens.apply_full_L(v2, o2, [0, 1], opts, "fp64")
+        torch.cuda.synchronize()
+        e0.record(stream)
+        ens.apply_full_L(v2, o2, [0, 1], opts, "fp64")
+        e1.record(stream)
+        torch.cuda.synchronize()
+        fp64_ms = e0.elapsed_time(e1)
+    fp64_value = 2 / (fp64_ms / 1e3) if fp64_ms else None
+
+    # ---------------- G(w) accuracy of the mixed chain vs the FP64 chain ----------------
+    accuracy = None
+    if rank == 0 and not a.no_accuracy and a.accuracy_steps > 0:
+        ens_obj = RS.SyntheticEnsemble(T=s.T, nat=s.nat, m=s.masses, w=s.w, pols=s.pols, N=a.N, rho=rho, X=X, Y=Y,
+                                       symmetries=s.symmetries, deg_space=s.deg_space, blocks_ids=s.blocks_ids,
+                                       supercell=(a.L,) * 3)
+        chains = {}
+        for prec in ("fp64", a.precision):
+            L = Lanczos(ens_obj, precision=prec)
+            L.symmetries, L.degenerate_space, L.sym_block_id = s.symmetries, s.deg_space, s.blocks_ids
+            L.N_degeneracy = np.array([len(d) for d in s.deg_space], dtype=np.intc)
+            L.n_syms, L.initialized, L.device_ensemble = s.n_syms, True, ens
+            L.prepare_random(seed=11, sector="R")
+            run_FT_batched([L], a.accuracy_steps, precision=prec)
+            chains[prec] = L
+        w_cm = np.linspace(0, 400, 500)
+        wr = w_cm / RY_TO_CM
+        eta = 5.0 / RY_TO_CM
+        g64 = chains["fp64"].get_green_function_continued_fraction(wr, use_terminator=False, smearing=eta)
+        gmx = chains[a.precision].get_green_function_continued_fraction(wr, use_terminator=False, smearing=eta)
+        k = min(len(chains["fp64"].a_coeffs), len(chains[a.precision].a_coeffs))
+        a64, amx = np.array(chains["fp64"].a_coeffs[:k]), np.array(chains[a.precision].a_coeffs[:k])
+        kb = min(len(chains["fp64"].b_coeffs), len(chains[a.precision].b_coeffs))
+        b64, bmx = np.array(chains["fp64"].b_coeffs[:kb]), np.array(chains[a.precision].b_coeffs[:kb])
+        accuracy = {"steps": a.accuracy_steps, "omega": "500 points 0-400 cm^-1, smearing 5 cm^-1",
+                    "g_rel_err_max": float(np.abs(gmx - g64).max() / np.abs(g64).max()),
+                    "g_rel_err_pointwise_median": float(np.median(np.abs(gmx - g64) / np.abs(g64))),
+                    "a_rel_err_max": float(np.max(np.abs(amx - a64) / np.abs(a64))),
+                    "b_rel_err_max": float(np.max(np.abs(bmx - b64) / np.abs(b64))) if kb else None}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "apply_L/s", "n_gpus": world, "steps": a.steps,
+                "warmup": a.warmup, "ms_per_step": ms_total / a.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": f"{a.precision} contractions (f32 accumulate) + f64 recurrence",
+                "data": "synthetic (seeded rock-salt ensemble)",
+                "config": {"workload": workload_name(a), "N": a.N, "n_modes": n, "N_sym": s.n_syms, "chains": nc,
+                           "applies_per_step_per_gpu": nb, "precision": a.precision,
+                           "l2": "inputs larger than L2 (ensemble operands several GB per precision)",
+                           "parallelism": f"replicas x{world} (independent chains per GPU)"},
+                "roofline": roofline, "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clocks, "fp64_gpu_value": fp64_value,
+                "ratio_vs_fp64_gpu": (value / world) / fp64_value if fp64_value else None,
+                "accuracy_vs_fp64": accuracy, "stage_share": stage_share,
+                "stage_ms": {k: round(v, 3) for k, (v, _) in prof.items()}}
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

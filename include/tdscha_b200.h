@@ -64,7 +64,7 @@ const char *tdscha_version(void);
  *   deg_space   n_blocks pointers, each to n_deg[b] int mode indices (contiguous, ascending)
  *   sym_blocks  n_blocks pointers, each to an (N_sym, n_deg[b], n_deg[b]) C-order table
  *   blocks_ids  (n) block of each mode
- * Every frequency inside a block must be equal to within 1e-6 relative (degenerate subspace).
+ * Every frequency inside a block must be equal to within 1e-10 relative (degenerate subspace).
  */
 int tdscha_ensemble_create(const double *X, const double *Y, const double *w, const double *rho,
                            int N, int n, double T, int N_sym, int n_blocks, const int *n_deg,
@@ -144,6 +144,17 @@ int tdscha_continued_fraction_device(int n_iter, const double *a, const double *
                                      int last_average, double smearing, int use_wigner, int reverse_L,
                                      double shift_value, double perturbation_modulus, double *gf_out,
                                      void *stream);
+
+/*
+ * Profiling hooks (no counterpart in the reference, whose only timers are wall clocks printed per
+ * apply, DynamicalLanczos.py:3521-3551).  When enabled, every averages call records CUDA events on
+ * its launching stream around each stage.  tdscha_read_profile synchronises, returns the summed
+ * milliseconds and the launch counts of the n_stages stages (0 transform, 1 contraction [a|b],
+ * 2 contraction [c|d], 3 weights, 4 contraction Z, 5 contraction F, 6 fold, 7 other) since the
+ * last read, and resets them.  Launch counts are kept even with profiling disabled.
+ */
+int tdscha_set_profiling(tdscha_ensemble *ens, int enable);
+int tdscha_read_profile(tdscha_ensemble *ens, double *ms, long long *launches, int n_stages);
 
 /*
  * The tensor-core contraction used by the averages, exposed for testing and reuse (no counterpart

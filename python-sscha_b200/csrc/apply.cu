@@ -178,6 +178,7 @@ int apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int
     double *dav = fav + (size_t)nb * n;
     TD_CHECK(nb <= 64, TDSCHA_EINVAL, "at most 64 vectors per apply call");
     TD_CUDA(cudaMemcpyAsync(tr_d, transpose_h, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+    e->prof.launches[ST_OTHER] += o.ignore_v3 ? 1 : 2;
     if (!o.ignore_v3) {
         prologue_kernel<<<grid_for((long long)nb * P), 256, 0, st>>>(nb, n, len, psi, tr_d, e->w, e->T, o.use_wigner, R, Ys);
         TD_CUDA(cudaGetLastError());

@@ -187,6 +187,32 @@ int tdscha_continued_fraction_device(int n_iter, const double *a, const double *
                                      reverse_L, shift_value, perturbation_modulus, gf_out, static_cast<cudaStream_t>(stream));
 }
 
+int tdscha_set_profiling(tdscha_ensemble *e, int enable) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    e->prof.enabled = enable != 0;
+    return 0;
+}
+
+int tdscha_read_profile(tdscha_ensemble *e, double *ms, long long *launches, int n_stages) {
+    TD_CHECK(e != nullptr && n_stages > 0, TDSCHA_EINVAL, "bad arguments");
+    TD_CUDA(cudaSetDevice(e->device));
+    for (int s = 0; s < n_stages && s < ST_COUNT; ++s) {
+        if (ms) ms[s] = 0.0;
+        if (launches) launches[s] = e->prof.launches[s];
+    }
+    for (auto &r : e->prof.recs) {
+        float t = 0.f;
+        TD_CUDA(cudaEventSynchronize(r.b));
+        TD_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+        if (ms && r.stage < n_stages) ms[r.stage] += t;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    e->prof.recs.clear();
+    for (int s = 0; s < ST_COUNT; ++s) e->prof.launches[s] = 0;
+    return 0;
+}
+
 int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, const void *A_lo, long long lda,
                        const void *B_hi, const void *B_lo, long long ldb, float *D, long long ldd, void *stream) {
     clear_error();

@@ -12,9 +12,9 @@
 
 namespace tdscha {
 
-constexpr int SYM_THREADS = 256;
-constexpr int FOLD_MAXE = 36;     // accumulator elements per thread: d_b * d_c <= 36 * 256 (dmax 96)
-constexpr int DMAX_SUPPORTED = 96;
+constexpr int SYM_THREADS = 256;   // 16 x 16 thread grid for the small block products
+constexpr int MT = 5;              // register micro-tile: each thread owns up to 5 x 5 outputs
+constexpr int DMAX_SUPPORTED = 16 * MT;
 
 // ------------------------------------------------------------------------------------------------
 // operand builders (once per ensemble and storage format)
@@ -129,19 +129,51 @@ __device__ __forceinline__ long long pair_index(int mu, int nu, int n) {   // mu
     return (long long)mu * n - ((long long)mu * (mu - 1)) / 2 + (nu - mu);
 }
 
+// acc (+)= A (m x k) . B (k x n) on shared-memory operands addressed with (row, col) strides; thread
+// (ty, tx) of the 16 x 16 grid owns rows ty + 16 i and columns tx + 16 j (i, j < MT).
+__device__ __forceinline__ void mm_tile(double (&acc)[MT][MT], const double *A, int a_rs, int a_cs, const double *B, int b_rs,
+                                        int b_cs, int m, int n, int k, int ty, int tx) {
+    for (int kk = 0; kk < k; ++kk) {
+        double a[MT], b[MT];
+#pragma unroll
+        for (int i = 0; i < MT; ++i) {
+            const int r = ty + 16 * i;
+            a[i] = r < m ? A[r * a_rs + kk * a_cs] : 0.0;
+        }
+#pragma unroll
+        for (int j = 0; j < MT; ++j) {
+            const int c = tx + 16 * j;
+            b[j] = c < n ? B[kk * b_rs + c * b_cs] : 0.0;
+        }
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int j = 0; j < MT; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+}
+
+__device__ __forceinline__ void zero_tile(double (&acc)[MT][MT]) {
+#pragma unroll
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < MT; ++j) acc[i][j] = 0.0;
+}
+
 __global__ void __launch_bounds__(SYM_THREADS)
 transform_kernel(SymTables t, const double *__restrict__ Ys, const double *__restrict__ R1, const double *__restrict__ ups,
                  int Jc, int j0, long long P, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo,
                  void *r1_hi, void *r1_lo) {
     extern __shared__ double sm[];
     const int dmax = t.dmax;
-    double *Sb = sm;                   // d_b x d_b
+    double *Sb = sm;                   // d_b x d_b   S_j block b (row-major: S[p][mu])
     double *Sc = Sb + dmax * dmax;     // d_c x d_c
-    double *tmp = Sc + dmax * dmax;    // d_b x d_c
+    double *Yt = Sc + dmax * dmax;     // d_b x d_c   Ys[b, c]
+    double *M1 = Yt + dmax * dmax;     // d_b x d_c   Ys[b, c] S_c
     const int r = blockIdx.x, b = blockIdx.y;
     const int k = r / Jc, j = j0 + r % Jc;
     const int n = t.n;
     const int sb = t.start[b], db = t.dim[b];
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
     const double *Yk = Ys + (long long)k * n * n;
     const double *Rk = R1 + (long long)k * n;
     const double *Sbg = t.sym + t.off[b] + (long long)j * db * db;
@@ -162,25 +194,30 @@ transform_kernel(SymTables t, const double *__restrict__ Ys, const double *__res
         const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
         __syncthreads();
         for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) Sc[e] = Scg[e];
+        for (int e = threadIdx.x; e < db * dc; e += blockDim.x) Yt[e] = Yk[(long long)(sb + e / dc) * n + sc + e % dc];
         __syncthreads();
-        // tmp[p', nu'] = sum_q' Ys[sb + p', sc + q'] S_c[q', nu']
-        for (int e = threadIdx.x; e < db * dc; e += blockDim.x) {
-            const int p = e / dc, nu = e % dc;
-            const double *yrow = Yk + (long long)(sb + p) * n + sc;
-            double acc = 0.0;
-            for (int q = 0; q < dc; ++q) acc += yrow[q] * Sc[q * dc + nu];
-            tmp[e] = acc;
-        }
+        double acc[MT][MT];
+        zero_tile(acc);
+        mm_tile(acc, Yt, dc, 1, Sc, dc, 1, db, dc, dc, ty, tx);          // M1 = Ys[b,c] S_c
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int jj = 0; jj < MT; ++jj) {
+                const int rr = ty + 16 * i, cc = tx + 16 * jj;
+                if (rr < db && cc < dc) M1[rr * dc + cc] = acc[i][jj];
+            }
         __syncthreads();
-        // out[mu', nu'] = sum_p' S_b[p', mu'] tmp[p', nu']
-        for (int e = threadIdx.x; e < db * dc; e += blockDim.x) {
-            const int mu = e / dc, nu = e % dc;
-            const int gm = sb + mu, gn = sc + nu;
-            if (gm > gn) continue;
-            double acc = 0.0;
-            for (int p = 0; p < db; ++p) acc += Sb[p * db + mu] * tmp[p * dc + nu];
-            store_split(fmt, B1_hi, B1_lo, (long long)r * Kp + pair_index(gm, gn, n), acc);
-        }
+        zero_tile(acc);
+        mm_tile(acc, Sb, 1, db, M1, dc, 1, db, dc, db, ty, tx);          // S_b^T M1
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int jj = 0; jj < MT; ++jj) {
+                const int mu = ty + 16 * i, nu = tx + 16 * jj;
+                const int gm = sb + mu, gn = sc + nu;
+                if (mu < db && nu < dc && gm <= gn)
+                    store_split(fmt, B1_hi, B1_lo, (long long)r * Kp + pair_index(gm, gn, n), acc[i][jj]);
+            }
     }
 }
 
@@ -225,10 +262,10 @@ fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ b
             double *__restrict__ partD, double *__restrict__ partF) {
     extern __shared__ double sm[];
     const int dmax = t.dmax;
-    double *Sb = sm;
-    double *Sc = Sb + dmax * dmax;
-    double *Wt = Sc + dmax * dmax;
-    double *tmp = Wt + dmax * dmax;
+    double *Sb = sm;                   // d_b x d_b  S_j block b, row-major S[mu][p]
+    double *ScT = Sb + dmax * dmax;    // d_c x d_c  transposed: ScT[q][nu] = S_c[nu][q]
+    double *Wt = ScT + dmax * dmax;    // d_b x d_c  W_j[b, c]
+    double *U = Wt + dmax * dmax;      // d_b x d_c  W_j[b, c] S_c^T
     const int b = bp_b[blockIdx.x], c = bp_c[blockIdx.x];
     const int fc = blockIdx.y, k = blockIdx.z;
     const int n = t.n;
@@ -236,9 +273,9 @@ fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ b
     const int fg = j0 / Jf + fc;
     const int ja = j0 + fc * Jf, jb = min(j0 + (fc + 1) * Jf, j0 + nj);
     const int ne = db * dc;
-    double acc[FOLD_MAXE];
-#pragma unroll
-    for (int u = 0; u < FOLD_MAXE; ++u) acc[u] = 0.0;
+    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
+    double acc[MT][MT];
+    zero_tile(acc);
     double facc = 0.0;   // f partial for mode sb + threadIdx.x (diagonal pairs only)
     for (int j = ja; j < jb; ++j) {
         const long long r = (long long)k * Jc + (j - j0);
@@ -246,7 +283,7 @@ fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ b
         const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
         __syncthreads();
         for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = Sbg[e];
-        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) Sc[e] = Scg[e];
+        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) ScT[(e % dc) * dc + e / dc] = Scg[e];
         for (int e = threadIdx.x; e < ne; e += blockDim.x) {
             const int p = e / dc, q = e % dc;
             int gm = sb + p, gn = sc + q;
@@ -255,13 +292,16 @@ fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ b
             Wt[e] = (gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn] * z;
         }
         __syncthreads();
-        // tmp = W S_c^T : tmp[p, nu] = sum_q W[p, q] S_c[nu, q]
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int p = e / dc, nu = e % dc;
-            double s = 0.0;
-            for (int q = 0; q < dc; ++q) s += Wt[p * dc + q] * Sc[nu * dc + q];
-            tmp[e] = s;
-        }
+        double u[MT][MT];
+        zero_tile(u);
+        mm_tile(u, Wt, dc, 1, ScT, dc, 1, db, dc, dc, ty, tx);        // U = W S_c^T
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int jj = 0; jj < MT; ++jj) {
+                const int rr = ty + 16 * i, cc = tx + 16 * jj;
+                if (rr < db && cc < dc) U[rr * dc + cc] = u[i][jj];
+            }
         if (b == c && threadIdx.x < db) {
             const AccT *Fr = F + r * ldf + sb;
             double s = 0.0;
@@ -269,23 +309,16 @@ fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ b
             facc += s;
         }
         __syncthreads();
-#pragma unroll
-        for (int u = 0; u < FOLD_MAXE; ++u) {
-            const int e = threadIdx.x + u * SYM_THREADS;
-            if (e < ne) {
-                const int mu = e / dc, nu = e % dc;
-                double s = 0.0;
-                for (int p = 0; p < db; ++p) s += Sb[mu * db + p] * tmp[p * dc + nu];
-                acc[u] += s;
-            }
-        }
+        mm_tile(acc, Sb, db, 1, U, dc, 1, db, dc, db, ty, tx);        // acc += S_b U
     }
     double *out = partD + ((long long)k * nf_total + fg) * (long long)n * n;
 #pragma unroll
-    for (int u = 0; u < FOLD_MAXE; ++u) {
-        const int e = threadIdx.x + u * SYM_THREADS;
-        if (e < ne) out[(long long)(sb + e / dc) * n + sc + e % dc] = acc[u];
-    }
+    for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int jj = 0; jj < MT; ++jj) {
+            const int mu = ty + 16 * i, nu = tx + 16 * jj;
+            if (mu < db && nu < dc) out[(long long)(sb + mu) * n + sc + nu] = acc[i][jj];
+        }
     if (b == c && threadIdx.x < db) partF[((long long)k * nf_total + fg) * n + sb + threadIdx.x] = facc;
 }
 
@@ -315,6 +348,33 @@ __global__ void fold_reduce_kernel(const double *partD, const double *partF, int
 // ------------------------------------------------------------------------------------------------
 // host orchestration
 // ------------------------------------------------------------------------------------------------
+void Profile::begin(int stage, cudaStream_t st, ProfRec *r) {
+    r->stage = stage;
+    r->a = r->b = nullptr;
+    if (!enabled) return;
+    cudaEventCreate(&r->a);
+    cudaEventCreate(&r->b);
+    cudaEventRecord(r->a, st);
+}
+void Profile::end(ProfRec *r, cudaStream_t st) {
+    if (!enabled || !r->a) return;
+    cudaEventRecord(r->b, st);
+    recs.push_back(*r);
+}
+
+// Profile one stage: records CUDA events around the launches on the launching stream when enabled,
+// counts launches always.
+struct StageScope {
+    tdscha_ensemble *e;
+    cudaStream_t st;
+    ProfRec r;
+    StageScope(tdscha_ensemble *e_, int stage, cudaStream_t st_, int n_launch = 1) : e(e_), st(st_) {
+        e->prof.launches[stage] += n_launch;
+        e->prof.begin(stage, st, &r);
+    }
+    ~StageScope() { e->prof.end(&r, st); }
+};
+
 static int grid_for(long long total, int threads = 256) {
     long long g = (total + threads - 1) / threads;
     return (int)std::min<long long>(std::max<long long>(g, 1), 148LL * 32);
@@ -597,7 +657,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     double *partF = reinterpret_cast<double *>(W + L.partF);
 
     SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax};
-    const size_t sm_tr = 3 * (size_t)e->dmax * e->dmax * sizeof(double);
+    const size_t sm_tr = 4 * (size_t)e->dmax * e->dmax * sizeof(double);
     const size_t sm_fold = 4 * (size_t)e->dmax * e->dmax * sizeof(double);
     TD_CUDA(cudaFuncSetAttribute(transform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tr));
     TD_CUDA(cudaFuncSetAttribute(fold_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fold));
@@ -607,36 +667,62 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         const int nj = std::min(Jc, e->N_sym - j0);
         const long long M = (long long)nb * nj;
         // rows r = k * nj + jj
-        transform_kernel<<<dim3((unsigned)M, e->n_blocks), SYM_THREADS, sm_tr, st>>>(
-            t, Ys, R1, e->ups, nj, j0, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
-        TD_CUDA(cudaGetLastError());
+        {
+            StageScope sc(e, ST_TRANSFORM, st);
+            transform_kernel<<<dim3((unsigned)M, e->n_blocks), SYM_THREADS, sm_tr, st>>>(
+                t, Ys, R1, e->ups, nj, j0, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
+            TD_CUDA(cudaGetLastError());
+        }
         // GEMM1: [a | b] = B1 . V^T      (M x 2N, K = Kp)
-        TD_TRY(gemm_abt(e, fmt, nprod, B1_hi, B1_lo, e->Kp, M, o.V_hi, o.V_lo, e->Kp, e->N2, e->Kp, D1, L.ld1, st));
+        {
+            StageScope sc(e, ST_GEMM_AB, st);
+            TD_TRY(gemm_abt(e, fmt, nprod, B1_hi, B1_lo, e->Kp, M, o.V_hi, o.V_lo, e->Kp, e->N2, e->Kp, D1, L.ld1, st));
+        }
         // [c | d] = r1 . [X; G]^T         (M x 2N, K = np)
-        TD_TRY(gemm_abt(e, fmt, nprod, r1_hi, r1_lo, e->np, M, o.XG_hi, o.XG_lo, e->np, e->N2, e->np, Dcd, L.ld1, st));
+        {
+            StageScope sc(e, ST_GEMM_CD, st);
+            TD_TRY(gemm_abt(e, fmt, nprod, r1_hi, r1_lo, e->np, M, o.XG_hi, o.XG_lo, e->np, e->N2, e->np, Dcd, L.ld1, st));
+        }
         // weights
-        if (fmt == FMT_F64)
-            weights_kernel<double><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
-                (const double *)D1, (const double *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
-        else
-            weights_kernel<float><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
-                (const float *)D1, (const float *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
-        TD_CUDA(cudaGetLastError());
+        {
+            StageScope sc(e, ST_WEIGHTS, st);
+            if (fmt == FMT_F64)
+                weights_kernel<double><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
+                    (const double *)D1, (const double *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo,
+                    AB_hi, AB_lo);
+            else
+                weights_kernel<float><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
+                    (const float *)D1, (const float *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo,
+                    AB_hi, AB_lo);
+            TD_CUDA(cudaGetLastError());
+        }
         // GEMM2: Z = Cw . VT^T            (M x P, K = N2p)
-        TD_TRY(gemm_abt(e, fmt, nprod, Cw_hi, Cw_lo, e->N2p, M, o.VT_hi, o.VT_lo, e->N2p, e->P, e->N2p, Z, L.ldz, st));
+        {
+            StageScope sc(e, ST_GEMM_Z, st);
+            TD_TRY(gemm_abt(e, fmt, nprod, Cw_hi, Cw_lo, e->N2p, M, o.VT_hi, o.VT_lo, e->N2p, e->P, e->N2p, Z, L.ldz, st));
+        }
         // F = AB . YXt^T                  (M x n, K = N2p)
-        TD_TRY(gemm_abt(e, fmt, nprod, AB_hi, AB_lo, e->N2p, M, o.YXt_hi, o.YXt_lo, e->N2p, e->n, e->N2p, F, L.ldf, st));
+        {
+            StageScope sc(e, ST_GEMM_F, st);
+            TD_TRY(gemm_abt(e, fmt, nprod, AB_hi, AB_lo, e->N2p, M, o.YXt_hi, o.YXt_lo, e->N2p, e->n, e->N2p, F, L.ldf, st));
+        }
         // fold this chunk into the partials
-        dim3 fg((unsigned)e->bp_b.size(), (unsigned)ceil_div(nj, Jf), (unsigned)nb);
-        if (fmt == FMT_F64)
-            fold_kernel<double><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const double *)Z, L.ldz,
-                                                                   (const double *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total, partD, partF);
-        else
-            fold_kernel<float><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const float *)Z, L.ldz,
-                                                                  (const float *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total, partD, partF);
-        TD_CUDA(cudaGetLastError());
+        {
+            StageScope sc(e, ST_FOLD, st);
+            dim3 fg((unsigned)e->bp_b.size(), (unsigned)ceil_div(nj, Jf), (unsigned)nb);
+            if (fmt == FMT_F64)
+                fold_kernel<double><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const double *)Z, L.ldz,
+                                                                       (const double *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total,
+                                                                       partD, partF);
+            else
+                fold_kernel<float><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const float *)Z, L.ldz,
+                                                                      (const float *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total,
+                                                                      partD, partF);
+            TD_CUDA(cudaGetLastError());
+        }
     }
     const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
+    StageScope sc(e, ST_OTHER, st);
     fold_reduce_kernel<<<grid_for((long long)nb * e->n * e->n), 256, 0, st>>>(partD, partF, nf_total, e->n, nb, e->d_blocks_ids,
                                                                                norm, d_out, f_out);
     TD_CUDA(cudaGetLastError());

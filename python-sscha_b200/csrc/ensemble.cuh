@@ -43,6 +43,22 @@ struct Workspace {
     size_t bytes = 0;
 };
 
+// Stages of one averages call, for the optional CUDA-event profile.
+enum Stage : int { ST_TRANSFORM = 0, ST_GEMM_AB, ST_GEMM_CD, ST_WEIGHTS, ST_GEMM_Z, ST_GEMM_F, ST_FOLD, ST_OTHER, ST_COUNT };
+
+struct ProfRec {
+    int stage;
+    cudaEvent_t a, b;
+};
+
+struct Profile {
+    bool enabled = false;
+    std::vector<ProfRec> recs;
+    long long launches[ST_COUNT] = {0};
+    void begin(int stage, cudaStream_t st, ProfRec *r);
+    void end(ProfRec *r, cudaStream_t st);
+};
+
 }  // namespace tdscha
 
 struct tdscha_ensemble {
@@ -65,6 +81,7 @@ struct tdscha_ensemble {
     tdscha::Workspace ws;
     cublasHandle_t cublas = nullptr;
     size_t base_bytes = 0;
+    tdscha::Profile prof;
 };
 
 namespace tdscha {

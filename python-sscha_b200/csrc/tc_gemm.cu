@@ -346,6 +346,10 @@ int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, c
     TD_CHECK(op.fmt == FMT_TF32 || op.fmt == FMT_BF16, TDSCHA_EINVAL, "tc::gemm: operand format must be bf16 or tf32");
     TD_CHECK(K % (tf32 ? 32 : 64) == 0, TDSCHA_EINVAL, "tc::gemm: K=%d not a multiple of the 128-byte K block", K);
     TD_CHECK(op.nprod == 1 || op.nprod == 3, TDSCHA_EINVAL, "tc::gemm: nprod must be 1 or 3");
+    constexpr long long LD_MAX = 1LL << 31;
+    TD_CHECK(op.lda >= K && op.ldb >= K && ldd >= N && op.lda < LD_MAX && op.ldb < LD_MAX && ldd < LD_MAX, TDSCHA_EINVAL,
+             "tc::gemm: leading dimensions lda=%lld ldb=%lld ldd=%lld inconsistent with K=%d N=%d", op.lda, op.ldb, ldd, K, N);
+    TD_CHECK(op.A_hi && op.B_hi && D && (op.nprod == 1 || (op.A_lo && op.B_lo)), TDSCHA_EINVAL, "tc::gemm: NULL operand");
     if (tf32) {
         if (op.nprod == 3) return launch_cfg<256, 2, true, 3>(op, M, N, K, D, ldd, st, err);
         return launch_cfg<256, 4, true, 1>(op, M, N, K, D, ldd, st, err);

@@ -64,7 +64,11 @@ def load():
     lib.tdscha_continued_fraction_device.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                      vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp]
-    for name in ("tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    lib.tdscha_tc_contract.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_longlong,
+                                       vp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, vp]
+    lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
+    lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
+    for name in ("tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -128,6 +132,18 @@ class DeviceEnsemble:
         check(self._lib.tdscha_ensemble_device_bytes(self.handle, ctypes.byref(b)))
         return b.value
 
+    STAGES = ("transform", "gemm_ab", "gemm_cd", "weights", "gemm_z", "gemm_f", "fold", "other")
+
+    def set_profiling(self, enable=True):
+        check(self._lib.tdscha_set_profiling(self.handle, int(enable)))
+
+    def read_profile(self):
+        """{stage: (milliseconds, launches)} since the last read (synchronises)."""
+        ms = np.zeros(len(self.STAGES))
+        cnt = (ctypes.c_longlong * len(self.STAGES))()
+        check(self._lib.tdscha_read_profile(self.handle, _d(ms), cnt, len(self.STAGES)))
+        return {s: (float(ms[i]), int(cnt[i])) for i, s in enumerate(self.STAGES)}
+
     def perturb_average(self, R1, Y1, apply_d4=1, precision="fp64"):
         """Host-buffer drop-in of GetPerturbAverageSym: returns (f_av (n), d2v (n, n))."""
         R1 = np.ascontiguousarray(R1, dtype=np.float64)
@@ -178,6 +194,23 @@ def continued_fraction(a, b, c, omega, gf_out, use_terminator, last_average, sme
                                                omega.data_ptr(), int(use_terminator), int(last_average),
                                                float(smearing), int(use_wigner), int(reverse_L), float(shift_value),
                                                float(modulus), gf_out.data_ptr(), _stream_ptr(stream)))
+
+
+def tc_contract(precision, A_hi, A_lo, B_hi, B_lo, D, stream=None):
+    """D (M x N fp32 CUDA tensor, row stride D.stride(0)) = A (M x K) . B (N x K)^T on the tensor cores.
+    A_*/B_* are row-major CUDA tensors (bf16, or fp32 holding tf32 values); *_lo may be None for
+    the one-product modes."""
+    lib = load()
+    M, K = A_hi.shape
+    N = B_hi.shape[0]
+    for t in (A_hi, B_hi, D) + tuple(x for x in (A_lo, B_lo) if x is not None):
+        if not t.is_cuda or t.stride(-1) != 1:
+            raise ValueError("operands must be CUDA tensors with unit inner stride")
+    if D.dtype.itemsize != 4 or D.shape[0] < M or D.shape[1] < N:
+        raise ValueError("D must be an fp32 tensor of at least M x N")
+    ptr = lambda t: None if t is None else t.data_ptr()   # noqa: E731
+    check(lib.tdscha_tc_contract(PREC[precision], M, N, K, ptr(A_hi), ptr(A_lo), A_hi.stride(0), ptr(B_hi),
+                                 ptr(B_lo), B_hi.stride(0), D.data_ptr(), D.stride(0), _stream_ptr(stream)))
 
 
 def get_perturb_average_sym(X, Y, w, rho, R1, Y1, T, apply_D4, N_syms, sym_list, n_deg, deg_space_list, blocks_ids,
