@@ -121,6 +121,21 @@ int tdscha_apply_full_L_device(tdscha_ensemble *ens, int nb, const double *psi, 
                                const tdscha_apply_opts *opts, int precision, double *out, void *stream);
 
 /*
+ * The two halves of apply_full_L around the averages (Modules/DynamicalLanczos.py:2936-2993 and
+ * :3195-3281 / 2227-2385), for a caller that computes the averages of configuration slices on
+ * several devices and reduces them (the reference's MPI_Allreduce, CModules/LanczosFunctions.c:2237,
+ * 2417, 2731):
+ *   prologue: psi (nb, len) -> R1 (nb, n), Y1 (nb, n, n)  (unpacking, transpose mixing, Wigner alpha)
+ *   epilogue: psi, f_av (nb, n), d2v_av (nb, n, n) -> out (nb, len)  (L1, packing, signs, reverse, shift)
+ * prologue -> tdscha_perturb_average_sym_device -> epilogue equals tdscha_apply_full_L_device.
+ */
+int tdscha_apply_prologue_device(tdscha_ensemble *ens, int nb, const double *psi, const int *transpose,
+                                 const tdscha_apply_opts *opts, double *R1_out, double *Y1_out, void *stream);
+int tdscha_apply_epilogue_device(tdscha_ensemble *ens, int nb, const double *psi, const int *transpose,
+                                 const tdscha_apply_opts *opts, const double *f_av, const double *d2v_av,
+                                 double *out, void *stream);
+
+/*
  * One bi-conjugate Lanczos step (DynamicalLanczos.py:6059-6153, n_rep_orth = 0) for nc chains,
  * all FP64 on the device.  Per chain c the arrays hold vectors of length len:
  *   Lq, pL        L q_k and L^T p_k;   q, p   current q_k, p_k;   q_prev, p_prev   q_{k-1}, p_{k-1}

@@ -189,6 +189,35 @@ int apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int
     return 0;
 }
 
+// The two halves of apply_full_L around the averages, for callers that reduce the averages of
+// configuration slices across devices themselves.  tr_d: device copy of the transpose flags.
+int apply_prologue_device(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
+                          double *R, double *Ys, cudaStream_t st) {
+    TD_CHECK(e && psi && tr_d && R && Ys && nb > 0, TDSCHA_EINVAL, "bad prologue arguments");
+    tdscha_apply_opts o{0, 0, 0, 0, 0, 0.0};
+    if (opts) o = *opts;
+    const int n = e->n;
+    const long long P = (long long)n * (n + 1) / 2;
+    e->prof.launches[ST_OTHER] += 1;
+    prologue_kernel<<<grid_for((long long)nb * P), 256, 0, st>>>(nb, n, n + 2 * P, psi, tr_d, e->w, e->T, o.use_wigner, R, Ys);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int apply_epilogue_device(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
+                          const double *fav, const double *dav, double *out, cudaStream_t st) {
+    TD_CHECK(e && psi && tr_d && out && nb > 0, TDSCHA_EINVAL, "bad epilogue arguments");
+    tdscha_apply_opts o{0, 0, 0, 0, 0, 0.0};
+    if (opts) o = *opts;
+    TD_CHECK(o.ignore_v3 || (fav && dav), TDSCHA_EINVAL, "averages required unless ignore_v3");
+    const int n = e->n;
+    const long long len = n + (long long)n * (n + 1);
+    e->prof.launches[ST_OTHER] += 1;
+    epilogue_kernel<<<grid_for((long long)nb * len), 256, 0, st>>>(nb, n, len, psi, tr_d, e->w, e->T, o, fav, dav, out);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 size_t apply_scratch_bytes(const tdscha_ensemble *e, int nb) {
     const size_t n = e->n;
     return 256 + (size_t)nb * (2 * n + 2 * n * n) * sizeof(double);

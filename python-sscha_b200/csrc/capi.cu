@@ -23,6 +23,10 @@ void clear_error() { g_err[0] = 0; }
 int apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose_h, const tdscha_apply_opts *opts,
                         int precision, double *out, cudaStream_t st, void *scratch, size_t scratch_bytes);
 size_t apply_scratch_bytes(const tdscha_ensemble *e, int nb);
+int apply_prologue_device(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
+                          double *R, double *Ys, cudaStream_t st);
+int apply_epilogue_device(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
+                          const double *fav, const double *dav, double *out, cudaStream_t st);
 int lanczos_step_device(int nc, long long len, const double *Lq, const double *pL, const double *q, const double *p,
                         const double *q_prev, const double *p_prev, const double *sc_in, const double *mask, double *q_next,
                         double *p_next, double *sc_out, cudaStream_t st, double *scratch, size_t scratch_bytes);
@@ -37,7 +41,7 @@ struct Scratch {
     size_t bytes = 0;
     int device = -1;
 };
-static thread_local Scratch g_scratch[2];
+static thread_local Scratch g_scratch[3];
 
 static int scratch_get(int slot, size_t bytes, void **out) {
     int dev = 0;
@@ -165,6 +169,38 @@ int tdscha_apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, co
     TD_TRY(scratch_get(0, need, &buf));
     TD_TRY(apply_full_L_device(e, nb, psi, transpose, opts, precision, out, st, buf, need));
     return check_err_word(e, st);
+}
+
+static int upload_flags(int nb, const int *transpose, cudaStream_t st, int **tr_d) {
+    TD_CHECK(transpose && nb > 0 && nb <= 4096, TDSCHA_EINVAL, "bad transpose flags");
+    void *buf = nullptr;
+    TD_TRY(scratch_get(2, 4096 * sizeof(int), &buf));
+    TD_CUDA(cudaMemcpyAsync(buf, transpose, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+    *tr_d = static_cast<int *>(buf);
+    return 0;
+}
+
+int tdscha_apply_prologue_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose,
+                                 const tdscha_apply_opts *opts, double *R1_out, double *Y1_out, void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int *tr_d = nullptr;
+    TD_TRY(upload_flags(nb, transpose, st, &tr_d));
+    return apply_prologue_device(e, nb, psi, tr_d, opts, R1_out, Y1_out, st);
+}
+
+int tdscha_apply_epilogue_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose,
+                                 const tdscha_apply_opts *opts, const double *f_av, const double *d2v_av, double *out,
+                                 void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int *tr_d = nullptr;
+    TD_TRY(upload_flags(nb, transpose, st, &tr_d));
+    return apply_epilogue_device(e, nb, psi, tr_d, opts, f_av, d2v_av, out, st);
 }
 
 int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const double *pL, const double *q, const double *p,

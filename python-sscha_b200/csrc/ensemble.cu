@@ -8,13 +8,11 @@
 
 #include "common.cuh"
 #include "ensemble.cuh"
+#include "symmetry.cuh"
 #include "tc_gemm.cuh"
 
 namespace tdscha {
 
-constexpr int SYM_THREADS = 256;   // 16 x 16 thread grid for the small block products
-constexpr int MT = 5;              // register micro-tile: each thread owns up to 5 x 5 outputs
-constexpr int DMAX_SUPPORTED = 16 * MT;
 
 // ------------------------------------------------------------------------------------------------
 // operand builders (once per ensemble and storage format)
@@ -115,113 +113,6 @@ __global__ void symmetrize_kernel(int nb, int n, const double *Y, double *Ys) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// symmetry transform: B1[r, p(mu,nu)] = (S_j^T Ys_k S_j)[mu, nu]  and  r1[r, mu] = ups_mu (S_j^T R1_k)_mu
-//   grid (rows r = k*Jc + jj, blocks b); the CTA owns the row block b of Y~_j, all column blocks c >= b.
-// ------------------------------------------------------------------------------------------------
-struct SymTables {
-    const double *sym;
-    const long long *off;
-    const int *start, *dim;
-    int n_blocks, n, dmax;
-};
-
-__device__ __forceinline__ long long pair_index(int mu, int nu, int n) {   // mu <= nu
-    return (long long)mu * n - ((long long)mu * (mu - 1)) / 2 + (nu - mu);
-}
-
-// acc (+)= A (m x k) . B (k x n) on shared-memory operands addressed with (row, col) strides; thread
-// (ty, tx) of the 16 x 16 grid owns rows ty + 16 i and columns tx + 16 j (i, j < MT).
-__device__ __forceinline__ void mm_tile(double (&acc)[MT][MT], const double *A, int a_rs, int a_cs, const double *B, int b_rs,
-                                        int b_cs, int m, int n, int k, int ty, int tx) {
-    for (int kk = 0; kk < k; ++kk) {
-        double a[MT], b[MT];
-#pragma unroll
-        for (int i = 0; i < MT; ++i) {
-            const int r = ty + 16 * i;
-            a[i] = r < m ? A[r * a_rs + kk * a_cs] : 0.0;
-        }
-#pragma unroll
-        for (int j = 0; j < MT; ++j) {
-            const int c = tx + 16 * j;
-            b[j] = c < n ? B[kk * b_rs + c * b_cs] : 0.0;
-        }
-#pragma unroll
-        for (int i = 0; i < MT; ++i)
-#pragma unroll
-            for (int j = 0; j < MT; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-    }
-}
-
-__device__ __forceinline__ void zero_tile(double (&acc)[MT][MT]) {
-#pragma unroll
-    for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < MT; ++j) acc[i][j] = 0.0;
-}
-
-__global__ void __launch_bounds__(SYM_THREADS)
-transform_kernel(SymTables t, const double *__restrict__ Ys, const double *__restrict__ R1, const double *__restrict__ ups,
-                 int Jc, int j0, long long P, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo,
-                 void *r1_hi, void *r1_lo) {
-    extern __shared__ double sm[];
-    const int dmax = t.dmax;
-    double *Sb = sm;                   // d_b x d_b   S_j block b (row-major: S[p][mu])
-    double *Sc = Sb + dmax * dmax;     // d_c x d_c
-    double *Yt = Sc + dmax * dmax;     // d_b x d_c   Ys[b, c]
-    double *M1 = Yt + dmax * dmax;     // d_b x d_c   Ys[b, c] S_c
-    const int r = blockIdx.x, b = blockIdx.y;
-    const int k = r / Jc, j = j0 + r % Jc;
-    const int n = t.n;
-    const int sb = t.start[b], db = t.dim[b];
-    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
-    const double *Yk = Ys + (long long)k * n * n;
-    const double *Rk = R1 + (long long)k * n;
-    const double *Sbg = t.sym + t.off[b] + (long long)j * db * db;
-    for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = Sbg[e];
-    if (b == 0) {   // zero padding columns of this row
-        for (long long p = P + threadIdx.x; p < Kp; p += blockDim.x) store_split(fmt, B1_hi, B1_lo, (long long)r * Kp + p, 0.0);
-        for (long long m = n + threadIdx.x; m < np; m += blockDim.x) store_split(fmt, r1_hi, r1_lo, (long long)r * np + m, 0.0);
-    }
-    __syncthreads();
-    // r1 for the modes of block b:  (S_j^T R)_mu' = sum_p' S_b[p', mu'] R[sb + p']
-    for (int mu = threadIdx.x; mu < db; mu += blockDim.x) {
-        double acc = 0.0;
-        for (int p = 0; p < db; ++p) acc += Sb[p * db + mu] * Rk[sb + p];
-        store_split(fmt, r1_hi, r1_lo, (long long)r * np + sb + mu, ups[sb + mu] * acc);
-    }
-    for (int c = b; c < t.n_blocks; ++c) {
-        const int sc = t.start[c], dc = t.dim[c];
-        const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
-        __syncthreads();
-        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) Sc[e] = Scg[e];
-        for (int e = threadIdx.x; e < db * dc; e += blockDim.x) Yt[e] = Yk[(long long)(sb + e / dc) * n + sc + e % dc];
-        __syncthreads();
-        double acc[MT][MT];
-        zero_tile(acc);
-        mm_tile(acc, Yt, dc, 1, Sc, dc, 1, db, dc, dc, ty, tx);          // M1 = Ys[b,c] S_c
-#pragma unroll
-        for (int i = 0; i < MT; ++i)
-#pragma unroll
-            for (int jj = 0; jj < MT; ++jj) {
-                const int rr = ty + 16 * i, cc = tx + 16 * jj;
-                if (rr < db && cc < dc) M1[rr * dc + cc] = acc[i][jj];
-            }
-        __syncthreads();
-        zero_tile(acc);
-        mm_tile(acc, Sb, 1, db, M1, dc, 1, db, dc, db, ty, tx);          // S_b^T M1
-#pragma unroll
-        for (int i = 0; i < MT; ++i)
-#pragma unroll
-            for (int jj = 0; jj < MT; ++jj) {
-                const int mu = ty + 16 * i, nu = tx + 16 * jj;
-                const int gm = sb + mu, gn = sc + nu;
-                if (mu < db && nu < dc && gm <= gn)
-                    store_split(fmt, B1_hi, B1_lo, (long long)r * Kp + pair_index(gm, gn, n), acc[i][jj]);
-            }
-    }
-}
-
-// ------------------------------------------------------------------------------------------------
 // weights: from [a | b] (D1) and [c | d] (Dcd) build Cw = [delta/2 | gamma] and AB = [alpha | beta]
 // ------------------------------------------------------------------------------------------------
 template <typename AccT>
@@ -249,77 +140,6 @@ __global__ void weights_kernel(const AccT *__restrict__ D1, const AccT *__restri
             store_split(fmt, AB_hi, AB_lo, r * N2p + col, 0.0);
         }
     }
-}
-
-// ------------------------------------------------------------------------------------------------
-// fold: partial[k][f] (block b, c) = sum_{j in chunk f} S_j W_j S_j^T  (and f partials on diagonal pairs)
-//   W_j[mu,nu] = e ups_mu ups_nu Z[r, p(mu,nu)]
-// ------------------------------------------------------------------------------------------------
-template <typename AccT>
-__global__ void __launch_bounds__(SYM_THREADS)
-fold_kernel(SymTables t, const int *__restrict__ bp_b, const int *__restrict__ bp_c, const AccT *__restrict__ Z, long long ldz,
-            const AccT *__restrict__ F, long long ldf, const double *__restrict__ ups, int Jc, int j0, int nj, int Jf, int nf_total,
-            double *__restrict__ partD, double *__restrict__ partF) {
-    extern __shared__ double sm[];
-    const int dmax = t.dmax;
-    double *Sb = sm;                   // d_b x d_b  S_j block b, row-major S[mu][p]
-    double *ScT = Sb + dmax * dmax;    // d_c x d_c  transposed: ScT[q][nu] = S_c[nu][q]
-    double *Wt = ScT + dmax * dmax;    // d_b x d_c  W_j[b, c]
-    double *U = Wt + dmax * dmax;      // d_b x d_c  W_j[b, c] S_c^T
-    const int b = bp_b[blockIdx.x], c = bp_c[blockIdx.x];
-    const int fc = blockIdx.y, k = blockIdx.z;
-    const int n = t.n;
-    const int sb = t.start[b], db = t.dim[b], sc = t.start[c], dc = t.dim[c];
-    const int fg = j0 / Jf + fc;
-    const int ja = j0 + fc * Jf, jb = min(j0 + (fc + 1) * Jf, j0 + nj);
-    const int ne = db * dc;
-    const int ty = threadIdx.x >> 4, tx = threadIdx.x & 15;
-    double acc[MT][MT];
-    zero_tile(acc);
-    double facc = 0.0;   // f partial for mode sb + threadIdx.x (diagonal pairs only)
-    for (int j = ja; j < jb; ++j) {
-        const long long r = (long long)k * Jc + (j - j0);
-        const double *Sbg = t.sym + t.off[b] + (long long)j * db * db;
-        const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
-        __syncthreads();
-        for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = Sbg[e];
-        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) ScT[(e % dc) * dc + e / dc] = Scg[e];
-        for (int e = threadIdx.x; e < ne; e += blockDim.x) {
-            const int p = e / dc, q = e % dc;
-            int gm = sb + p, gn = sc + q;
-            if (gm > gn) { int s = gm; gm = gn; gn = s; }
-            const double z = (double)Z[r * ldz + pair_index(gm, gn, n)];
-            Wt[e] = (gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn] * z;
-        }
-        __syncthreads();
-        double u[MT][MT];
-        zero_tile(u);
-        mm_tile(u, Wt, dc, 1, ScT, dc, 1, db, dc, dc, ty, tx);        // U = W S_c^T
-#pragma unroll
-        for (int i = 0; i < MT; ++i)
-#pragma unroll
-            for (int jj = 0; jj < MT; ++jj) {
-                const int rr = ty + 16 * i, cc = tx + 16 * jj;
-                if (rr < db && cc < dc) U[rr * dc + cc] = u[i][jj];
-            }
-        if (b == c && threadIdx.x < db) {
-            const AccT *Fr = F + r * ldf + sb;
-            double s = 0.0;
-            for (int p = 0; p < db; ++p) s += Sb[threadIdx.x * db + p] * (double)Fr[p];
-            facc += s;
-        }
-        __syncthreads();
-        mm_tile(acc, Sb, db, 1, U, dc, 1, db, dc, db, ty, tx);        // acc += S_b U
-    }
-    double *out = partD + ((long long)k * nf_total + fg) * (long long)n * n;
-#pragma unroll
-    for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int jj = 0; jj < MT; ++jj) {
-            const int mu = ty + 16 * i, nu = tx + 16 * jj;
-            if (mu < db && nu < dc) out[(long long)(sb + mu) * n + sc + nu] = acc[i][jj];
-        }
-    if (b == c && threadIdx.x < db) partF[((long long)k * nf_total + fg) * n + sb + threadIdx.x] = facc;
 }
 
 __global__ void fold_reduce_kernel(const double *partD, const double *partF, int nf, int n, int nb,
@@ -504,6 +324,12 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
         set_error("ensemble set-up kernels failed");
         return fail(TDSCHA_ECUDA);
     }
+    {
+        size_t pcb = 0;
+        int prc = build_pair_classes(dim, e->pairs, &pcb);
+        if (prc) return fail(prc);
+        e->base_bytes += pcb;
+    }
     if (cublasCreate(&e->cublas) != CUBLAS_STATUS_SUCCESS) {
         set_error("cublasCreate failed");
         return fail(TDSCHA_ECUDA);
@@ -530,6 +356,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);
+    free_pair_classes(e->pairs);
     if (e->cublas) cublasDestroy(e->cublas);
     delete e;
     cudaSetDevice(prev);
@@ -657,11 +484,6 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     double *partF = reinterpret_cast<double *>(W + L.partF);
 
     SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax};
-    const size_t sm_tr = 4 * (size_t)e->dmax * e->dmax * sizeof(double);
-    const size_t sm_fold = 4 * (size_t)e->dmax * e->dmax * sizeof(double);
-    TD_CUDA(cudaFuncSetAttribute(transform_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_tr));
-    TD_CUDA(cudaFuncSetAttribute(fold_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fold));
-    TD_CUDA(cudaFuncSetAttribute(fold_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_fold));
 
     for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
         const int nj = std::min(Jc, e->N_sym - j0);
@@ -669,9 +491,8 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         // rows r = k * nj + jj
         {
             StageScope sc(e, ST_TRANSFORM, st);
-            transform_kernel<<<dim3((unsigned)M, e->n_blocks), SYM_THREADS, sm_tr, st>>>(
-                t, Ys, R1, e->ups, nj, j0, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
-            TD_CUDA(cudaGetLastError());
+            TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo,
+                                 fmt != FMT_F64, st));
         }
         // GEMM1: [a | b] = B1 . V^T      (M x 2N, K = Kp)
         {
@@ -709,16 +530,12 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         // fold this chunk into the partials
         {
             StageScope sc(e, ST_FOLD, st);
-            dim3 fg((unsigned)e->bp_b.size(), (unsigned)ceil_div(nj, Jf), (unsigned)nb);
             if (fmt == FMT_F64)
-                fold_kernel<double><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const double *)Z, L.ldz,
-                                                                       (const double *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total,
-                                                                       partD, partF);
+                TD_TRY(sym_fold<double>(t, e->pairs, nb, nj, j0, Jf, nf_total, (const double *)Z, L.ldz, (const double *)F, L.ldf,
+                                        e->ups, partD, partF, st));
             else
-                fold_kernel<float><<<fg, SYM_THREADS, sm_fold, st>>>(t, e->d_bp_b, e->d_bp_c, (const float *)Z, L.ldz,
-                                                                      (const float *)F, L.ldf, e->ups, nj, j0, nj, Jf, nf_total,
-                                                                      partD, partF);
-            TD_CUDA(cudaGetLastError());
+                TD_TRY(sym_fold<float>(t, e->pairs, nb, nj, j0, Jf, nf_total, (const float *)Z, L.ldz, (const float *)F, L.ldf,
+                                       e->ups, partD, partF, st));
         }
     }
     const double norm = 1.0 / (e->N_eff * (double)e->N_sym);

@@ -23,6 +23,7 @@
 #include <cublas_v2.h>
 #include <vector>
 #include "common.cuh"
+#include "symmetry.cuh"
 
 struct tdscha_ensemble;
 
@@ -82,6 +83,7 @@ struct tdscha_ensemble {
     cublasHandle_t cublas = nullptr;
     size_t base_bytes = 0;
     tdscha::Profile prof;
+    tdscha::PairClasses pairs;
 };
 
 namespace tdscha {

@@ -17,7 +17,9 @@
 // the caller's error word, drains its own TMA copies (bounded), frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
+#include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -26,7 +28,7 @@ namespace tdscha {
 namespace tc {
 
 constexpr int BM = 128;
-constexpr int NUM_THREADS = 192;
+constexpr int NUM_THREADS = 320;   // producer, MMA, 8 epilogue warps
 constexpr unsigned long long WAIT_BUDGET_NS = 4000000000ull;   // 4 s per wait
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -139,34 +141,46 @@ struct Cfg {
     static constexpr int K_ELEMS = TF32 ? 32 : 64;            // K per stage (128 B of K)
     static constexpr int UMMA_K = TF32 ? 8 : 16;              // K per instruction (32 B)
     static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-    static constexpr uint32_t TMEM_COLS = BN < 32 ? 32 : BN;
+    static constexpr uint32_t TMEM_COLS = 2 * BN;             // two accumulator buffers
+    static constexpr int EPI_WARPS = 8;                       // 2 warps per TMEM lane quadrant
+    static constexpr int EPI_COLS = BN / 2;                   // columns owned by one epilogue thread
 };
 
+// Persistent: CTA c processes tiles c, c + gridDim.x, ... (m fastest).  Each tile's K loop is split
+// into chunks of `drain` k-blocks; a chunk accumulates from zero in one of two TMEM buffers (the MMA
+// warp moves on to the other buffer) and the epilogue warps add it into round-to-nearest fp32
+// registers, which bounds the error of the tensor core's own fp32 accumulation to `drain` k-blocks.
 template <int BN, int STAGES, bool TF32, int NPROD>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
-               int M, int N, int K, float *__restrict__ D, long long ldd, unsigned *err) {
+               int M, int N, int K, int drain, float *__restrict__ D, long long ldd, unsigned *err) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem + STAGES * C::STAGE_BYTES);
-    // bars[0..S) full, bars[S..2S) empty, bars[2S] accumulator ready
-    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 1);
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 2);
+    // bars[0..S) full, [S..2S) empty, [2S, 2S+2) accumulator full, [2S+2, 2S+4) accumulator empty
+    uint64_t *acc_full = bars + 2 * STAGES;
+    uint64_t *acc_empty = bars + 2 * STAGES + 2;
+    volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 4);
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * BM;
-    const int n0 = blockIdx.x * BN;
     const int num_kb = K / C::K_ELEMS;
+    const int num_m = (M + BM - 1) / BM, num_n = (N + BN - 1) / BN;
+    const int num_tiles = num_m * num_n;
+    const int chunks_per_tile = (num_kb + drain - 1) / drain;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(smem_u32(&bars[s]), 1);
             mbar_init(smem_u32(&bars[STAGES + s]), 1);
         }
-        mbar_init(smem_u32(&bars[2 * STAGES]), 1);
+        for (int x = 0; x < 2; ++x) {
+            mbar_init(smem_u32(&acc_full[x]), 1);
+            mbar_init(smem_u32(&acc_empty[x]), C::EPI_WARPS);
+        }
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -180,86 +194,121 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem_base = *tmem_slot;
 
-    int issued = 0;   // stages handed to TMA by the producer (for the drain on abort)
+    long long issued = 0;   // k-blocks handed to TMA by the producer (for the drain on abort)
     if (warp == 0 && lane == 0) {
         // ---------------- TMA producer ----------------
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA_hi)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB_hi)) : "memory");
-        for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % STAGES;
-            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-            if (!mbar_wait(smem_u32(&bars[STAGES + s]), ph ^ 1u, abort_flag)) { *abort_flag = 1; break; }
-            uint8_t *st = smem + s * C::STAGE_BYTES;
-            const uint32_t full = smem_u32(&bars[s]);
-            mbar_expect_tx(full, C::STAGE_BYTES);
-            const int kc = kb * C::K_ELEMS;
-            tma_load_2d(smem_u32(st), &tmA_hi, kc, m0, full);
-            tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES), &tmB_hi, kc, n0, full);
-            if constexpr (NPROD == 3) {
-                tma_load_2d(smem_u32(st + C::A_BYTES), &tmA_lo, kc, m0, full);
-                tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES), &tmB_lo, kc, n0, full);
+        long long g = 0;
+        for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
+            const int m0 = (t % num_m) * BM, n0 = (t / num_m) * BN;
+            for (int kb = 0; kb < num_kb; ++kb, ++g) {
+                const int s = (int)(g % STAGES);
+                const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+                if (!mbar_wait(smem_u32(&bars[STAGES + s]), ph ^ 1u, abort_flag)) { *abort_flag = 1; break; }
+                uint8_t *st = smem + s * C::STAGE_BYTES;
+                const uint32_t full = smem_u32(&bars[s]);
+                mbar_expect_tx(full, C::STAGE_BYTES);
+                const int kc = kb * C::K_ELEMS;
+                tma_load_2d(smem_u32(st), &tmA_hi, kc, m0, full);
+                tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES), &tmB_hi, kc, n0, full);
+                if constexpr (NPROD == 3) {
+                    tma_load_2d(smem_u32(st + C::A_BYTES), &tmA_lo, kc, m0, full);
+                    tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES), &tmB_lo, kc, n0, full);
+                }
+                issued = g + 1;
             }
-            issued = kb + 1;
         }
     } else if (warp == 1 && lane == 0) {
         // ---------------- MMA issuer ----------------
         constexpr uint32_t idesc = make_idesc(TF32, BM, BN);
+        long long g = 0, ch = 0;
         bool ok = true;
-        for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % STAGES;
-            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-            if (!mbar_wait(smem_u32(&bars[s]), ph, abort_flag)) { ok = false; *abort_flag = 1; break; }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint8_t *st = smem + s * C::STAGE_BYTES;
-            const uint32_t a_hi = smem_u32(st);
-            const uint32_t b_hi = smem_u32(st + C::NOPS * C::A_BYTES);
+        for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+            for (int c = 0; c < chunks_per_tile && ok; ++c, ++ch) {
+                const int X = (int)(ch & 1);
+                const uint32_t use = (uint32_t)(ch >> 1);
+                if (!mbar_wait(smem_u32(&acc_empty[X]), (use & 1u) ^ 1u, abort_flag)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t dtm = tmem_base + (uint32_t)(X * BN);
+                const int kb_end = min(num_kb, (c + 1) * drain);
+                for (int kb = c * drain; kb < kb_end; ++kb, ++g) {
+                    const int s = (int)(g % STAGES);
+                    const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
+                    if (!mbar_wait(smem_u32(&bars[s]), ph, abort_flag)) { ok = false; break; }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    uint8_t *st = smem + s * C::STAGE_BYTES;
+                    const uint32_t a_hi = smem_u32(st);
+                    const uint32_t b_hi = smem_u32(st + C::NOPS * C::A_BYTES);
 #pragma unroll
-            for (int k = 0; k < C::K_ELEMS / C::UMMA_K; ++k) {
-                const uint32_t koff = k * 32;   // bytes inside the 128-byte swizzled row
-                const uint32_t acc = (kb > 0 || k > 0) ? 1u : 0u;
-                umma<TF32>(tmem_base, sw128_desc(a_hi + koff), sw128_desc(b_hi + koff), idesc, acc);
-                if constexpr (NPROD == 3) {
-                    const uint32_t a_lo = smem_u32(st + C::A_BYTES);
-                    const uint32_t b_lo = smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES);
-                    umma<TF32>(tmem_base, sw128_desc(a_hi + koff), sw128_desc(b_lo + koff), idesc, 1u);
-                    umma<TF32>(tmem_base, sw128_desc(a_lo + koff), sw128_desc(b_hi + koff), idesc, 1u);
-                }
-            }
-            umma_commit(smem_u32(&bars[STAGES + s]));   // slot s free once these MMAs retire
-        }
-        if (ok) umma_commit(smem_u32(&bars[2 * STAGES]));   // accumulator complete
-    } else if (warp >= 2) {
-        // ---------------- epilogue ----------------
-        const int q = warp & 3;              // TMEM lane quadrant this warp may access
-        const int row = q * 32 + lane;
-        const bool ready = mbar_wait(smem_u32(&bars[2 * STAGES]), 0u, abort_flag);
-        if (!ready) {
-            *abort_flag = 1;
-        } else {
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const long long grow = (long long)m0 + row;
-#pragma unroll 1
-            for (int c = 0; c < BN / 32; ++c) {
-                uint32_t r[32];
-                tmem_ld32(tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(c * 32), r);
-                if (grow < M) {
-                    float *drow = D + grow * ldd;
-                    const int cb = n0 + c * 32;
-                    if (cb + 32 <= N && ((ldd & 3) == 0)) {
-#pragma unroll
-                        for (int v = 0; v < 8; ++v) {
-                            float4 f4 = make_float4(__uint_as_float(r[4 * v]), __uint_as_float(r[4 * v + 1]),
-                                                    __uint_as_float(r[4 * v + 2]), __uint_as_float(r[4 * v + 3]));
-                            *reinterpret_cast<float4 *>(drow + cb + 4 * v) = f4;
+                    for (int k = 0; k < C::K_ELEMS / C::UMMA_K; ++k) {
+                        const uint32_t koff = k * 32;   // bytes inside the 128-byte swizzled row
+                        const uint32_t acc = (kb > c * drain || k > 0) ? 1u : 0u;
+                        umma<TF32>(dtm, sw128_desc(a_hi + koff), sw128_desc(b_hi + koff), idesc, acc);
+                        if constexpr (NPROD == 3) {
+                            const uint32_t a_lo = smem_u32(st + C::A_BYTES);
+                            const uint32_t b_lo = smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES);
+                            umma<TF32>(dtm, sw128_desc(a_hi + koff), sw128_desc(b_lo + koff), idesc, 1u);
+                            umma<TF32>(dtm, sw128_desc(a_lo + koff), sw128_desc(b_hi + koff), idesc, 1u);
                         }
+                    }
+                    umma_commit(smem_u32(&bars[STAGES + s]));   // slot s free once these MMAs retire
+                }
+                if (!ok) break;
+                umma_commit(smem_u32(&acc_full[X]));             // chunk accumulated in buffer X
+            }
+        }
+        if (!ok) *abort_flag = 1;
+    } else if (warp >= 2) {
+        // ---------------- epilogue: drain chunks into fp32 registers, store each tile ----------------
+        const int ew = warp - 2;
+        const int q = warp & 3;              // TMEM lane quadrant this warp may access
+        const int half = ew >> 2;            // which half of the BN columns this warp owns
+        const int row = q * 32 + lane;
+        long long ch = 0;
+        bool ok = true;
+        for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+            const int m0 = (t % num_m) * BM, n0 = (t / num_m) * BN;
+            float acc[C::EPI_COLS];
+#pragma unroll
+            for (int i = 0; i < C::EPI_COLS; ++i) acc[i] = 0.f;
+            for (int c = 0; c < chunks_per_tile; ++c, ++ch) {
+                const int X = (int)(ch & 1);
+                const uint32_t use = (uint32_t)(ch >> 1);
+                if (!mbar_wait(smem_u32(&acc_full[X]), use & 1u, abort_flag)) { ok = false; break; }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(X * BN + half * C::EPI_COLS);
+#pragma unroll
+                for (int sub = 0; sub < C::EPI_COLS / 32; ++sub) {
+                    uint32_t r[32];
+                    tmem_ld32(tbase + (uint32_t)(sub * 32), r);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) acc[sub * 32 + i] += __uint_as_float(r[i]);
+                }
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[X])) : "memory");
+            }
+            if (!ok) break;
+            const long long grow = (long long)m0 + row;
+            if (grow < M) {
+                float *drow = D + grow * ldd;
+                const int cb0 = n0 + half * C::EPI_COLS;
+#pragma unroll
+                for (int v = 0; v < C::EPI_COLS / 4; ++v) {
+                    const int cb = cb0 + 4 * v;
+                    if (cb + 4 <= N && ((ldd & 3) == 0)) {
+                        *reinterpret_cast<float4 *>(drow + cb) =
+                            make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
                     } else {
 #pragma unroll
-                        for (int v = 0; v < 32; ++v)
-                            if (cb + v < N) drow[cb + v] = __uint_as_float(r[v]);
+                        for (int e = 0; e < 4; ++e)
+                            if (cb + e < N) drow[cb + e] = acc[4 * v + e];
                     }
                 }
             }
         }
+        if (!ok) *abort_flag = 1;
     }
 
     // ---------------- teardown ----------------
@@ -270,8 +319,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         if (warp == 0 && lane == 0) {
             // drain the TMA copies this CTA still has in flight (bounded)
             volatile int never = 0;
-            for (int kb = (issued > STAGES ? issued - STAGES : 0); kb < issued; ++kb)
-                mbar_wait(smem_u32(&bars[kb % STAGES]), (uint32_t)(kb / STAGES) & 1u, &never);
+            for (long long g = (issued > STAGES ? issued - STAGES : 0); g < issued; ++g)
+                mbar_wait(smem_u32(&bars[g % STAGES]), (uint32_t)(g / STAGES) & 1u, &never);
         }
         __syncthreads();
     }
@@ -319,6 +368,16 @@ static int make_map(CUtensorMap *map, const void *base, bool tf32, long long row
     return 0;
 }
 
+// k-blocks accumulated in TMEM before the epilogue drains them (TDSCHA_DRAIN_KB overrides; tuning knob)
+static int default_drain() {
+    static int d = -1;
+    if (d < 0) {
+        const char *env = getenv("TDSCHA_DRAIN_KB");
+        d = env ? std::max(1, atoi(env)) : 4;
+    }
+    return d;
+}
+
 template <int BN, int STAGES, bool TF32, int NPROD>
 static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
@@ -334,8 +393,14 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     }
     auto kern = tc_gemm_kernel<BN, STAGES, TF32, NPROD>;
     TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
-    dim3 grid(ceil_div(N, BN), ceil_div(M, BM));
-    kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, D, ldd, err);
+    int dev = 0, sms = 148;
+    TD_CUDA(cudaGetDevice(&dev));
+    TD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long tiles = (long long)ceil_div(M, BM) * ceil_div(N, BN);
+    const int num_kb = K / C::K_ELEMS;
+    const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(), num_kb);
+    dim3 grid((unsigned)std::min<long long>(tiles, sms));
+    kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, D, ldd, err);
     TD_CUDA(cudaGetLastError());
     return 0;
 }

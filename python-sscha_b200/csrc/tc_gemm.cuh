@@ -16,6 +16,7 @@ struct GemmOperands {
     long long lda;   // elements; lda * element size must be a multiple of 16 bytes
     const void *B_hi, *B_lo;
     long long ldb;
+    int drain_kb = 0;   // k-blocks per TMEM chunk drained to fp32 registers (0 = library default)
 };
 
 // K must be a multiple of 64 (bf16) or 32 (tf32); operands must be readable up to K columns.

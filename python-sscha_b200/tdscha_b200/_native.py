@@ -66,9 +66,11 @@ def load():
                                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp]
     lib.tdscha_tc_contract.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_longlong,
                                        vp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, vp]
+    lib.tdscha_apply_prologue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp]
+    lib.tdscha_apply_epilogue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp, vp]
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
-    for name in ("tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    for name in ("tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -166,6 +168,20 @@ class DeviceEnsemble:
         tr = np.ascontiguousarray(np.asarray(transpose, dtype=np.intc).reshape(nb))
         check(self._lib.tdscha_apply_full_L_device(self.handle, nb, psi.data_ptr(), _i(tr), ctypes.byref(opts),
                                                    PREC[precision], out.data_ptr(), _stream_ptr(stream)))
+
+
+    def apply_prologue(self, psi, R_out, Y_out, transpose, opts, stream=None):
+        nb = psi.shape[0]
+        tr = np.ascontiguousarray(np.asarray(transpose, dtype=np.intc).reshape(nb))
+        check(self._lib.tdscha_apply_prologue_device(self.handle, nb, psi.data_ptr(), _i(tr), ctypes.byref(opts),
+                                                     R_out.data_ptr(), Y_out.data_ptr(), _stream_ptr(stream)))
+
+    def apply_epilogue(self, psi, f_av, d_av, out, transpose, opts, stream=None):
+        nb = psi.shape[0]
+        tr = np.ascontiguousarray(np.asarray(transpose, dtype=np.intc).reshape(nb))
+        check(self._lib.tdscha_apply_epilogue_device(self.handle, nb, psi.data_ptr(), _i(tr), ctypes.byref(opts),
+                                                     f_av.data_ptr(), d_av.data_ptr(), out.data_ptr(),
+                                                     _stream_ptr(stream)))
 
 
 def _stream_ptr(stream):
