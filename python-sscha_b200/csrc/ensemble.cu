@@ -531,11 +531,11 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         {
             StageScope sc(e, ST_FOLD, st);
             if (fmt == FMT_F64)
-                TD_TRY(sym_fold<double>(t, e->pairs, nb, nj, j0, Jf, nf_total, (const double *)Z, L.ldz, (const double *)F, L.ldf,
-                                        e->ups, partD, partF, st));
+                TD_TRY(sym_fold<double>(t, e->pairs, e->d_blocks_ids, nb, nj, j0, Jf, nf_total, (const double *)Z, L.ldz,
+                                        (const double *)F, L.ldf, e->ups, partD, partF, false, st));
             else
-                TD_TRY(sym_fold<float>(t, e->pairs, nb, nj, j0, Jf, nf_total, (const float *)Z, L.ldz, (const float *)F, L.ldf,
-                                       e->ups, partD, partF, st));
+                TD_TRY(sym_fold<float>(t, e->pairs, e->d_blocks_ids, nb, nj, j0, Jf, nf_total, (const float *)Z, L.ldz,
+                                       (const float *)F, L.ldf, e->ups, partD, partF, true, st));
         }
     }
     const double norm = 1.0 / (e->N_eff * (double)e->N_sym);

@@ -117,18 +117,19 @@ __global__ void pad_kernel(long long M, long long P, long long Kp, int n, long l
 }
 
 // ---- fold ------------------------------------------------------------------------------------------
-// grid (pairs of the class, fold chunks of Jf symmetries, nb); FP64 products and accumulation.
-template <typename AccT, int MT>
-__global__ void __launch_bounds__(SYM_THREADS)
+// grid (pairs of the class, fold chunks of Jf symmetries, nb).  The two block products of one
+// symmetry run in the compute type T over <= d terms; their result is summed over symmetries in FP64.
+template <typename T, typename AccT, int MT>
+__global__ void __launch_bounds__(SYM_THREADS, 2)
 fold_kernel(SymTables t, const int *__restrict__ pb, const int *__restrict__ pc, const AccT *__restrict__ Z, long long ldz,
             const AccT *__restrict__ F, long long ldf, const double *__restrict__ ups, int nj, int j0, int Jf, int nf_total,
             double *__restrict__ partD, double *__restrict__ partF) {
     constexpr int DM = 16 * MT;
     extern __shared__ __align__(16) unsigned char sm_raw[];
-    double *Sb = reinterpret_cast<double *>(sm_raw);   // d_b x d_b  S_j block b, row-major S[mu][p]
-    double *ScT = Sb + DM * DM;                          // d_c x d_c  transposed: ScT[q][nu] = S_c[nu][q]
-    double *Wt = ScT + DM * DM;                          // d_b x d_c  W_j[b, c]
-    double *U = Wt + DM * DM;                            // d_b x d_c  W_j[b, c] S_c^T
+    T *Sb = reinterpret_cast<T *>(sm_raw);   // d_b x d_b  S_j block b, row-major S[mu][p]
+    T *ScT = Sb + DM * DM;                   // d_c x d_c  transposed: ScT[q][nu] = S_c[nu][q]
+    T *Wt = ScT + DM * DM;                   // d_b x d_c  W_j[b, c]
+    T *U = Wt + DM * DM;                     // d_b x d_c  W_j[b, c] S_c^T
     const int b = pb[blockIdx.x], c = pc[blockIdx.x];
     const int fc = blockIdx.y, k = blockIdx.z;
     const int n = t.n;
@@ -144,19 +145,19 @@ fold_kernel(SymTables t, const int *__restrict__ pb, const int *__restrict__ pc,
         const double *Sbg = t.sym + t.off[b] + (long long)j * db * db;
         const double *Scg = t.sym + t.off[c] + (long long)j * dc * dc;
         __syncthreads();
-        for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = Sbg[e];
-        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) ScT[(e % dc) * dc + e / dc] = Scg[e];
+        for (int e = threadIdx.x; e < db * db; e += blockDim.x) Sb[e] = (T)Sbg[e];
+        for (int e = threadIdx.x; e < dc * dc; e += blockDim.x) ScT[(e % dc) * dc + e / dc] = (T)Scg[e];
         for (int e = threadIdx.x; e < db * dc; e += blockDim.x) {
             const int p = e / dc, q = e % dc;
             int gm = sb + p, gn = sc + q;
             if (gm > gn) { const int s = gm; gm = gn; gn = s; }
             const double z = (double)Z[r * ldz + sym_pair_index(gm, gn, n)];
-            Wt[e] = (gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn] * z;
+            Wt[e] = (T)((gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn] * z);
         }
         __syncthreads();
-        double u[MT][MT];
+        T u[MT][MT];
         zero_tile(u);
-        mm_tile(u, Wt, dc, 1, ScT, dc, 1, db, dc, dc, ty, tx);        // U = W S_c^T
+        mm_tile(u, Wt, dc, 1, ScT, dc, 1, db, dc, dc, ty, tx);        // U = W S_c^T (<= d_c terms)
 #pragma unroll
         for (int i = 0; i < MT; ++i)
 #pragma unroll
@@ -167,11 +168,16 @@ fold_kernel(SymTables t, const int *__restrict__ pb, const int *__restrict__ pc,
         if (b == c && threadIdx.x < db) {
             const AccT *Fr = F + r * ldf + sb;
             double s = 0.0;
-            for (int p = 0; p < db; ++p) s += Sb[threadIdx.x * db + p] * (double)Fr[p];
+            for (int p = 0; p < db; ++p) s += (double)Sb[threadIdx.x * db + p] * (double)Fr[p];
             facc += s;
         }
         __syncthreads();
-        mm_tile(acc, Sb, db, 1, U, dc, 1, db, dc, db, ty, tx);        // acc += S_b U
+        zero_tile(u);
+        mm_tile(u, Sb, db, 1, U, dc, 1, db, dc, db, ty, tx);          // S_b U (<= d_b terms) ...
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+            for (int jj = 0; jj < MT; ++jj) acc[i][jj] += (double)u[i][jj];   // ... then summed over j in FP64
     }
     double *out = partD + ((long long)k * nf_total + fg) * (long long)n * n;
 #pragma unroll
@@ -258,12 +264,12 @@ int sym_transform(const SymTables &t, const PairClasses &pc, int nb, int nj, int
     return transform_all<double>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st);
 }
 
-template <typename AccT, int MT>
+template <typename T, typename AccT, int MT>
 static int launch_fold(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, int Jf, int nf_total, const AccT *Z,
                        long long ldz, const AccT *F, long long ldf, const double *ups, double *partD, double *partF, cudaStream_t st) {
     if (!pc.count[MT]) return 0;
-    const size_t smem = 4 * (size_t)(16 * MT) * (16 * MT) * sizeof(double);
-    auto kern = fold_kernel<AccT, MT>;
+    const size_t smem = 4 * (size_t)(16 * MT) * (16 * MT) * sizeof(T);
+    auto kern = fold_kernel<T, AccT, MT>;
     TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, Jf), (unsigned)nb);
     kern<<<grid, SYM_THREADS, smem, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
@@ -271,20 +277,29 @@ static int launch_fold(const SymTables &t, const PairClasses &pc, int nb, int nj
     return 0;
 }
 
-template <typename AccT>
-int sym_fold(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, int Jf, int nf_total, const AccT *Z, long long ldz,
-             const AccT *F, long long ldf, const double *ups, double *partD, double *partF, cudaStream_t st) {
-    TD_TRY((launch_fold<AccT, 1>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
-    TD_TRY((launch_fold<AccT, 2>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
-    TD_TRY((launch_fold<AccT, 3>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
-    TD_TRY((launch_fold<AccT, 4>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
-    TD_TRY((launch_fold<AccT, 5>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
+template <typename T, typename AccT>
+static int fold_all(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, int Jf, int nf_total, const AccT *Z,
+                    long long ldz, const AccT *F, long long ldf, const double *ups, double *partD, double *partF, cudaStream_t st) {
+    TD_TRY((launch_fold<T, AccT, 1>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
+    TD_TRY((launch_fold<T, AccT, 2>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
+    TD_TRY((launch_fold<T, AccT, 3>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
+    TD_TRY((launch_fold<T, AccT, 4>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
+    TD_TRY((launch_fold<T, AccT, 5>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st)));
     return 0;
 }
 
-template int sym_fold<float>(const SymTables &, const PairClasses &, int, int, int, int, int, const float *, long long,
-                             const float *, long long, const double *, double *, double *, cudaStream_t);
-template int sym_fold<double>(const SymTables &, const PairClasses &, int, int, int, int, int, const double *, long long,
-                              const double *, long long, const double *, double *, double *, cudaStream_t);
+template <typename AccT>
+int sym_fold(const SymTables &t, const PairClasses &pc, const int *blocks_ids, int nb, int nj, int j0, int Jf, int nf_total,
+             const AccT *Z, long long ldz, const AccT *F, long long ldf, const double *ups, double *partD, double *partF,
+             bool fp32_compute, cudaStream_t st) {
+    (void)blocks_ids;
+    if (fp32_compute) return fold_all<float, AccT>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);
+    return fold_all<double, AccT>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);
+}
+
+template int sym_fold<float>(const SymTables &, const PairClasses &, const int *, int, int, int, int, int, const float *, long long,
+                             const float *, long long, const double *, double *, double *, bool, cudaStream_t);
+template int sym_fold<double>(const SymTables &, const PairClasses &, const int *, int, int, int, int, int, const double *,
+                              long long, const double *, long long, const double *, double *, double *, bool, cudaStream_t);
 
 }  // namespace tdscha

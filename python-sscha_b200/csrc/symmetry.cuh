@@ -40,9 +40,11 @@ int sym_transform(const SymTables &t, const PairClasses &pc, int nb, int nj, int
                   const double *ups, long long P, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo,
                   void *r1_hi, void *r1_lo, bool fp32_compute, cudaStream_t st);
 
-// Z (rows r as above, packed pairs, ldz), F (rows r, ldf); partials per (k, fold chunk fg)
+// Z (rows r as above, packed pairs, ldz), F (rows r, ldf); partials per (k, fold chunk fg).  The
+// per-symmetry block products run in FP32 when fp32_compute and are summed over symmetries in FP64.
 template <typename AccT>
-int sym_fold(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, int Jf, int nf_total, const AccT *Z, long long ldz,
-             const AccT *F, long long ldf, const double *ups, double *partD, double *partF, cudaStream_t st);
+int sym_fold(const SymTables &t, const PairClasses &pc, const int *blocks_ids, int nb, int nj, int j0, int Jf, int nf_total,
+             const AccT *Z, long long ldz, const AccT *F, long long ldf, const double *ups, double *partD, double *partF,
+             bool fp32_compute, cudaStream_t st);
 
 }  // namespace tdscha

@@ -368,14 +368,17 @@ static int make_map(CUtensorMap *map, const void *base, bool tf32, long long row
     return 0;
 }
 
-// k-blocks accumulated in TMEM before the epilogue drains them (TDSCHA_DRAIN_KB overrides; tuning knob)
-static int default_drain() {
-    static int d = -1;
-    if (d < 0) {
+// k-blocks accumulated in TMEM before the epilogue drains them.  Split modes drain every k-block:
+// their error is otherwise dominated by the tensor core's own fp32 accumulation; single-product
+// modes are limited by operand rounding and drain every 16.  TDSCHA_DRAIN_KB overrides (tuning).
+static int default_drain(int nprod) {
+    static int env_d = -2;
+    if (env_d == -2) {
         const char *env = getenv("TDSCHA_DRAIN_KB");
-        d = env ? std::max(1, atoi(env)) : 4;
+        env_d = env ? std::max(1, atoi(env)) : -1;
     }
-    return d;
+    if (env_d > 0) return env_d;
+    return nprod == 3 ? 1 : 16;
 }
 
 template <int BN, int STAGES, bool TF32, int NPROD>
@@ -398,7 +401,7 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     TD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const long long tiles = (long long)ceil_div(M, BM) * ceil_div(N, BN);
     const int num_kb = K / C::K_ELEMS;
-    const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(), num_kb);
+    const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(NPROD), num_kb);
     dim3 grid((unsigned)std::min<long long>(tiles, sms));
     kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, D, ldd, err);
     TD_CUDA(cudaGetLastError());
