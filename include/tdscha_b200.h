@@ -150,6 +150,27 @@ int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const do
                                double *q_next, double *p_next, double *sc_out, void *stream);
 
 /*
+ * tdscha_lanczos_step_device with no device allocation at all.  There is no counterpart in the
+ * reference.  It is meant for host programs that cannot call cudaMalloc while they drive the
+ * recurrence: applications that hand out all device memory from their own fixed arena, code that
+ * must not add an implicit device synchronisation (cudaMalloc/cudaFree synchronise), and real-time
+ * or embedded runners with a fixed memory budget.  The step's reduction partials live instead in a
+ * fixed array inside this library (4 doubles per chain per reduction block, 303 KB), which every GPU
+ * that loads the library holds until the process exits.
+ *   - nc must be at most 32; larger requests fail with TDSCHA_EINVAL and a message.
+ *   - Runs on the current device.  The first call on each device looks up the array's device
+ *     address (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array: calls that overlap on the GPU (e.g. on different streams)
+ *     race and give wrong results.  Each call writes every partial it reads, so no clearing is
+ *     needed between calls.
+ *   - Arguments, outputs and errors are those of tdscha_lanczos_step_device.
+ */
+int tdscha_lanczos_step_device_noalloc(int nc, long long len, const double *Lq, const double *pL,
+                                       const double *q, const double *p, const double *q_prev,
+                                       const double *p_prev, const double *sc_in, const double *mask,
+                                       double *q_next, double *p_next, double *sc_out, void *stream);
+
+/*
  * Continued-fraction Green function (DynamicalLanczos.py:4951-5047) on the device.
  * a (n_iter), b (n_iter-1 or more), c (same as b or NULL = symmetric) FP64 device arrays;
  * omega (n_w) device; gf_out (2 * n_w) interleaved re, im.

@@ -11,6 +11,7 @@
 //   get_green_function_continued_fraction :4951-5047
 #include <cmath>
 #include <cuComplex.h>
+#include <mutex>
 
 #include "common.cuh"
 #include "ensemble.cuh"
@@ -351,6 +352,54 @@ int lanczos_step_device(int nc, long long len, const double *Lq, const double *p
 }
 
 size_t lanczos_scratch_bytes(int nc) { return (size_t)nc * LZ_BLOCKS * 4 * sizeof(double); }
+
+// ---- Lanczos step without any allocation ---------------------------------------------------------
+// The step's only temporaries are its per-block reduction partials (4 doubles per chain and block).
+// For callers that cannot allocate device memory, they live in this fixed file-scope array, which
+// every GPU that loads the library holds until the process exits.
+constexpr int LZ_NOALLOC_MAX_CHAINS = 32;
+static __device__ __align__(256) double g_lz_noalloc_scratch[(size_t)LZ_NOALLOC_MAX_CHAINS * LZ_BLOCKS * 4];
+
+// Device address of the array on each device, looked up once (with that device current).
+static std::mutex g_noalloc_mutex;
+static void *g_noalloc_addr[128] = {nullptr};
+
+static int noalloc_scratch_address(double **out) {
+    int dev = 0;
+    TD_CUDA(cudaGetDevice(&dev));
+    TD_CHECK(dev >= 0 && dev < 128, TDSCHA_EINVAL, "device index %d out of range", dev);
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_addr[dev]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_lz_noalloc_scratch);
+        TD_CHECK(e == cudaSuccess && p != nullptr, TDSCHA_ECUDA, "cudaGetSymbolAddress of the Lanczos scratch failed: %s",
+                 cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = static_cast<double *>(g_noalloc_addr[dev]);
+    return 0;
+}
+
+}  // namespace tdscha
+
+extern "C" int tdscha_lanczos_step_device_noalloc(int nc, long long len, const double *Lq, const double *pL,
+                                                  const double *q, const double *p, const double *q_prev,
+                                                  const double *p_prev, const double *sc_in, const double *mask,
+                                                  double *q_next, double *p_next, double *sc_out, void *stream) {
+    using namespace tdscha;
+    clear_error();
+    TD_CHECK(nc > 0 && nc <= LZ_NOALLOC_MAX_CHAINS, TDSCHA_EINVAL,
+             "tdscha_lanczos_step_device_noalloc: %d chains requested, its fixed scratch holds at most %d", nc,
+             LZ_NOALLOC_MAX_CHAINS);
+    double *scratch = nullptr;
+    TD_TRY(noalloc_scratch_address(&scratch));
+    // every partial the kernels read is written earlier in the same call: nothing needs clearing
+    return lanczos_step_device(nc, len, Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_out,
+                               static_cast<cudaStream_t>(stream), scratch,
+                               (size_t)LZ_NOALLOC_MAX_CHAINS * LZ_BLOCKS * 4 * sizeof(double));
+}
+
+namespace tdscha {
 
 // ---- continued fraction -------------------------------------------------------------------------
 struct CFParams {

@@ -61,6 +61,7 @@ def load():
     lib.tdscha_apply_full_L_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), ctypes.c_int, vp, vp]
     lib.tdscha_lanczos_step_device.argtypes = [ctypes.c_int, ctypes.c_longlong, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
                                                vp, vp]
+    lib.tdscha_lanczos_step_device_noalloc.argtypes = list(lib.tdscha_lanczos_step_device.argtypes)
     lib.tdscha_continued_fraction_device.argtypes = [ctypes.c_int, vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                                      vp, ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
                                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp]
@@ -70,7 +71,7 @@ def load():
     lib.tdscha_apply_epilogue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp, vp]
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
-    for name in ("tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    for name in ("tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -198,6 +199,16 @@ def lanczos_step(Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_o
     check(lib.tdscha_lanczos_step_device(nc, length, ptr(Lq), ptr(pL), ptr(q), ptr(p), ptr(q_prev), ptr(p_prev),
                                          ptr(sc_in), ptr(mask), ptr(q_next), ptr(p_next), ptr(sc_out),
                                          _stream_ptr(stream)))
+
+
+def lanczos_step_noalloc(Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_out, stream=None):
+    """Same step through tdscha_lanczos_step_device_noalloc (fixed in-library scratch, <= 32 chains)."""
+    lib = load()
+    nc, length = Lq.shape
+    ptr = lambda t: None if t is None else t.data_ptr()   # noqa: E731
+    check(lib.tdscha_lanczos_step_device_noalloc(nc, length, ptr(Lq), ptr(pL), ptr(q), ptr(p), ptr(q_prev),
+                                                 ptr(p_prev), ptr(sc_in), ptr(mask), ptr(q_next), ptr(p_next),
+                                                 ptr(sc_out), _stream_ptr(stream)))
 
 
 def continued_fraction(a, b, c, omega, gf_out, use_terminator, last_average, smearing, use_wigner, reverse_L,
