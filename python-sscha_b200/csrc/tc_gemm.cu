@@ -20,6 +20,9 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -132,6 +135,18 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Tile order of the persistent schedule: groups of `gm` M-tiles, N-tiles of a group in turn, M
+// fastest inside a group.  The ~148 tiles in flight then form a gm x (148/gm) block that shares its
+// A rows and B rows through L2, instead of one N column of tiles streaming all of A from HBM.
+__device__ __forceinline__ void tile_coords(int t, int num_m, int num_n, int gm, int &m_blk, int &n_blk) {
+    const int per_group = gm * num_n;
+    const int g = t / per_group, rem = t % per_group;
+    const int m_first = g * gm;
+    const int rows = min(gm, num_m - m_first);
+    n_blk = rem / rows;
+    m_blk = m_first + rem % rows;
+}
+
 template <int BN, int STAGES, bool TF32, int NPROD>
 struct Cfg {
     static constexpr int A_BYTES = BM * 128;                 // one 128 x (128 B) tile
@@ -154,7 +169,7 @@ template <int BN, int STAGES, bool TF32, int NPROD>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
-               int M, int N, int K, int drain, float *__restrict__ D, long long ldd, unsigned *err) {
+               int M, int N, int K, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -201,7 +216,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB_hi)) : "memory");
         long long g = 0;
         for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
-            const int m0 = (t % num_m) * BM, n0 = (t / num_m) * BN;
+            int mb, nbk;
+            tile_coords(t, num_m, num_n, group_m, mb, nbk);
+            const int m0 = mb * BM, n0 = nbk * BN;
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
                 const int s = (int)(g % STAGES);
                 const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
@@ -268,7 +285,9 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         long long ch = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
-            const int m0 = (t % num_m) * BM, n0 = (t / num_m) * BN;
+            int mb, nbk;
+            tile_coords(t, num_m, num_n, group_m, mb, nbk);
+            const int m0 = mb * BM, n0 = nbk * BN;
             float acc[C::EPI_COLS];
 #pragma unroll
             for (int i = 0; i < C::EPI_COLS; ++i) acc[i] = 0.f;
@@ -381,6 +400,67 @@ static int default_drain(int nprod) {
     return nprod == 3 ? 1 : 16;
 }
 
+// ---- tile-order autotuner -------------------------------------------------------------------------
+// The best tile-group size depends on the problem shape (the two L2 halves of the part make it hard
+// to predict), so on the first call for a (format, products, M, N, K) the launcher times a few
+// candidates on the caller's stream (fastest of two runs each; every run writes the same D) and
+// remembers the winner.  Small problems, or TDSCHA_AUTOTUNE=0, use the m-fastest order.
+struct TuneKey {
+    int tf32, nprod, M, N, K, dev;
+    bool operator<(const TuneKey &o) const {
+        return std::tie(tf32, nprod, M, N, K, dev) < std::tie(o.tf32, o.nprod, o.M, o.N, o.K, o.dev);
+    }
+};
+static std::mutex g_tune_mutex;
+static std::map<TuneKey, int> g_tune;
+
+template <typename Launch>
+static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long long tiles, int sms, cudaStream_t st,
+                       Launch &launch, int *gm_out) {
+    int dev = 0;
+    TD_CUDA(cudaGetDevice(&dev));
+    const TuneKey key{tf32, nprod, M, N, K, dev};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) { *gm_out = it->second; return 0; }
+    }
+    const char *env = getenv("TDSCHA_AUTOTUNE");
+    const bool enabled = !(env && atoi(env) == 0);
+    int best = num_m;
+    if (enabled && tiles >= 8LL * sms) {
+        const int cand_all[] = {num_m, 48, 24, 13, 6};
+        cudaEvent_t e0, e1;
+        TD_CUDA(cudaEventCreate(&e0));
+        TD_CUDA(cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        for (int ci = 0; ci < 5; ++ci) {
+            const int cand = cand_all[ci];
+            bool dup = cand > num_m;
+            for (int cj = 0; cj < ci; ++cj) dup = dup || cand_all[cj] == cand;
+            if (dup) continue;
+            float t_min = 1e30f;
+            for (int rep = 0; rep < 2; ++rep) {
+                TD_CUDA(cudaEventRecord(e0, st));
+                launch(cand);
+                TD_CUDA(cudaGetLastError());
+                TD_CUDA(cudaEventRecord(e1, st));
+                TD_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                TD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                t_min = std::min(t_min, ms);
+            }
+            if (t_min < best_ms) { best_ms = t_min; best = cand; }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune[key] = best;
+    *gm_out = best;
+    return 0;
+}
+
 template <int BN, int STAGES, bool TF32, int NPROD>
 static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
@@ -403,7 +483,17 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     const int num_kb = K / C::K_ELEMS;
     const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(NPROD), num_kb);
     dim3 grid((unsigned)std::min<long long>(tiles, sms));
-    kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, D, ldd, err);
+    const int num_m = ceil_div(M, BM);
+    auto launch = [&](int gm) {
+        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err);
+    };
+    if (const char *env = getenv("TDSCHA_GROUP_M")) {   // tuning knob: fixed tile-group size
+        launch(std::max(1, std::min(num_m, atoi(env))));
+    } else {
+        int gm = 0;
+        TD_TRY(tuned_group(TF32 ? 1 : 0, NPROD, M, N, K, num_m, tiles, sms, st, launch, &gm));
+        launch(gm);
+    }
     TD_CUDA(cudaGetLastError());
     return 0;
 }
