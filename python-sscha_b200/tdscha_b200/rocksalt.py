@@ -289,3 +289,39 @@ def make_ensemble(L, N, T=300.0, seed=0, k2=2.0, k3=-3.0, k4=6.0, with_symmetrie
                              symmetries=s.symmetries, deg_space=s.deg_space, blocks_ids=s.blocks_ids,
                              supercell=(L, L, L), nat_uc=2, effective_charges=random_born_charges(seed=seed),
                              raman_tensor=random_raman_tensor(seed=seed), system=s)
+
+
+# ------------------------------------------------------------------------------------------------
+# The seeded chain of the precision check: one bi-conjugate chain from a seeded random unit vector
+# on R^(1), G(w) on 500 points 0-400 cm^-1 with 5 cm^-1 smearing and no terminator.
+# ------------------------------------------------------------------------------------------------
+CHAIN_SEED = 11
+RY_TO_CM = 109737.31568160
+
+
+def gf_grid():
+    """(omega in Ry, smearing in Ry) of the precision check."""
+    return np.linspace(0.0, 400.0, 500) / RY_TO_CM, 5.0 / RY_TO_CM
+
+
+def seeded_chain(system, X, Y, rho, device_ensemble, precision, steps, seed=CHAIN_SEED):
+    """Run `steps` bi-conjugate steps of the seeded chain on `device_ensemble` in `precision`;
+    returns the Lanczos object (a/b/c coefficients filled)."""
+    from .DynamicalLanczos import Lanczos, run_FT_batched
+    s = system
+    eo = SyntheticEnsemble(T=s.T, nat=s.nat, m=s.masses, w=s.w, pols=s.pols, N=X.shape[0], rho=rho, X=X, Y=Y,
+                           symmetries=s.symmetries, deg_space=s.deg_space, blocks_ids=s.blocks_ids,
+                           supercell=(round((s.nat // 2) ** (1 / 3)),) * 3)
+    lanc = Lanczos(eo, precision=precision)
+    lanc.symmetries, lanc.degenerate_space, lanc.sym_block_id = s.symmetries, s.deg_space, s.blocks_ids
+    lanc.N_degeneracy = np.array([len(d) for d in s.deg_space], dtype=np.intc)
+    lanc.n_syms, lanc.initialized, lanc.device_ensemble = s.n_syms, True, device_ensemble
+    lanc.prepare_random(seed=seed, sector="R")
+    run_FT_batched([lanc], steps, precision=precision, verbose=False)
+    return lanc
+
+
+def ensemble_checksum(X, Y, rho):
+    """Order-sensitive float summary of the sampled ensemble (identifies the inputs of a stored chain)."""
+    k = np.arange(1, X.shape[0] + 1, dtype=np.float64)[:, None]
+    return np.array([float((X * k).sum()), float((Y * k).sum()), float(rho.sum())])
