@@ -73,6 +73,28 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
     }
 }
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+
+// Loose alignment of the CTAs' tile starts.  Each producer counts its tile starts in a global
+// counter; before loading its i-th tile it waits (at most `budget_ns`, then goes on regardless)
+// until every CTA that has an i-th tile has started it.  CTAs then walk the K range of concurrent
+// tiles together and the A / B panels they share are read from HBM once and hit in L2 afterwards;
+// without it they drift apart over the long K loops and most panel reads miss.  Purely a
+// performance hint: results never depend on it.
+__device__ __forceinline__ void tile_start_sync(unsigned *counter, unsigned target, unsigned long long budget_ns) {
+    atomicAdd(counter, 1u);
+    if (budget_ns == 0) return;
+    const unsigned long long t0 = globaltimer();
+    while (ld_acquire_gpu(counter) < target) {
+        if (globaltimer() - t0 > budget_ns) break;
+        __nanosleep(128);
+    }
+}
+
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, int c0, int c1, uint32_t bar) {
     asm volatile(
         "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
@@ -169,7 +191,8 @@ template <int BN, int STAGES, bool TF32, int NPROD>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
-               int M, int N, int K, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err) {
+               int M, int N, int K, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err,
+               unsigned *tile_sync, unsigned sync_ns) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -215,7 +238,10 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA_hi)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB_hi)) : "memory");
         long long g = 0;
-        for (int t = blockIdx.x; t < num_tiles && !*abort_flag; t += gridDim.x) {
+        unsigned target = 0;   // tile starts of all CTAs up to and including this round
+        for (int t = blockIdx.x, round = 0; t < num_tiles && !*abort_flag; t += gridDim.x, ++round) {
+            target += (unsigned)min((int)gridDim.x, num_tiles - round * (int)gridDim.x);
+            if (tile_sync) tile_start_sync(tile_sync, target, round > 0 ? sync_ns : 0ull);
             int mb, nbk;
             tile_coords(t, num_m, num_n, group_m, mb, nbk);
             const int m0 = mb * BM, n0 = nbk * BN;
@@ -429,7 +455,7 @@ static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long
     const bool enabled = !(env && atoi(env) == 0);
     int best = num_m;
     if (enabled && tiles >= 8LL * sms) {
-        const int cand_all[] = {num_m, 48, 24, 13, 6};
+        const int cand_all[] = {num_m, 48, 24, 12, 6};
         cudaEvent_t e0, e1;
         TD_CUDA(cudaEventCreate(&e0));
         TD_CUDA(cudaEventCreate(&e1));
@@ -461,6 +487,28 @@ static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long
     return 0;
 }
 
+// One tile-start counter per device (zeroed on the stream before every launch).
+static std::mutex g_sync_mutex;
+static unsigned *g_sync_counter[64] = {nullptr};
+
+static int tile_sync_counter(int dev, unsigned **out) {
+    std::lock_guard<std::mutex> lock(g_sync_mutex);
+    TD_CHECK(dev >= 0 && dev < 64, TDSCHA_EINVAL, "device index %d out of range", dev);
+    if (!g_sync_counter[dev]) TD_CUDA(cudaMalloc(&g_sync_counter[dev], 256));
+    *out = g_sync_counter[dev];
+    return 0;
+}
+
+// Budget of one tile-start wait (TDSCHA_TILE_SYNC_US, 0 disables the alignment).
+static unsigned tile_sync_budget_ns() {
+    static long long v = -1;
+    if (v < 0) {
+        const char *env = getenv("TDSCHA_TILE_SYNC_US");
+        v = env ? std::max(0, atoi(env)) * 1000LL : 50000LL;
+    }
+    return (unsigned)v;
+}
+
 template <int BN, int STAGES, bool TF32, int NPROD>
 static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
@@ -484,8 +532,13 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(NPROD), num_kb);
     dim3 grid((unsigned)std::min<long long>(tiles, sms));
     const int num_m = ceil_div(M, BM);
+    const unsigned sync_ns = tile_sync_budget_ns();
+    unsigned *counter = nullptr;
+    if (sync_ns > 0 && tiles > grid.x) TD_TRY(tile_sync_counter(dev, &counter));
     auto launch = [&](int gm) {
-        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err);
+        if (counter) cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
+        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err,
+                                                        counter, sync_ns);
     };
     if (const char *env = getenv("TDSCHA_GROUP_M")) {   // tuning knob: fixed tile-group size
         launch(std::max(1, std::min(num_m, atoi(env))));
