@@ -94,6 +94,12 @@ __global__ void thermal_kernel(const double *w, int n, double T, double *ups, do
     psi[m] = (1.0 + 2.0 * nb) / (2.0 * w[m]);
 }
 
+__global__ void to_f32_kernel(const double *a, long long count, float *out) {
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < count;
+         idx += (long long)gridDim.x * blockDim.x)
+        out[idx] = (float)a[idx];
+}
+
 __global__ void scale_rows_kernel(const double *A, const double *s, int N, int n, double *out) {
     long long total = (long long)N * n;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
@@ -279,6 +285,7 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
         (rc = dev_alloc((void **)&e->rho, N * sizeof(double), &acc)) || (rc = dev_alloc((void **)&e->w, n * sizeof(double), &acc)) ||
         (rc = dev_alloc((void **)&e->ups, n * sizeof(double), &acc)) || (rc = dev_alloc((void **)&e->psi, n * sizeof(double), &acc)) ||
         (rc = dev_alloc((void **)&e->sym, soff * sizeof(double), &acc)) ||
+        (rc = dev_alloc((void **)&e->sym32, soff * sizeof(float), &acc)) ||
         (rc = dev_alloc((void **)&e->d_blk_start, n_blocks * sizeof(int), &acc)) ||
         (rc = dev_alloc((void **)&e->d_blk_dim, n_blocks * sizeof(int), &acc)) ||
         (rc = dev_alloc((void **)&e->d_blk_sym_off, n_blocks * sizeof(long long), &acc)) ||
@@ -318,6 +325,7 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
 #undef TD_UP
     if (cudaMemset(e->d_err, 0, sizeof(unsigned)) != cudaSuccess) return fail(TDSCHA_ECUDA);
     thermal_kernel<<<ceil_div(n, 128), 128>>>(e->w, n, T, e->ups, e->psi);
+    to_f32_kernel<<<grid_for(soff), 256>>>(e->sym, soff, e->sym32);
     scale_rows_kernel<<<grid_for((long long)N * n), 256>>>(e->Y, e->psi, N, n, e->G);
     scale_rows_kernel<<<grid_for((long long)N * n), 256>>>(e->X, e->ups, N, n, e->Xt);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
@@ -351,7 +359,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaGetDevice(&prev);
     cudaSetDevice(e->device);
     cudaDeviceSynchronize();
-    void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->d_blk_start, e->d_blk_dim,
+    void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->sym32, e->d_blk_start, e->d_blk_dim,
                   e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -483,7 +491,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     double *partD = reinterpret_cast<double *>(W + L.partD);
     double *partF = reinterpret_cast<double *>(W + L.partF);
 
-    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax};
+    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->sym32};
 
     for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
         const int nj = std::min(Jc, e->N_sym - j0);

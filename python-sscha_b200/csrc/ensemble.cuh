@@ -74,6 +74,7 @@ struct tdscha_ensemble {
     // device arrays
     double *X = nullptr, *Y = nullptr, *G = nullptr, *Xt = nullptr;
     double *rho = nullptr, *w = nullptr, *ups = nullptr, *psi = nullptr, *sym = nullptr;
+    float *sym32 = nullptr;                        // fp32 copy of the symmetry tables
     int *d_blk_start = nullptr, *d_blk_dim = nullptr, *d_blocks_ids = nullptr, *d_bp_b = nullptr, *d_bp_c = nullptr;
     long long *d_blk_sym_off = nullptr;
     int *d_pair_mu = nullptr, *d_pair_nu = nullptr;

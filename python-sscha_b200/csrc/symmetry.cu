@@ -1,5 +1,6 @@
 // symmetry.cu -- block-pair kernels for the symmetry transform and fold (see symmetry.cuh).
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "symmetry.cuh"
@@ -260,7 +261,7 @@ int sym_transform(const SymTables &t, const PairClasses &pc, int nb, int nj, int
         pad_kernel<<<g, 256, 0, st>>>(M, P, Kp, t.n, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
         TD_CUDA(cudaGetLastError());
     }
-    if (fp32_compute) return transform_all<float>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st);
+    if (fp32_compute) return sym_transform_tc(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st);
     return transform_all<double>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st);
 }
 
@@ -293,6 +294,9 @@ int sym_fold(const SymTables &t, const PairClasses &pc, const int *blocks_ids, i
              const AccT *Z, long long ldz, const AccT *F, long long ldf, const double *ups, double *partD, double *partF,
              bool fp32_compute, cudaStream_t st) {
     (void)blocks_ids;
+    if constexpr (std::is_same<AccT, float>::value) {
+        if (fp32_compute) return sym_fold_tc(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);
+    }
     if (fp32_compute) return fold_all<float, AccT>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);
     return fold_all<double, AccT>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);
 }

@@ -23,6 +23,7 @@ struct SymTables {
     const long long *off;      // offset of block b's table
     const int *start, *dim;    // first mode and size of block b
     int n_blocks, n, dmax;
+    const float *sym32;        // the same tables in fp32 (mixed-precision modes)
 };
 
 // Block pairs (b <= c) grouped by micro-tile class MT = ceil(max(d_b, d_c) / 16).
@@ -39,6 +40,14 @@ void free_pair_classes(PairClasses &pc);
 int sym_transform(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, const double *Ys, const double *R1,
                   const double *ups, long long P, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo,
                   void *r1_hi, void *r1_lo, bool fp32_compute, cudaStream_t st);
+
+// The same two stages on the tensor pipe (mma.sync, three-term tf32 splitting), used by the
+// mixed-precision modes; FP64 keeps sym_transform / sym_fold with T = double.
+int sym_transform_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, const double *Ys, const double *R1,
+                     const double *ups, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo, void *r1_hi,
+                     void *r1_lo, cudaStream_t st);
+int sym_fold_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, int Jf, int nf_total, const float *Z,
+                long long ldz, const float *F, long long ldf, const double *ups, double *partD, double *partF, cudaStream_t st);
 
 // Z (rows r as above, packed pairs, ldz), F (rows r, ldf); partials per (k, fold chunk fg).  The
 // per-symmetry block products run in FP32 when fp32_compute and are summed over symmetries in FP64.
