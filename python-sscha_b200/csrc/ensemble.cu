@@ -94,10 +94,17 @@ __global__ void thermal_kernel(const double *w, int n, double T, double *ups, do
     psi[m] = (1.0 + 2.0 * nb) / (2.0 * w[m]);
 }
 
-__global__ void to_f32_kernel(const double *a, long long count, float *out) {
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < count;
-         idx += (long long)gridDim.x * blockDim.x)
-        out[idx] = (float)a[idx];
+// (N_sym, d, d) fp64 table -> (N_sym, dp, dp) fp32 zero-padded copies, as given and transposed
+__global__ void pad_sym_kernel(const double *S, int N_sym, int d, int dp, float *P, float *PT) {
+    const long long total = (long long)N_sym * dp * dp;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long j = idx / ((long long)dp * dp);
+        const int e = (int)(idx % ((long long)dp * dp)), p = e / dp, q = e % dp;
+        const bool in = p < d && q < d;
+        P[idx] = in ? (float)S[(j * d + p) * d + q] : 0.f;
+        PT[idx] = in ? (float)S[(j * d + q) * d + p] : 0.f;
+    }
 }
 
 __global__ void scale_rows_kernel(const double *A, const double *s, int N, int n, double *out) {
@@ -270,6 +277,13 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
     e->blk_sym_off.resize(n_blocks);
     long long soff = 0;
     for (int b = 0; b < n_blocks; ++b) { e->blk_sym_off[b] = soff; soff += (long long)N_sym * dim[b] * dim[b]; }
+    std::vector<long long> offP(n_blocks);
+    long long soffP = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        const long long dp = (dim[b] + 3) & ~3;
+        offP[b] = soffP;
+        soffP += (long long)N_sym * dp * dp;
+    }
     for (int b = 0; b < n_blocks; ++b)
         for (int c = b; c < n_blocks; ++c) { e->bp_b.push_back(b); e->bp_c.push_back(c); }
     double neff = 0;
@@ -285,7 +299,9 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
         (rc = dev_alloc((void **)&e->rho, N * sizeof(double), &acc)) || (rc = dev_alloc((void **)&e->w, n * sizeof(double), &acc)) ||
         (rc = dev_alloc((void **)&e->ups, n * sizeof(double), &acc)) || (rc = dev_alloc((void **)&e->psi, n * sizeof(double), &acc)) ||
         (rc = dev_alloc((void **)&e->sym, soff * sizeof(double), &acc)) ||
-        (rc = dev_alloc((void **)&e->sym32, soff * sizeof(float), &acc)) ||
+        (rc = dev_alloc((void **)&e->symP, soffP * sizeof(float), &acc)) ||
+        (rc = dev_alloc((void **)&e->symPT, soffP * sizeof(float), &acc)) ||
+        (rc = dev_alloc((void **)&e->d_offP, n_blocks * sizeof(long long), &acc)) ||
         (rc = dev_alloc((void **)&e->d_blk_start, n_blocks * sizeof(int), &acc)) ||
         (rc = dev_alloc((void **)&e->d_blk_dim, n_blocks * sizeof(int), &acc)) ||
         (rc = dev_alloc((void **)&e->d_blk_sym_off, n_blocks * sizeof(long long), &acc)) ||
@@ -317,6 +333,7 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
     TD_UP(e->d_blk_start, start.data(), n_blocks * sizeof(int));
     TD_UP(e->d_blk_dim, dim.data(), n_blocks * sizeof(int));
     TD_UP(e->d_blk_sym_off, e->blk_sym_off.data(), n_blocks * sizeof(long long));
+    TD_UP(e->d_offP, offP.data(), n_blocks * sizeof(long long));
     TD_UP(e->d_blocks_ids, blocks_ids, n * sizeof(int));
     TD_UP(e->d_bp_b, e->bp_b.data(), e->bp_b.size() * sizeof(int));
     TD_UP(e->d_bp_c, e->bp_c.data(), e->bp_c.size() * sizeof(int));
@@ -325,7 +342,11 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
 #undef TD_UP
     if (cudaMemset(e->d_err, 0, sizeof(unsigned)) != cudaSuccess) return fail(TDSCHA_ECUDA);
     thermal_kernel<<<ceil_div(n, 128), 128>>>(e->w, n, T, e->ups, e->psi);
-    to_f32_kernel<<<grid_for(soff), 256>>>(e->sym, soff, e->sym32);
+    for (int b = 0; b < n_blocks; ++b) {
+        const long long dp = (dim[b] + 3) & ~3;
+        pad_sym_kernel<<<grid_for((long long)N_sym * dp * dp), 256>>>(e->sym + e->blk_sym_off[b], N_sym, dim[b], (int)dp,
+                                                                      e->symP + offP[b], e->symPT + offP[b]);
+    }
     scale_rows_kernel<<<grid_for((long long)N * n), 256>>>(e->Y, e->psi, N, n, e->G);
     scale_rows_kernel<<<grid_for((long long)N * n), 256>>>(e->X, e->ups, N, n, e->Xt);
     if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) {
@@ -359,7 +380,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaGetDevice(&prev);
     cudaSetDevice(e->device);
     cudaDeviceSynchronize();
-    void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->sym32, e->d_blk_start, e->d_blk_dim,
+    void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->symP, e->symPT, e->d_offP, e->d_blk_start, e->d_blk_dim,
                   e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base};
     for (void *p : ps)
         if (p) cudaFree(p);
@@ -491,7 +512,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     double *partD = reinterpret_cast<double *>(W + L.partD);
     double *partF = reinterpret_cast<double *>(W + L.partF);
 
-    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->sym32};
+    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->symP, e->symPT, e->d_offP};
 
     for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
         const int nj = std::min(Jc, e->N_sym - j0);

@@ -74,7 +74,8 @@ struct tdscha_ensemble {
     // device arrays
     double *X = nullptr, *Y = nullptr, *G = nullptr, *Xt = nullptr;
     double *rho = nullptr, *w = nullptr, *ups = nullptr, *psi = nullptr, *sym = nullptr;
-    float *sym32 = nullptr;                        // fp32 copy of the symmetry tables
+    float *symP = nullptr, *symPT = nullptr;       // padded fp32 symmetry tables (as given, transposed)
+    long long *d_offP = nullptr;                   // block offsets into symP / symPT
     int *d_blk_start = nullptr, *d_blk_dim = nullptr, *d_blocks_ids = nullptr, *d_bp_b = nullptr, *d_bp_c = nullptr;
     long long *d_blk_sym_off = nullptr;
     int *d_pair_mu = nullptr, *d_pair_nu = nullptr;

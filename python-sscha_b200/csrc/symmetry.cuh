@@ -23,7 +23,11 @@ struct SymTables {
     const long long *off;      // offset of block b's table
     const int *start, *dim;    // first mode and size of block b
     int n_blocks, n, dmax;
-    const float *sym32;        // the same tables in fp32 (mixed-precision modes)
+    // fp32 copies for the tensor-core kernels of the mixed-precision modes: block b's (N_sym, DP, DP)
+    // tables with DP = d_b rounded up to 4 (zero padded), as given (symP) and transposed (symPT),
+    // starting at element offP[b]
+    const float *symP, *symPT;
+    const long long *offP;
 };
 
 // Block pairs (b <= c) grouped by micro-tile class MT = ceil(max(d_b, d_c) / 16).

@@ -8,15 +8,18 @@
 //
 //   * One warp task = one 16 x 8 output tile, so even a (72-mode, 3-mode) block pair keeps most of
 //     the 16 warps busy.
+//   * Fragments come from shared memory through ldmatrix (one instruction per four tf32 values of
+//     a warp tile).  B operands are stored n-major ([n][k]), the layout ldmatrix hands out as the
+//     "col" fragment, so the symmetry blocks come from a transposed copy where needed and the
+//     intermediate products are written transposed.
 //   * Operands reused across symmetries or tiles (the Ys block, the intermediate product) are kept
-//     in shared memory already split, as (hi, lo) float2 pairs; the symmetry blocks are fp32 and
-//     split while the fragments are loaded.
-//   * Symmetry j + 1's blocks are copied (cp.async) into the second half of a double buffer while
-//     symmetry j is computed.
-//   * Block dimensions are zero-padded to 16 on the row side of an A operand and 8 elsewhere.
-//     Leading dimensions make every fragment load free of bank conflicts: fp32 arrays read as
-//     (row g, column t) use ld = 4 (mod 8), fp32 arrays read as (row t, column g) use ld = 8
-//     (mod 16), float2 arrays use ld = 4 (mod 8) (in float2 units).
+//     already split into tf32 hi / lo arrays; symmetry blocks and the fold's weights are fp32 and
+//     split after the ldmatrix.
+//   * Symmetry j + 1's blocks (16-byte cp.async from zero-padded fp32 tables) are copied into the
+//     second half of a double buffer while symmetry j is computed.
+//   * Block dimensions are zero-padded to 16 on the m side and 8 on the n and k sides.  Every
+//     shared array has leading dimension ld = 4 (mod 8) floats, which makes the ldmatrix row
+//     addresses and the transposed fragment stores free of bank conflicts.
 #include <algorithm>
 #include <cstdint>
 #include <cuda_bf16.h>
@@ -29,12 +32,12 @@ namespace {
 constexpr int THREADS = 512;
 constexpr int NW = THREADS / 32;
 
-__host__ __device__ constexpr int ld_gt(int d) { return d + ((4 - d % 8) + 8) % 8; }     // ld = 4 (mod 8)
-__host__ __device__ constexpr int ld_tg(int d) { return d + ((8 - d % 16) + 16) % 16; }  // ld = 8 (mod 16)
+__host__ __device__ constexpr int ld_for(int d) { return d + ((4 - d % 8) + 8) % 8; }   // ld = 4 (mod 8)
 
 __device__ __forceinline__ long long pair_index(int mu, int nu, int n) {   // mu <= nu, row-major upper triangle
     return (long long)mu * n - ((long long)mu * (mu - 1)) / 2 + (nu - mu);
 }
+__device__ __forceinline__ uint32_t smem_u32(const void *p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
 __device__ __forceinline__ uint32_t to_tf32(float v) {
     uint32_t r;
@@ -45,73 +48,96 @@ __device__ __forceinline__ void split_tf32(float v, uint32_t &hi, uint32_t &lo) 
     hi = to_tf32(v);
     lo = to_tf32(v - __uint_as_float(hi));
 }
-__device__ __forceinline__ float2 split2(float v) {
-    uint32_t h, l;
-    split_tf32(v, h, l);
-    return make_float2(__uint_as_float(h), __uint_as_float(l));
-}
 __device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
         "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};"
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
 }
+// ldmatrix of 8 x 8 b16 matrices = 8 rows x 4 fp32 words: thread 4g + t receives word t of row g.
+__device__ __forceinline__ void ldsm_x4(uint32_t (&r)[4], uint32_t addr) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]) : "r"(addr));
+}
+__device__ __forceinline__ void ldsm_x2(uint32_t (&r)[2], uint32_t addr) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x2.shared.b16 {%0,%1}, [%2];" : "=r"(r[0]), "=r"(r[1]) : "r"(addr));
+}
 
-// 4-byte asynchronous global -> shared copies; `valid` false writes a zero instead (src-size 0).
+// asynchronous global -> shared copies; `valid` false writes zeros instead (src-size 0)
 __device__ __forceinline__ void cp_async4(float *dst, const float *src, bool valid) {
-    const uint32_t d = static_cast<uint32_t>(__cvta_generic_to_shared(dst));
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(d), "l"(src), "r"(valid ? 4 : 0) : "memory");
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 4 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async16(float *dst, const float *src, bool valid) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(valid ? 16 : 0) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int PENDING>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory"); }
 
-// Operand views of one warp tile.  Element (r, c) of the logical operand:
-//   F32   : p[r * ld + c]          fp32, split on load
-//   F32T  : p[c * ld + r]          fp32 stored transposed, split on load
-//   F2    : q[r * ld + c]          float2 (hi, lo), already split
-enum OpKind { F32, F32T, F2 };
-template <int KIND>
-__device__ __forceinline__ void load_op(const void *p, int ld, int r, int c, uint32_t &hi, uint32_t &lo) {
-    if constexpr (KIND == F2) {
-        const float2 v = static_cast<const float2 *>(p)[r * ld + c];
-        hi = __float_as_uint(v.x);
-        lo = __float_as_uint(v.y);
-    } else if constexpr (KIND == F32) {
-        split_tf32(static_cast<const float *>(p)[r * ld + c], hi, lo);
-    } else {
-        split_tf32(static_cast<const float *>(p)[c * ld + r], hi, lo);
+// rows x cols (cols a multiple of 4) of a (dp x dp) zero-padded fp32 table into shared memory with
+// leading dimension ld; rows / chunks beyond the table are zero filled
+template <int LD>
+__device__ __forceinline__ void copy_table(float *dst, const float *src, int dp, int rows, int cols) {
+    const int cpr = cols >> 2;
+    for (int e = threadIdx.x; e < rows * cpr; e += THREADS) {
+        const int r = e / cpr, ch = e - r * cpr;
+        const bool v = r < dp && 4 * ch < dp;
+        cp_async16(dst + r * LD + 4 * ch, v ? src + (long long)r * dp + 4 * ch : src, v);
     }
 }
 
-// c += A[m0:m0+16, 0:8 kt] . B[0:8 kt, n0:n0+8], three-term tf32 split.  Fragment layouts of
-// m16n8k8 (g = lane / 4, t = lane % 4): a0 (g, t), a1 (g + 8, t), a2 (g, t + 4), a3 (g + 8, t + 4);
-// b0 (t, g), b1 (t + 4, g); c0/c1 (g, 2t / 2t + 1), c2/c3 (g + 8, 2t / 2t + 1).
-template <int AK, int BK>
-__device__ __forceinline__ void warp_tile(float (&c)[4], const void *A, int lda, const void *B, int ldb, int m0, int n0, int kt) {
-    const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+// c += A[m0:m0+16, 0:8 kt] . B[0:8 kt, n0:n0+8] with three-term tf32 splitting.  A is stored
+// row-major [m][k], B n-major [n][k], both with leading dimension LD.  A_SPLIT / B_SPLIT: the
+// operand is given as separate hi / lo arrays; otherwise it is one fp32 array split on load.
+// Fragment layouts of m16n8k8 (g = lane / 4, t = lane % 4): a0 (g, t), a1 (g + 8, t),
+// a2 (g, t + 4), a3 (g + 8, t + 4); b0 (k = t, n = g), b1 (k = t + 4, n = g).
+template <int LD, bool A_SPLIT, bool B_SPLIT>
+__device__ __forceinline__ void warp_tile(float (&c)[4], const float *Ahi, const float *Alo, const float *Bhi, const float *Blo,
+                                          int m0, int n0, int kt) {
+    const int lane = threadIdx.x & 31, q = lane >> 3, r8 = lane & 7;
+    const uint32_t a_off = (uint32_t)(((m0 + r8 + 8 * (q & 1)) * LD + 4 * (q >> 1)) * 4);
+    const uint32_t b_off = (uint32_t)(((n0 + r8) * LD + 4 * (q & 1)) * 4);
+    const uint32_t ah_base = smem_u32(Ahi) + a_off, bh_base = smem_u32(Bhi) + b_off;
+    const uint32_t al_base = A_SPLIT ? smem_u32(Alo) + a_off : 0u, bl_base = B_SPLIT ? smem_u32(Blo) + b_off : 0u;
 #pragma unroll 2
     for (int ks = 0; ks < kt; ++ks) {
-        const int k0 = ks * 8;
-        uint32_t ah[4], al[4], bh0, bl0, bh1, bl1;
-        load_op<AK>(A, lda, m0 + g, k0 + t, ah[0], al[0]);
-        load_op<AK>(A, lda, m0 + g + 8, k0 + t, ah[1], al[1]);
-        load_op<AK>(A, lda, m0 + g, k0 + t + 4, ah[2], al[2]);
-        load_op<AK>(A, lda, m0 + g + 8, k0 + t + 4, ah[3], al[3]);
-        load_op<BK>(B, ldb, k0 + t, n0 + g, bh0, bl0);
-        load_op<BK>(B, ldb, k0 + t + 4, n0 + g, bh1, bl1);
-        mma_tf32(c, al, bh0, bh1);   // small terms first
-        mma_tf32(c, ah, bl0, bl1);
-        mma_tf32(c, ah, bh0, bh1);
+        uint32_t ah[4], al[4], bh[2], bl[2];
+        if constexpr (A_SPLIT) {
+            ldsm_x4(ah, ah_base + ks * 32);
+            ldsm_x4(al, al_base + ks * 32);
+        } else {
+            uint32_t raw[4];
+            ldsm_x4(raw, ah_base + ks * 32);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) split_tf32(__uint_as_float(raw[i]), ah[i], al[i]);
+        }
+        if constexpr (B_SPLIT) {
+            ldsm_x2(bh, bh_base + ks * 32);
+            ldsm_x2(bl, bl_base + ks * 32);
+        } else {
+            uint32_t raw[2];
+            ldsm_x2(raw, bh_base + ks * 32);
+#pragma unroll
+            for (int i = 0; i < 2; ++i) split_tf32(__uint_as_float(raw[i]), bh[i], bl[i]);
+        }
+        mma_tf32(c, al, bh[0], bh[1]);   // small terms first
+        mma_tf32(c, ah, bl[0], bl[1]);
+        mma_tf32(c, ah, bh[0], bh[1]);
     }
 }
 
-// store a warp tile's accumulators as split (hi, lo) pairs into a float2 array
-__device__ __forceinline__ void store_tile_f2(float2 *X, int ld, int m0, int n0, const float (&c)[4]) {
+// a warp tile's accumulators, transposed ([n][m]) and split, into hi / lo arrays
+template <int LD>
+__device__ __forceinline__ void store_tile_t(float *Xhi, float *Xlo, int m0, int n0, const float (&c)[4]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
-    const float2 a0 = split2(c[0]), a1 = split2(c[1]), a2 = split2(c[2]), a3 = split2(c[3]);
-    *reinterpret_cast<float4 *>(&X[(m0 + g) * ld + n0 + 2 * t]) = make_float4(a0.x, a0.y, a1.x, a1.y);
-    *reinterpret_cast<float4 *>(&X[(m0 + g + 8) * ld + n0 + 2 * t]) = make_float4(a2.x, a2.y, a3.x, a3.y);
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const int idx = (n0 + 2 * t + (e & 1)) * LD + m0 + g + 8 * (e >> 1);
+        uint32_t h, l;
+        split_tf32(c[e], h, l);
+        Xhi[idx] = __uint_as_float(h);
+        Xlo[idx] = __uint_as_float(l);
+    }
 }
 
 // bf16 / tf32 hi + lo of an fp32 value into the GEMM operand arrays
@@ -130,21 +156,17 @@ __device__ __forceinline__ void store_split_f(Format fmt, void *hi, void *lo, lo
 template <int MT>
 struct TcShape {
     static constexpr int DM = 16 * MT;   // padded block size of the class
-    static constexpr int L2 = ld_gt(DM);  // float2 arrays
-    static constexpr int LG = ld_gt(DM);  // fp32 arrays read (row g, column t)
-    static constexpr int LT = ld_tg(DM);  // fp32 arrays read (row t, column g)
-    // transform: Yk2 + M12 (float2) + 2 x (S_b, S_c) fp32
-    static constexpr size_t TRANSFORM_SMEM = (size_t)DM * (2 * L2 * 8 + 4 * LT * 4);
-    // fold: 2 x (S_b, S_c, W) fp32 + U2 float2
-    static constexpr size_t FOLD_SMEM = (size_t)DM * (6 * LG * 4 + L2 * 8);
+    static constexpr int LD = ld_for(DM);
+    static constexpr int ARR = DM * LD;   // floats per shared array
+    static constexpr size_t SMEM = (size_t)8 * ARR * sizeof(float);
     // fold step-2 tiles per warp (16 x 8 tiles of the largest block pair of the class)
     static constexpr int TILES_PER_WARP = ((DM / 16) * (DM / 8) + NW - 1) / NW;
 };
 
 // ---- transform ---------------------------------------------------------------------------------------
 // grid (pairs of the class, j-chunks of JT symmetries, nb).  Per symmetry:
-//   step 1  M1 (d_b x d_c) = Ys_k[b, c] . S_c        (A = Yk2, B = S_c)
-//   step 2  T  (d_b x d_c) = S_b^T . M1               (A = S_b read transposed, B = M12)
+//   step 1  M1 (d_b x d_c) = Ys_k[b, c] . S_c       A = Y (split), B[n][k] = S_c^T (transposed table)
+//   step 2  T  (d_b x d_c) = S_b^T . M1              A = S_b^T (transposed table), B[n][k] = M1^T (split)
 // T is staged in shared memory and written row by row to B1 (packed pairs, format fmt) for
 // global modes mu <= nu.
 template <int MT>
@@ -153,43 +175,39 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
                     const double *__restrict__ Ys, const double *__restrict__ R1, const double *__restrict__ ups, long long Kp,
                     long long np, Format fmt, void *B1_hi, void *B1_lo, void *r1_hi, void *r1_lo) {
     using S = TcShape<MT>;
-    constexpr int DM = S::DM, L2 = S::L2, LT = S::LT;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    float2 *Yk2 = reinterpret_cast<float2 *>(sm_raw);    // [DM][L2]  Ys_k[b, c] (mu, nu), split
-    float2 *M12 = Yk2 + DM * L2;                          // [DM][L2]  Ys_k[b, c] S_c (mu', nu'), split
-    float *Sbuf = reinterpret_cast<float *>(M12 + DM * L2);   // 2 x ([DM][LT] S_b (p, mu), [DM][LT] S_c (nu, nu'))
+    constexpr int LD = S::LD, ARR = S::ARR;
+    extern __shared__ __align__(16) float smf[];
+    float *Yhi = smf, *Ylo = smf + ARR;               // Ys_k[b, c] (mu, nu)
+    float *MThi = smf + 2 * ARR, *MTlo = smf + 3 * ARR;   // M1^T (nu', mu')
+    float *Tab = smf + 4 * ARR;                       // buffers x {S_b^T (mu, p), S_c^T (nu', nu)}
     const int b = pb[blockIdx.x], c = pc[blockIdx.x];
     const int k = blockIdx.z;
     const int ja = j0 + blockIdx.y * JT, jb = min(ja + JT, j0 + nj);
     const int n = tb.n;
     const int sb = tb.start[b], db = tb.dim[b], sc = tb.start[c], dc = tb.dim[c];
-    const int DB = (db + 15) & ~15, DC = (dc + 7) & ~7;
+    const int DB = (db + 15) & ~15, DB8 = (db + 7) & ~7, DC = (dc + 7) & ~7;
+    const int dpb = (db + 3) & ~3, dpc = (dc + 3) & ~3;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const float *Sb_base = tb.sym32 + tb.off[b], *Sc_base = tb.sym32 + tb.off[c];
-    auto issue = [&](int j, int buf) {   // symmetry j's two blocks (zero padded) into buffer `buf`
-        float *sbd = Sbuf + buf * 2 * DM * LT, *scd = sbd + DM * LT;
-        const float *Sbg = Sb_base + (long long)j * db * db, *Scg = Sc_base + (long long)j * dc * dc;
-        for (int p = warp; p < DB; p += NW)
-            for (int q = lane; q < DB; q += 32) {
-                const bool v = p < db && q < db;
-                cp_async4(&sbd[p * LT + q], v ? Sbg + p * db + q : Sbg, v);
-            }
-        for (int p = warp; p < DC; p += NW)
-            for (int q = lane; q < DC; q += 32) {
-                const bool v = p < dc && q < dc;
-                cp_async4(&scd[p * LT + q], v ? Scg + p * dc + q : Scg, v);
-            }
+    const float *Tb_base = tb.symPT + tb.offP[b], *Tc_base = tb.symPT + tb.offP[c];
+    auto issue = [&](int j, int buf) {
+        float *stb = Tab + buf * 2 * ARR, *stc = stb + ARR;
+        copy_table<LD>(stb, Tb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
+        copy_table<LD>(stc, Tc_base + (long long)j * dpc * dpc, dpc, DC, DC);
         cp_async_commit();
     };
     if (ja < jb) issue(ja, 0);
     const double *Yg = Ys + (long long)k * n * n;
     for (int mu = warp; mu < DB; mu += NW)
-        for (int nu = lane; nu < DC; nu += 32)
-            Yk2[mu * L2 + nu] = split2((mu < db && nu < dc) ? (float)Yg[(long long)(sb + mu) * n + sc + nu] : 0.f);
+        for (int nu = lane; nu < DC; nu += 32) {
+            uint32_t h, l;
+            split_tf32((mu < db && nu < dc) ? (float)Yg[(long long)(sb + mu) * n + sc + nu] : 0.f, h, l);
+            Yhi[mu * LD + nu] = __uint_as_float(h);
+            Ylo[mu * LD + nu] = __uint_as_float(l);
+        }
     const int mt = DB / 16, nt = DC / 8, tiles = mt * nt;
     for (int j = ja; j < jb; ++j) {
         const int cur = (j - ja) & 1;
-        float *Sb = Sbuf + cur * 2 * DM * LT, *Sc = Sb + DM * LT;
+        float *STb = Tab + cur * 2 * ARR, *STc = STb + ARR;
         const long long r = (long long)k * nj + (j - j0);
         if (j + 1 < jb) {            // prefetch the next symmetry, then wait for this one
             issue(j + 1, cur ^ 1);
@@ -201,24 +219,24 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
         for (int ti = warp; ti < tiles; ti += NW) {
             const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            warp_tile<F2, F32>(acc, Yk2, L2, Sc, LT, m0, n0, DC / 8);
-            store_tile_f2(M12, L2, m0, n0, acc);
+            warp_tile<LD, true, false>(acc, Yhi, Ylo, STc, nullptr, m0, n0, DC / 8);
+            store_tile_t<LD>(MThi, MTlo, m0, n0, acc);
         }
         if (b == c && (int)threadIdx.x < db) {   // r1 for the modes of block b: ups o (S_b^T R)
             const double *Rk = R1 + (long long)k * n + sb;
             double s = 0.0;
-            for (int p = 0; p < db; ++p) s += (double)Sb[p * LT + threadIdx.x] * Rk[p];
+            for (int p = 0; p < db; ++p) s += (double)STb[threadIdx.x * LD + p] * Rk[p];
             store_split(fmt, r1_hi, r1_lo, r * np + sb + threadIdx.x, ups[sb + threadIdx.x] * s);
         }
         __syncthreads();             // M1 complete; S_c of this symmetry no longer needed
-        float *Tb = Sc;              // step-2 result staged where S_c was
+        float *T = STc;              // step-2 result staged where S_c^T was
         for (int ti = warp; ti < tiles; ti += NW) {
             const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            warp_tile<F32T, F2>(acc, Sb, LT, M12, L2, m0, n0, DB / 8);
+            warp_tile<LD, false, true>(acc, STb, nullptr, MThi, MTlo, m0, n0, DB8 / 8);
             const int g = lane >> 2, t = lane & 3;
-            *reinterpret_cast<float2 *>(&Tb[(m0 + g) * LT + n0 + 2 * t]) = make_float2(acc[0], acc[1]);
-            *reinterpret_cast<float2 *>(&Tb[(m0 + g + 8) * LT + n0 + 2 * t]) = make_float2(acc[2], acc[3]);
+            *reinterpret_cast<float2 *>(&T[(m0 + g) * LD + n0 + 2 * t]) = make_float2(acc[0], acc[1]);
+            *reinterpret_cast<float2 *>(&T[(m0 + g + 8) * LD + n0 + 2 * t]) = make_float2(acc[2], acc[3]);
         }
         __syncthreads();
         // one row mu per warp: consecutive lanes write consecutive packed pairs
@@ -227,7 +245,7 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
             const long long row = r * Kp + pair_index(gm, gm, n) - gm;   // + gn gives pair(gm, gn)
             for (int nu = lane; nu < dc; nu += 32) {
                 const int gn = sc + nu;
-                if (gm <= gn) store_split_f(fmt, B1_hi, B1_lo, row + gn, Tb[mu * LT + nu]);
+                if (gm <= gn) store_split_f(fmt, B1_hi, B1_lo, row + gn, T[mu * LD + nu]);
             }
         }
         __syncthreads();             // buffers of this symmetry free for the prefetch two steps ahead
@@ -237,48 +255,41 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
 // ---- fold ---------------------------------------------------------------------------------------------
 // grid (pairs of the class, fold chunks of Jf symmetries, nb).  Per symmetry:
 //   W  (d_b x d_c) = ups_mu ups_nu (2 on the diagonal) Z[r, pair(mu, nu)]
-//   step 1  U = W . S_c^T                   (A = W, B = S_c read transposed)
-//   step 2  D += S_b . U                    (A = S_b, B = U2); fp32 per symmetry, summed in fp64
+//   step 1  U = W . S_c^T          A = W (fp32), B[n][k] = S_c (table as given)
+//   step 2  D += S_b . U           A = S_b (table as given), B[n][k] = U^T (split); fp32 per
+//                                  symmetry, summed over symmetries in fp64
 template <int MT>
 __global__ void __launch_bounds__(THREADS)
 fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__ pc, const float *__restrict__ Z, long long ldz,
                const float *__restrict__ F, long long ldf, const double *__restrict__ ups, int nj, int j0, int Jf, int nf_total,
                double *__restrict__ partD, double *__restrict__ partF) {
     using S = TcShape<MT>;
-    constexpr int DM = S::DM, L2 = S::L2, LG = S::LG;
-    extern __shared__ __align__(16) unsigned char sm_raw[];
-    float2 *U2 = reinterpret_cast<float2 *>(sm_raw);        // [DM][L2]  W S_c^T (mu', nu'), split
-    float *Sbuf = reinterpret_cast<float *>(U2 + DM * L2);  // 2 x ([DM][LG] S_b (mu, p), S_c (nu', nu), W (mu, nu))
+    constexpr int LD = S::LD, ARR = S::ARR;
+    extern __shared__ __align__(16) float smf[];
+    float *UThi = smf, *UTlo = smf + ARR;   // U^T (nu', mu')
+    float *Buf = smf + 2 * ARR;             // buffers x {S_b (mu, p), S_c (nu', nu), W (mu, nu)}
     const int b = pb[blockIdx.x], c = pc[blockIdx.x];
     const int fc = blockIdx.y, k = blockIdx.z;
     const int n = tb.n;
     const int sb = tb.start[b], db = tb.dim[b], sc = tb.start[c], dc = tb.dim[c];
-    const int DB = (db + 15) & ~15, DC = (dc + 7) & ~7;
+    const int DB = (db + 15) & ~15, DB8 = (db + 7) & ~7, DC = (dc + 7) & ~7;
+    const int dpb = (db + 3) & ~3, dpc = (dc + 3) & ~3;
     const int fg = j0 / Jf + fc;
     const int ja = j0 + fc * Jf, jb = min(j0 + (fc + 1) * Jf, j0 + nj);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
     const int mt = DB / 16, nt = DC / 8, tiles = mt * nt;
-    const float *Sb_base = tb.sym32 + tb.off[b], *Sc_base = tb.sym32 + tb.off[c];
-    auto issue = [&](int j, int buf) {   // symmetry j's blocks and its raw Z block into buffer `buf`
-        float *sbd = Sbuf + buf * 3 * DM * LG, *scd = sbd + DM * LG, *wd = scd + DM * LG;
-        const float *Sbg = Sb_base + (long long)j * db * db, *Scg = Sc_base + (long long)j * dc * dc;
+    const float *Pb_base = tb.symP + tb.offP[b], *Pc_base = tb.symP + tb.offP[c];
+    auto issue = [&](int j, int buf) {
+        float *snb = Buf + buf * 3 * ARR, *snc = snb + ARR, *wd = snc + ARR;
+        copy_table<LD>(snb, Pb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
+        copy_table<LD>(snc, Pc_base + (long long)j * dpc * dpc, dpc, DC, DC);
         const float *Zr = Z + ((long long)k * nj + (j - j0)) * ldz;
-        for (int p = warp; p < DB; p += NW)
-            for (int q = lane; q < DB; q += 32) {
-                const bool v = p < db && q < db;
-                cp_async4(&sbd[p * LG + q], v ? Sbg + p * db + q : Sbg, v);
-            }
-        for (int p = warp; p < DC; p += NW)
-            for (int q = lane; q < DC; q += 32) {
-                const bool v = p < dc && q < dc;
-                cp_async4(&scd[p * LG + q], v ? Scg + p * dc + q : Scg, v);
-            }
         for (int mu = warp; mu < DB; mu += NW)
             for (int nu = lane; nu < DC; nu += 32) {
                 const bool v = mu < db && nu < dc;
                 int gm = sb + mu, gn = sc + nu;
                 if (gm > gn) { const int s2 = gm; gm = gn; gn = s2; }
-                cp_async4(&wd[mu * LG + nu], v ? Zr + pair_index(gm, gn, n) : Zr, v);
+                cp_async4(&wd[mu * LD + nu], v ? Zr + pair_index(gm, gn, n) : Zr, v);
             }
         cp_async_commit();
     };
@@ -287,7 +298,7 @@ fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__
         for (int mu = warp; mu < db; mu += NW)
             for (int nu = lane; nu < dc; nu += 32) {
                 const int gm = sb + mu, gn = sc + nu;
-                wd[mu * LG + nu] *= (float)((gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn]);
+                wd[mu * LD + nu] *= (float)((gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn]);
             }
     };
     constexpr int TPW = S::TILES_PER_WARP;   // step-2 tiles warp, warp + NW, ...: fp64 sums in registers
@@ -300,7 +311,7 @@ fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__
     if (ja < jb) issue(ja, 0);
     for (int j = ja; j < jb; ++j) {
         const int cur = (j - ja) & 1;
-        float *Sb = Sbuf + cur * 3 * DM * LG, *Sc = Sb + DM * LG, *W = Sc + DM * LG;
+        float *SNb = Buf + cur * 3 * ARR, *SNc = SNb + ARR, *W = SNc + ARR;
         const long long r = (long long)k * nj + (j - j0);
         if (j + 1 < jb) {
             issue(j + 1, cur ^ 1);
@@ -313,13 +324,13 @@ fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__
         for (int ti = warp; ti < tiles; ti += NW) {
             const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
             float acc[4] = {0.f, 0.f, 0.f, 0.f};
-            warp_tile<F32, F32T>(acc, W, LG, Sc, LG, m0, n0, DC / 8);
-            store_tile_f2(U2, L2, m0, n0, acc);
+            warp_tile<LD, false, false>(acc, W, nullptr, SNc, nullptr, m0, n0, DC / 8);
+            store_tile_t<LD>(UThi, UTlo, m0, n0, acc);
         }
         if (b == c && (int)threadIdx.x < db) {
             const float *Fr = F + r * ldf + sb;
             double s = 0.0;
-            for (int p = 0; p < db; ++p) s += (double)Sb[threadIdx.x * LG + p] * (double)Fr[p];
+            for (int p = 0; p < db; ++p) s += (double)SNb[threadIdx.x * LD + p] * (double)Fr[p];
             facc += s;
         }
         __syncthreads();
@@ -329,12 +340,12 @@ fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__
             if (ti < tiles) {
                 const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
                 float acc[4] = {0.f, 0.f, 0.f, 0.f};
-                warp_tile<F32, F2>(acc, Sb, LG, U2, L2, m0, n0, DB / 8);
+                warp_tile<LD, false, true>(acc, SNb, nullptr, UThi, UTlo, m0, n0, DB8 / 8);
 #pragma unroll
                 for (int e = 0; e < 4; ++e) accD[i][e] += (double)acc[e];
             }
         }
-        __syncthreads();   // U2 and this symmetry's buffers free
+        __syncthreads();   // U^T and this symmetry's buffers free
     }
     double *out = partD + ((long long)k * nf_total + fg) * (long long)n * n;
 #pragma unroll
@@ -357,13 +368,12 @@ int launch_transform_tc(const SymTables &t, const PairClasses &pc, int nb, int n
                         void *r1_lo, cudaStream_t st) {
     if (!pc.count[MT]) return 0;
     using S = TcShape<MT>;
-    static_assert(S::TRANSFORM_SMEM <= 227 * 1024, "transform shared memory");
+    static_assert(S::SMEM <= 227 * 1024, "shared memory");
     constexpr int JT = 16;
     auto kern = transform_tc_kernel<MT>;
-    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::TRANSFORM_SMEM));
+    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, JT), (unsigned)nb);
-    kern<<<grid, THREADS, S::TRANSFORM_SMEM, st>>>(t, pc.b[MT], pc.c[MT], nj, j0, JT, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo,
-                                                    r1_hi, r1_lo);
+    kern<<<grid, THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], nj, j0, JT, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
     TD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -373,11 +383,11 @@ int launch_fold_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, in
                    long long ldz, const float *F, long long ldf, const double *ups, double *partD, double *partF, cudaStream_t st) {
     if (!pc.count[MT]) return 0;
     using S = TcShape<MT>;
-    static_assert(S::FOLD_SMEM <= 227 * 1024, "fold shared memory");
+    static_assert(S::SMEM <= 227 * 1024, "shared memory");
     auto kern = fold_tc_kernel<MT>;
-    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::FOLD_SMEM));
+    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, Jf), (unsigned)nb);
-    kern<<<grid, THREADS, S::FOLD_SMEM, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
+    kern<<<grid, THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
     TD_CUDA(cudaGetLastError());
     return 0;
 }
