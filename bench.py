@@ -29,7 +29,7 @@ for _p in (REPO, os.path.join(REPO, "python-sscha_b200")):
 
 # DRAM bytes (read + write) of one [a|b] contraction launch, from a 1-pass ncu capture of the same
 # workload (profiles/tc_gemm_c2.md); keyed by (L, N, chains, precision).
-MEASURED_TRAFFIC = {(4, 10000, 8, "bf16x3"): 1.425e12}
+MEASURED_TRAFFIC = {(4, 10000, 8, "bf16x3"): 3.062e11}
 METRIC = "apply_L/s at 128 atoms N=1e4: mixed+batched vs FP64 GPU at G(w) rel err <=1e-5"
 
 
