@@ -164,6 +164,7 @@ class Lanczos(object):
     def init(self, use_symmetries=True):
         self.prepare_symmetrization(no_sym=not use_symmetries)
         self.initialized = True
+        self._make_linops()
 
     def prepare_symmetrization(self, no_sym=False, verbose=True, symmetries=None):
         """Mode-space symmetry blocks (DynamicalLanczos.py:686-782).  ``symmetries`` may be a tuple
@@ -330,6 +331,320 @@ class Lanczos(object):
                                    self.reverse_L, self.shift_value, self.perturbation_modulus)
         g = gf.cpu().numpy()
         return (g[0::2] + 1j * g[1::2]).reshape(w_array.shape)
+
+    # ---- consumers of apply_full_L (DynamicalLanczos.py:2391-2502, 3761-3972, 4571-4613, 5273-5307,
+    #      5454-5789, 6381-6421) -------------------------------------------------------------------
+    def _make_linops(self):
+        """L_linop / M_linop as the reference builds them (DynamicalLanczos.py:468-479, 3749-3759):
+        matvec = apply_full_L, rmatvec = its transpose, preconditioner = the harmonic inverse.  The
+        matvec here leaves self.psi untouched."""
+        import scipy.sparse.linalg as sla
+        ln = len(self.psi)
+        self.L_linop = sla.LinearOperator((ln, ln), matvec=lambda x: self._apply_host(x, False, self._opts()),
+                                          rmatvec=lambda x: self._apply_host(x, True, self._opts()), dtype=TYPE_DP)
+        self.M_linop = sla.LinearOperator((ln, ln), matvec=self.apply_L1_inverse_FT,
+                                          rmatvec=lambda x: self.apply_L1_inverse_FT(x, transpose=True), dtype=TYPE_DP)
+
+    def _l1_inverse_coefficients(self):
+        """Pair-sector coefficients of the inverse free propagator (DynamicalLanczos.py:2391-2502).
+        Pairs follow the packed order of psi: row-major upper triangle (mu <= nu), w_a = w[nu], w_b = w[mu]."""
+        n = self.n_modes
+        r, c = np.triu_indices(n)
+        w_a, w_b = self.w[c], self.w[r]
+        n_a = np.zeros(np.shape(w_a), dtype=TYPE_DP)
+        n_b = np.zeros(np.shape(w_a), dtype=TYPE_DP)
+        not_populated_a = 0.01 * w_a * __RyToK__ > self.T
+        not_populated_b = 0.01 * w_a * __RyToK__ > self.T      # the reference tests w_a for both (:2434)
+        if self.T > 0:
+            with np.errstate(over="ignore"):
+                n_a = 1 / (np.exp(w_a / np.double(self.T / __RyToK__)) - 1)
+                n_b = 1 / (np.exp(w_b / np.double(self.T / __RyToK__)) - 1)
+            n_a[not_populated_a] = 0
+            n_b[not_populated_b] = 0
+        X_ab = -w_a ** 2 - w_b ** 2 - (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+        Y_ab = -(8 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+        X1_ab = -(2 * n_a * n_b + n_a + n_b) * (2 * n_a * n_b + n_a + n_b + 1) * (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+        Y1_ab = -w_a ** 2 - w_b ** 2 + (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+        den = X_ab * Y1_ab - X1_ab * Y_ab
+        den_mask = den < __EPSILON__
+        den[den_mask] = np.inf
+        X_new, Y_new, X1_new, Y1_new = -Y1_ab / den, Y_ab / den, X1_ab / den, -X_ab / den
+        X_new[den_mask] = -1 / X_ab[den_mask]
+        if self.T > __EPSILON__:
+            new_mask = (w_a == w_b) & (n_a > __EPSILON__)
+            Y1_new[new_mask] = -1 / Y1_ab[new_mask]
+        return X_new, Y_new, X1_new, Y1_new
+
+    def apply_L1_inverse_FT(self, psi, transpose=False):
+        """Inverse of the harmonic (free) part of L, the preconditioner of the static solvers
+        (DynamicalLanczos.py:2391-2502); host, O(n^2)."""
+        n = self.n_modes
+        out = np.zeros(np.shape(self.psi), dtype=TYPE_DP)
+        if self.ignore_harmonic:
+            return out
+        psi = np.asarray(psi, dtype=TYPE_DP)
+        m = n * (n + 1) // 2
+        sY, sA = n, n + m
+        assert len(psi) == sA + m, ("ERROR, the initial vector for the Lanczos algorithm has a wrong dimension. "
+                                    "This may be caused by the Lanczos initialized at the wrong temperature.")
+        X_new, Y_new, X1_new, Y1_new = self._l1_inverse_coefficients()
+        out[:n] = (psi[:n] / self.w) / self.w
+        out[sY:sA] = X_new * psi[sY:sA]
+        if not transpose:
+            out[sY:sA] += Y_new * psi[sA:]
+            out[sA:] += X1_new * psi[sY:sA]
+        else:
+            out[sA:] += Y_new * psi[sY:sA]
+            out[sY:sA] += X1_new * psi[sA:]
+        out[sA:] += Y1_new * psi[sA:]
+        return out
+
+    def _bicgstab_batched(self, B, X0, rtol, maxiter, use_preconditioning, callback=None):
+        """BiCGSTAB for the columns of B (k, |psi|) at once on the device, one batched apply of the
+        still-active columns per operator application.  Per column it is scipy's bicgstab
+        (scipy.sparse.linalg, rtol / atol = 0 semantics, breakdown tolerances eps^2); returns the
+        solutions and scipy-style info codes (0 converged, maxiter, -10 / -11 breakdown)."""
+        torch = _torch()
+        dev = "cuda"
+        n = self.n_modes
+        m = n * (n + 1) // 2
+        opts = self._opts()
+        if use_preconditioning and not self.ignore_harmonic:
+            co = [torch.as_tensor(a, device=dev) for a in self._l1_inverse_coefficients()]
+            inv_w2 = torch.as_tensor(1.0 / self.w / self.w, device=dev)
+
+            def psolve(x):
+                y = torch.empty_like(x)
+                y[:, :n] = x[:, :n] * inv_w2
+                xY, xA = x[:, n:n + m], x[:, n + m:]
+                y[:, n:n + m] = co[0] * xY + co[1] * xA
+                y[:, n + m:] = co[2] * xY + co[3] * xA
+                return y
+        else:
+            def psolve(x):
+                return x.clone()
+
+        def matvec(x):
+            out = torch.empty_like(x)
+            self.device_ensemble.apply_full_L(x.contiguous(), out, [0] * x.shape[0], opts, self.precision)
+            return out
+
+        def dot(a, b):
+            return (a * b).sum(dim=1)
+
+        b = torch.as_tensor(np.asarray(B, dtype=TYPE_DP), device=dev)
+        x = torch.as_tensor(np.asarray(X0, dtype=TYPE_DP), device=dev).clone()
+        k = b.shape[0]
+        bnrm = torch.linalg.norm(b, dim=1)
+        atol = rtol * bnrm
+        info = np.full(k, maxiter, dtype=np.int64)
+        active = (bnrm > 0).cpu().numpy()
+        info[~active] = 0
+        r = b - matvec(x) if bool((x != 0).any()) else b.clone()
+        rt = r.clone()
+        p = torch.zeros_like(r)
+        v = torch.zeros_like(r)
+        rho_prev = torch.ones(k, dtype=torch.float64, device=dev)
+        alpha = torch.ones_like(rho_prev)
+        omega = torch.ones_like(rho_prev)
+        tiny = np.finfo(np.float64).eps ** 2
+        first = np.ones(k, dtype=bool)
+        for _ in range(maxiter):
+            done = (torch.linalg.norm(r, dim=1) < atol).cpu().numpy() & active
+            info[done] = 0
+            active &= ~done
+            idx = np.nonzero(active)[0]
+            if len(idx) == 0:
+                break
+            it = torch.as_tensor(idx, device=dev)
+            ra, rta = r[it], rt[it]
+            rho = dot(rta, ra)
+            bad = (rho.abs() < tiny).cpu().numpy()
+            om_bad = ((omega[it].abs() < tiny).cpu().numpy()) & ~first[idx]
+            info[idx[bad]] = -10
+            info[idx[om_bad & ~bad]] = -11
+            keep = ~(bad | om_bad)
+            active[idx[~keep]] = False
+            idx = idx[keep]
+            if len(idx) == 0:
+                continue
+            it = torch.as_tensor(idx, device=dev)
+            kt = torch.as_tensor(keep, device=dev)
+            rho, ra, rta = rho[kt], ra[kt], rta[kt]
+            fr = torch.as_tensor(first[idx], device=dev)
+            beta = torch.where(fr, torch.zeros_like(rho), (rho / rho_prev[it]) * (alpha[it] / omega[it]))
+            pa = torch.where(fr[:, None], ra, (p[it] - omega[it][:, None] * v[it]) * beta[:, None] + ra)
+            first[idx] = False
+            phat = psolve(pa)
+            va = matvec(phat)
+            rv = dot(rta, va)
+            zero_rv = (rv == 0).cpu().numpy()
+            if zero_rv.any():
+                info[idx[zero_rv]] = -11
+                active[idx[zero_rv]] = False
+            al = rho / torch.where(rv == 0, torch.ones_like(rv), rv)
+            sa = ra - al[:, None] * va
+            conv = (torch.linalg.norm(sa, dim=1) < atol[it]).cpu().numpy() & ~zero_rv
+            xa = x[it] + al[:, None] * phat
+            # columns that converged on s take x + alpha phat and stop here
+            cidx = np.nonzero(conv)[0]
+            if len(cidx):
+                ct = torch.as_tensor(cidx, device=dev)
+                x[it[ct]] = xa[ct]
+                info[idx[cidx]] = 0
+                active[idx[cidx]] = False
+            go = np.nonzero(~conv & ~zero_rv)[0]
+            p[it], v[it], alpha[it], rho_prev[it] = pa, va, al, rho
+            if len(go) == 0:
+                continue
+            gt = torch.as_tensor(go, device=dev)
+            ig = it[gt]
+            shat = psolve(sa[gt])
+            t = matvec(shat)
+            sg = sa[gt]
+            om = dot(t, sg) / dot(t, t)
+            omega[ig] = om
+            x[ig] = xa[gt] + om[:, None] * shat
+            r[ig] = sg - om[:, None] * t
+            if callback is not None:
+                callback(x)
+        return x.cpu().numpy(), info
+
+    def run_biconjugate_gradient(self, verbose=True, tol=5e-4, maxiter=1000, save_g=None, save_each=1,
+                                 use_preconditioning=True, algorithm="bicgstab", batched=True, batch=16):
+        """Static response by solving L x = e_i for every mode i (DynamicalLanczos.py:3761-3972);
+        returns G^-1, the mass-rescaled free energy Hessian.  ``batched`` (default) solves ``batch``
+        right-hand sides at a time with a device BiCGSTAB in which every operator application is
+        one batched GPU apply; ``batched=False`` runs scipy's solver (``algorithm`` bicgstab | bicg |
+        cg-minimize) with one GPU apply per matvec, as the reference does."""
+        import scipy.optimize
+        import scipy.sparse.linalg as sla
+        self._check_init()
+        if self.L_linop is None or self.M_linop is None:
+            self._make_linops()
+        n = self.n_modes
+        G_one_phonon = np.zeros((n, n), dtype=np.double)
+        if verbose:
+            print("\n====================\nBICONJUGATE GRADIENT\n====================\n")
+        if batched:
+            if algorithm.lower() != "bicgstab":
+                raise ValueError(f"batched=True runs bicgstab; got algorithm '{algorithm}' (pass batched=False)")
+            for i0 in range(0, n, batch):
+                cols = list(range(i0, min(n, i0 + batch)))
+                B = np.zeros((len(cols), len(self.psi)), dtype=TYPE_DP)
+                for q, i in enumerate(cols):
+                    B[q, i] = 1.0
+                X0 = np.stack([self.apply_L1_inverse_FT(bq) for bq in B])
+                t1 = time.time()
+                X, info = self._bicgstab_batched(B, X0, tol, maxiter, use_preconditioning)
+                if verbose:
+                    print(f"modes {cols[0] + 1}-{cols[-1] + 1} / {n}: solved in {time.time() - t1:.2f} s, info {info.tolist()}")
+                assert np.all(info >= 0), f"Error on input or breakdown of biconjugate gradient algorithm (info = {info})"
+                if verbose and np.any(info > 0):
+                    print(f"The biconjugate gradient did not converge after {maxiter} iterations for modes "
+                          f"{[cols[q] + 1 for q in np.nonzero(info > 0)[0]]}: reduce the tolerance or raise maxiter")
+                G_one_phonon[cols, :] = X[:, :n]
+                if save_g is not None:
+                    np.save(save_g, G_one_phonon)
+        else:
+            for i in range(n):
+                b = np.zeros(len(self.psi), dtype=TYPE_DP)
+                b[i] = 1
+                x0 = self.M_linop.matvec(b)
+                M_prec = self.M_linop if use_preconditioning else None
+                alg = algorithm.lower()
+                if alg == "bicgstab":
+                    res, info = sla.bicgstab(self.L_linop, b, x0=x0, rtol=tol, maxiter=maxiter, M=M_prec)
+                elif alg == "bicg":
+                    res, info = sla.bicg(self.L_linop, b, x0=x0, rtol=tol, maxiter=maxiter, M=M_prec)
+                elif alg == "cg-minimize":
+                    def func(x, bb):
+                        r = self.L_linop.matvec(x) - bb
+                        Hinv_r = self.M_linop.matvec(self.M_linop.rmatvec(r)) if use_preconditioning else r
+                        return 0.5 * np.sum(r * Hinv_r), self.L_linop.rmatvec(Hinv_r)
+                    opt = scipy.optimize.minimize(func, x0, args=(b.copy(),), method="bfgs", jac=True,
+                                                  options={"gtol": tol, "maxiter": maxiter, "disp": verbose, "norm": 2})
+                    res, info = opt.x.copy(), (0 if opt.success else 1)
+                else:
+                    raise ValueError(f"Error, algorithm type '{algorithm}' in subroutine run_biconjugate_gradient not "
+                                     "implemented. the only supported algorithms are ['bicgstab', 'bicg', 'cg-minimize']")
+                assert info >= 0, f"Error on input or breakdown of biconjugate gradient algorithm (info = {info})"
+                G_one_phonon[i, :] = res[:n]
+                if save_g is not None and i % save_each == 0:
+                    np.save(save_g, G_one_phonon)
+        if save_g is not None:
+            np.save(save_g, G_one_phonon)
+        disp = np.max(np.abs(G_one_phonon - G_one_phonon.T))
+        assert disp < 1e-4, "Error, the resulting one-phonon Green function is not Hermitian."
+        G = 0.5 * (G_one_phonon + G_one_phonon.T)
+        return np.linalg.inv(G)
+
+    def get_full_L_operator_FT(self, verbose=False, debug_d3=None, symmetrize=True, overwrite_L_operator=True,
+                               batch=64, max_bytes=16 << 30):
+        """The full L matrix (DynamicalLanczos.py:5454-5789), built column by column from batched
+        device applies of unit vectors, so it is exactly the operator that apply_full_L applies
+        (symmetrised averages, current flags).  Memory |psi|^2 x 8 B on the host."""
+        if debug_d3 is not None:
+            raise NotImplementedError("debug_d3: the explicit third-order tensor path is not part of the B200 mode")
+        torch = _torch()
+        self._check_init()
+        ln = len(self.psi)
+        if ln * ln * 8 > max_bytes:
+            raise MemoryError(f"the full L operator needs {ln * ln * 8 / 2**30:.1f} GiB (limit {max_bytes / 2**30:.1f} GiB)")
+        L = np.zeros((ln, ln), dtype=TYPE_DP)
+        opts = self._opts()
+        for c0 in range(0, ln, batch):
+            k = min(batch, ln - c0)
+            E = torch.zeros((k, ln), dtype=torch.float64, device="cuda")
+            E[torch.arange(k, device="cuda"), torch.arange(c0, c0 + k, device="cuda")] = 1.0
+            out = torch.empty_like(E)
+            self.device_ensemble.apply_full_L(E, out, [0] * k, opts, self.precision)
+            L[:, c0:c0 + k] = out.cpu().numpy().T
+        if overwrite_L_operator:
+            import scipy.sparse.linalg as sla
+            self.L_linop = sla.LinearOperator(L.shape, matvec=L.dot, rmatvec=L.T.dot, dtype=TYPE_DP)
+        return L
+
+    def run_full_diag(self, number, discard_dyn=True, n_iter=100):
+        """ARPACK (scipy eigsh) on L_linop (DynamicalLanczos.py:6381-6421)."""
+        import scipy.sparse.linalg as sla
+        self._check_init()
+        if self.L_linop is None:
+            self._make_linops()
+        eigvals, eigvects = sla.eigsh(self.L_linop, k=number, v0=self.psi, ncv=n_iter)
+        self.eigvals = eigvals
+        self.eigvects = eigvects
+        if discard_dyn:
+            eigvects = eigvects[:self.n_modes, :]
+        return eigvals, eigvects
+
+    def build_lanczos_matrix_from_coeffs(self, use_arnoldi=False):
+        """Tridiagonal (bi-conjugate: b below, c above the diagonal) Lanczos matrix, sign-reversed
+        and shifted like L (DynamicalLanczos.py:4571-4613)."""
+        N_size = len(self.a_coeffs)
+        matrix = np.zeros((N_size, N_size), dtype=TYPE_DP)
+        if not use_arnoldi:
+            for i in range(N_size):
+                matrix[i, i] = self.a_coeffs[i]
+                if i >= 1:
+                    c_coeff = self.b_coeffs[i - 1]
+                    if len(self.c_coeffs) == len(self.b_coeffs):
+                        c_coeff = self.c_coeffs[i - 1]
+                    matrix[i - 1, i] = c_coeff
+                    matrix[i, i - 1] = self.b_coeffs[i - 1]
+        else:
+            assert len(self.b_coeffs) > len(self.c_coeffs), "Error, cannot Arnoldi with non-symmetric Lanczos not implemented"
+            for i in range(N_size):
+                matrix[:i + 1, i] = self.arnoldi_matrix[i]
+                matrix[i, :i + 1] = self.arnoldi_matrix[i]
+        sign = -1 if self.reverse_L else 1
+        return sign * matrix - sign * np.eye(N_size) * self.shift_value
+
+    def get_static_frequency(self, smearing=0):
+        """sqrt(1 / Re G(omega -> 0 + i eta)), negative when imaginary (DynamicalLanczos.py:5273-5307)."""
+        gf = self.get_green_function_continued_fraction(np.array([0]), False, smearing=smearing)
+        w2 = 1 / np.real(gf[0])
+        return np.float64(np.sqrt(np.abs(w2)) * np.sign(w2))
 
     # ---- checkpoints (DynamicalLanczos.py:3597-3758) -----------------------------------------
     def save_status(self, file):
