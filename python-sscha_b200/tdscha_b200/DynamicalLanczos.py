@@ -18,9 +18,11 @@ Differences from the reference that a user sees:
 from __future__ import annotations
 
 import difflib
+import json
 import os
 import sys
 import time
+import warnings
 
 import numpy as np
 
@@ -645,6 +647,88 @@ class Lanczos(object):
         gf = self.get_green_function_continued_fraction(np.array([0]), False, smearing=smearing)
         w2 = 1 / np.real(gf[0])
         return np.float64(np.sqrt(np.abs(w2)) * np.sign(w2))
+
+    # ---- input / output files of the stand-alone Lanczos program (DynamicalLanczos.py:815-1000,
+    #      3572-3595; CModules/Lanczos.cpp:47-269, 533-800) ---------------------------------------
+    def prepare_input_files(self, root_name="tdscha", n_steps=100, start_from_scratch=True, directory=".", run_symm=False):
+        """Write <root>.json, .ndegs, .blockid, .masses, .freqs, .rho, .X.dat, .Y.dat, .psi,
+        .block<i>, .symsb<i> for the stand-alone program (tdscha_lanczos_b200 here, tdscha-lanczos.x
+        in the reference), in the reference's formats."""
+        Nsyms = np.shape(self.symmetries[0])[0]
+        json_data = {"T": self.T, "n_steps": n_steps, "ignore_v2": self.ignore_harmonic, "ignore_v3": self.ignore_v3,
+                     "ignore_v4": self.ignore_v4, "use_wigner": self.use_wigner, "run_sym": run_symm,
+                     "data": {"n_configs": int(self.N), "n_modes": int(self.n_modes), "n_syms": int(Nsyms),
+                              "n_blocks": len(self.symmetries), "perturbation_modulus": float(self.perturbation_modulus),
+                              "reverse": bool(self.reverse_L), "shift": float(self.shift_value)}}
+        if not start_from_scratch:
+            raise NotImplementedError("Error, restarting from a previous calculation is not yet implemented.")
+        root_fname = os.path.join(directory, root_name)
+        os.makedirs(directory, exist_ok=True)
+        with open(root_fname + ".json", "w") as fp:
+            json.dump(json_data, fp)
+        np.savetxt(root_fname + ".ndegs", self.N_degeneracy, fmt="%d")
+        np.savetxt(root_fname + ".blockid", self.sym_block_id, fmt="%d")
+        np.savetxt(root_fname + ".masses", self.m)
+        np.savetxt(root_fname + ".freqs", self.w)
+        np.savetxt(root_fname + ".rho", self.rho)
+        np.savetxt(root_fname + ".X.dat", self.X)
+        np.savetxt(root_fname + ".Y.dat", self.Y)
+        np.savetxt(root_fname + ".psi", self.psi)
+        for i in range(len(self.symmetries)):
+            np.savetxt(root_fname + ".block{:d}".format(i), self.degenerate_space[i], fmt="%d")
+            ns, b1, b2 = self.symmetries[i].shape
+            with open(root_fname + ".symsb{:d}".format(i), "w") as fp:
+                for isym in range(ns):
+                    for k1 in range(b1):
+                        fp.write("".join(" {:22.16f}".format(v) for v in self.symmetries[i][isym, k1]))
+                        fp.write("\n")
+                    fp.write("\n")
+
+    def load_from_input_files(self, root_name="tdscha", directory="."):
+        """Read the program's results (<root>.abc, and .qbasis.out / .pbasis.out / .snorm.out when
+        present) and the general variables of <root>.json."""
+        if not os.path.exists(directory):
+            raise IOError("Error, the specified directory '{}' does not exist".format(directory))
+        abc_file = os.path.join(directory, "{}.abc".format(root_name))
+        if not os.path.exists(abc_file):
+            raise IOError(f"Error, the file '{abc_file}' does not exist. please, check if you correctly run the "
+                          "stand-alone Lanczos program.")
+        data_abc = np.loadtxt(abc_file, dtype=np.double)
+        self.a_coeffs = data_abc[:, 0]
+        self.b_coeffs = data_abc[:, 1]
+        self.c_coeffs = data_abc[:, 2]
+        for attr, suffix in (("basis_Q", "qbasis.out"), ("basis_P", "pbasis.out"), ("s_norm", "snorm.out")):
+            fname = os.path.join(directory, "{}.{}".format(root_name, suffix))
+            if os.path.exists(fname):
+                v = np.loadtxt(fname, dtype=np.double)
+                setattr(self, attr, v.ravel() if attr == "s_norm" else v)
+            else:
+                warnings.warn(f"File {fname} not found. {attr} not loaded.")
+        with open(os.path.join(directory, root_name + ".json"), "r") as fp:
+            json_data = json.load(fp)
+        self.perturbation_modulus = json_data["data"]["perturbation_modulus"]
+        self.T = json_data["T"]
+        self.ignore_harmonic = json_data["ignore_v2"]
+        self.ignore_v3 = json_data["ignore_v3"]
+        self.ignore_v4 = json_data["ignore_v4"]
+        self.N = json_data["data"]["n_configs"]
+        self.n_modes = json_data["data"]["n_modes"]
+        self.reverse_L = json_data["data"]["reverse"]
+        self.shift_value = json_data["data"]["shift"]
+
+    def save_abc(self, file):
+        total_len = len(self.c_coeffs)
+        abc = np.zeros((total_len, 3), dtype=np.double)
+        abc[:, 0] = self.a_coeffs[:total_len]
+        abc[:, 1] = self.b_coeffs
+        abc[:, 2] = self.c_coeffs
+        np.savetxt(file, abc, header="a; b; c")
+
+    def load_abc(self, file):
+        abc = np.loadtxt(file)
+        self.a_coeffs = abc[:, 0]
+        self.b_coeffs = abc[:, 1]
+        self.c_coeffs = abc[:, 2]
 
     # ---- checkpoints (DynamicalLanczos.py:3597-3758) -----------------------------------------
     def save_status(self, file):

@@ -20,6 +20,8 @@ CSRC = os.path.join(ROOT, "csrc")
 INCLUDE = os.path.join(REPO, "include")
 LIB_DIR = os.path.join(PKG_DIR, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libtdscha_b200.so")
+DRIVER_SRC = os.path.join(ROOT, "driver", "tdscha_lanczos_b200.cpp")
+DRIVER_PATH = os.path.join(LIB_DIR, "tdscha_lanczos_b200")
 OBJ_DIR = os.path.join(ROOT, "_build")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -71,7 +73,20 @@ def build(verbose=False, force=False):
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)
+    build_driver(verbose=verbose, force=force)
     return LIB_PATH
+
+
+def build_driver(verbose=False, force=False):
+    """The stand-alone Lanczos program (driver/tdscha_lanczos_b200.cpp), linked against the library."""
+    deps = [DRIVER_SRC, LIB_PATH] + glob.glob(os.path.join(INCLUDE, "*.h"))
+    if force or _stale(DRIVER_PATH, deps):
+        cmd = [_nvcc(), "-std=c++17", "-O2"] + ARCH + ["-I", INCLUDE, DRIVER_SRC, "-o", DRIVER_PATH, "-L", LIB_DIR, "-ltdscha_b200",
+               "-Xlinker", "-rpath=$ORIGIN"]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+    return DRIVER_PATH
 
 
 if __name__ == "__main__":
