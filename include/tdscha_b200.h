@@ -203,6 +203,26 @@ int tdscha_read_profile(tdscha_ensemble *ens, double *ms, long long *launches, i
 int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, const void *A_lo, long long lda,
                        const void *B_hi, const void *B_lo, long long ldb, float *D, long long ldd, void *stream);
 
+/*
+ * Inputs of the Lanczos from an ensemble, computed on the GPU (host buffers in and out).
+ *
+ * tdscha_project_ensemble: X = (u o sqrt(m)) . pols and Y = (f / sqrt(m)) . pols, the
+ * mass-rescaled displacements and forces in the polarisation basis -- the projection at
+ * Modules/DynamicalLanczos.py:431-435 (u in Bohr, f in Ry/Bohr after the reference's subtraction
+ * of the SSCHA and mean forces, :389-425).  u, f (N, 3 nat); masses (3 nat); pols (3 nat, n);
+ * X_out, Y_out (N, n); all C order, FP64.
+ *
+ * tdscha_symmetries_on_modes: the symmetry group on the degenerate blocks of the modes,
+ * S_b^j = E_b^T P_j E_b (N_sym, d_b, d_b) per block, with (P_j v)[perm_j(a)] = R_j v[a] on
+ * mass-weighted displacements.  This replaces the tables that DynamicalLanczos.py:749-756
+ * takes from cellconstructor's GetSymmetriesOnModesDeg.  perm (N_sym, nat) image atoms, rot
+ * (N_sym, 3, 3) Cartesian rotations, pols (3 nat, n); blocks of at most 80 modes.
+ */
+int tdscha_project_ensemble(const double *u, const double *f, const double *masses, const double *pols, int N,
+                            int nat3, int n, double *X_out, double *Y_out);
+int tdscha_symmetries_on_modes(const double *pols, int nat, int n, int N_sym, const int *perm, const double *rot,
+                               int n_blocks, const int *n_deg, const int *const *deg_space, double *const *sym_out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,6 +6,7 @@
 
 #include "common.cuh"
 #include "ensemble.cuh"
+#include "modes.cuh"
 #include "tc_gemm.cuh"
 
 namespace tdscha {
@@ -267,3 +268,16 @@ int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, con
 }
 
 }  // extern "C"
+
+extern "C" int tdscha_project_ensemble(const double *u, const double *f, const double *masses, const double *pols, int N,
+                                       int nat3, int n, double *X_out, double *Y_out) {
+    clear_error();
+    return tdscha::project_ensemble(u, f, masses, pols, N, nat3, n, X_out, Y_out);
+}
+
+extern "C" int tdscha_symmetries_on_modes(const double *pols, int nat, int n, int N_sym, const int *perm, const double *rot,
+                                          int n_blocks, const int *n_deg, const int *const *deg_space,
+                                          double *const *sym_out) {
+    clear_error();
+    return tdscha::symmetries_on_modes(pols, nat, n, N_sym, perm, rot, n_blocks, n_deg, deg_space, sym_out);
+}

@@ -67,6 +67,9 @@ def load():
                                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp]
     lib.tdscha_tc_contract.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_longlong,
                                        vp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, vp]
+    lib.tdscha_project_ensemble.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
+    lib.tdscha_symmetries_on_modes.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, dp, ctypes.c_int, ip,
+                                               ctypes.POINTER(ip), ctypes.POINTER(dp)]
     lib.tdscha_apply_prologue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp]
     lib.tdscha_apply_epilogue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp, vp]
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
@@ -267,3 +270,40 @@ def get_perturb_average_sym(X, Y, w, rho, R1, Y1, T, apply_D4, N_syms, sym_list,
     check(lib.tdscha_GetPerturbAverageSym(_d(X), _d(Y), _d(w), _d(rho), _d(R1), _d(Y1), float(T), int(apply_D4),
                                           int(N_syms), len(syms), sym_ptrs, _i(n_deg), deg_ptrs, _i(bid), N, n,
                                           _d(f_out), _d(d2v_out)))
+
+
+def project_ensemble(u, f, masses, pols):
+    """X = (u o sqrt(m)) . pols, Y = (f / sqrt(m)) . pols on the GPU (tdscha_project_ensemble)."""
+    lib = load()
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    f = np.ascontiguousarray(f, dtype=np.float64)
+    m = np.ascontiguousarray(masses, dtype=np.float64)
+    P = np.ascontiguousarray(pols, dtype=np.float64)
+    N, nat3 = u.shape
+    if f.shape != u.shape or m.shape != (nat3,) or P.shape[0] != nat3:
+        raise ValueError(f"shapes: u {u.shape}, f {f.shape}, masses {m.shape}, pols {P.shape}")
+    n = P.shape[1]
+    X = np.empty((N, n))
+    Y = np.empty((N, n))
+    check(lib.tdscha_project_ensemble(_d(u), _d(f), _d(m), _d(P), N, nat3, n, _d(X), _d(Y)))
+    return X, Y
+
+
+def symmetries_on_modes(pols, perm, rot, deg_space):
+    """Per degenerate block the (N_sym, d, d) tables S_b^j = E_b^T P_j E_b on the GPU
+    (tdscha_symmetries_on_modes); perm (N_sym, nat) image atoms, rot (N_sym, 3, 3)."""
+    lib = load()
+    P = np.ascontiguousarray(pols, dtype=np.float64)
+    perm = np.ascontiguousarray(perm, dtype=np.intc)
+    rot = np.ascontiguousarray(rot, dtype=np.float64)
+    N_sym, nat = perm.shape
+    if rot.shape != (N_sym, 3, 3) or P.shape[0] != 3 * nat:
+        raise ValueError(f"shapes: perm {perm.shape}, rot {rot.shape}, pols {P.shape}")
+    degs = [np.ascontiguousarray(d, dtype=np.intc) for d in deg_space]
+    out = [np.empty((N_sym, len(d), len(d))) for d in degs]
+    n_deg = np.array([len(d) for d in degs], dtype=np.intc)
+    deg_ptrs = (ip * len(degs))(*[_i(d) for d in degs])
+    out_ptrs = (dp * len(out))(*[_d(o) for o in out])
+    check(lib.tdscha_symmetries_on_modes(_d(P), nat, P.shape[1], N_sym, _i(perm), _d(rot), len(degs), _i(n_deg), deg_ptrs,
+                                         out_ptrs))
+    return out
