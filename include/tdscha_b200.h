@@ -204,6 +204,19 @@ int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, con
                        const void *B_hi, const void *B_lo, long long ldb, float *D, long long ldd, void *stream);
 
 /*
+ * Vector-Jacobian product of the averages (the outputs of tdscha_perturb_average_sym_device)
+ * with respect to the ensemble's forces Y and weights rho -- the building block of dG(w)/dY,
+ * dG(w)/drho (the reference has no derivatives; no counterpart there).  For nb perturbations
+ * (R1 (nb, n), Ys (nb, n, n) symmetric, device) and cotangents fbar (nb, n), Dbar (nb, n, n)
+ * symmetric (device) it writes, summed over the nb vectors,
+ *   Ybar (N, n)  = d[ sum_k <fbar_k, f_k> + <Dbar_k, D_k>_F ] / dY,   rhobar (N) = the same / drho
+ * (device buffers, overwritten).  FP64 throughout; N_eff = sum(rho) is differentiated too.
+ */
+int tdscha_perturb_average_vjp_device(tdscha_ensemble *ens, int nb, const double *R1, const double *Ys, int apply_d4,
+                                      const double *fbar, const double *Dbar, double *Ybar, double *rhobar,
+                                      void *stream);
+
+/*
  * Inputs of the Lanczos from an ensemble, computed on the GPU (host buffers in and out).
  *
  * tdscha_project_ensemble: X = (u o sqrt(m)) . pols and Y = (f / sqrt(m)) . pols, the

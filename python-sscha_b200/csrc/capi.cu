@@ -281,3 +281,13 @@ extern "C" int tdscha_symmetries_on_modes(const double *pols, int nat, int n, in
     clear_error();
     return tdscha::symmetries_on_modes(pols, nat, n, N_sym, perm, rot, n_blocks, n_deg, deg_space, sym_out);
 }
+
+extern "C" int tdscha_perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                                                 const double *fbar, const double *Dbar, double *Ybar, double *rhobar,
+                                                 void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    return tdscha::perturb_average_vjp_device(e, nb, R1, Ys, apply_d4, fbar, Dbar, Ybar, rhobar,
+                                              static_cast<cudaStream_t>(stream));
+}

@@ -381,7 +381,8 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaSetDevice(e->device);
     cudaDeviceSynchronize();
     void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->symP, e->symPT, e->d_offP, e->d_blk_start, e->d_blk_dim,
-                  e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base};
+                  e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base,
+                  e->vjp_ws.base, e->YX};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);
@@ -571,6 +572,215 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     StageScope sc(e, ST_OTHER, st);
     fold_reduce_kernel<<<grid_for((long long)nb * e->n * e->n), 256, 0, st>>>(partD, partF, nf_total, e->n, nb, e->d_blocks_ids,
                                                                                norm, d_out, f_out);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// ================================================================================================
+// Vector-Jacobian product of the averages w.r.t. (Y, rho).
+//
+// With the forward quantities per (row r = (k, j), configuration i): a, b = [a|b], c, d = [c|d],
+// weights gamma = rho (-c/3 + d4 a/8), delta = rho (-d/3 + d4 b/4), alpha = -rho a/6,
+// beta = -rho b/3, the pairing <fbar, f_av> + <Dbar, D_av> equals
+//   norm sum_{r,i} rho_i [ delta'/2 A' + gamma' B' + alpha' C' + beta' D' ]      (primes: rho_i = 1)
+// where [A'|B'] = Q . V^T with Q_j[p] = 2 ups_mu ups_nu (S_j^T Dbar S_j)[mu nu] (packed) and
+// [C'|D'] = phi . [Y; X~]^T with phi_j = S_j^T fbar; Q and phi come from the symmetry transform of
+// (2 ups ups Dbar, fbar / ups) (ups is constant on a degenerate block).  Y enters through
+// g = psi o y (second half of V, d = r1 . g) and directly through C' = phi . y:
+//   Vbar[N+i, :] = sum_r K1_ri B1_r + K2_ri Q_r,  K1 = d4 A'/8 - D'/3, K2 = -c/3 + d4 a/8
+//   gbar_i       = (d V[N+i] / d g_i)^T Vbar[N+i] + sum_r K3_ri r1_r,  K3 = -A'/6
+//   Ybar_i       = norm rho_i (psi o gbar_i + sum_r K4_ri phi_r),  K4 = -a/6
+//   rhobar_i     = norm sum_r BR_ri - Phi / N_eff,  Phi = norm sum_{r,i} rho_i BR_ri
+// ================================================================================================
+__global__ void vjp_cotangent_kernel(int nb, int n, const double *__restrict__ fbar, const double *__restrict__ Dbar,
+                                     const double *__restrict__ ups, double *__restrict__ Rq, double *__restrict__ Dq) {
+    const long long nn = (long long)n * n, total = (long long)nb * nn;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long e = idx % nn;
+        const int mu = (int)(e / n), nu = (int)(e % n);
+        Dq[idx] = 2.0 * ups[mu] * ups[nu] * Dbar[idx];
+        if (e < n) Rq[(idx / nn) * n + e] = fbar[(idx / nn) * n + e] / ups[e];
+    }
+}
+
+__global__ void build_YX_kernel(const double *Y, const double *Xt, int N, int n, long long np, double *YX) {
+    const long long total = 2LL * N * np;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx / np, m = idx % np;
+        YX[idx] = m < n ? ((k < N) ? Y[k * n + m] : Xt[(k - N) * n + m]) : 0.0;
+    }
+}
+
+__global__ void vjp_coef_kernel(long long M, int N, long long ld, const double *__restrict__ D1, const double *__restrict__ Dcd,
+                                const double *__restrict__ DA, const double *__restrict__ DC, int d4, double *__restrict__ K1,
+                                double *__restrict__ K2, double *__restrict__ K3, double *__restrict__ K4, double *__restrict__ BR) {
+    const long long total = M * N;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / N, i = idx % N;
+        const double a = D1[r * ld + i], b = D1[r * ld + N + i], c = Dcd[r * ld + i], d = Dcd[r * ld + N + i];
+        const double Ap = DA[r * ld + i], Bp = DA[r * ld + N + i], Cp = DC[r * ld + i], Dp = DC[r * ld + N + i];
+        const double k2 = -c / 3.0 + (d4 ? a / 8.0 : 0.0);
+        K1[idx] = (d4 ? Ap / 8.0 : 0.0) - Dp / 3.0;
+        K2[idx] = k2;
+        K3[idx] = -Ap / 6.0;
+        K4[idx] = -a / 6.0;
+        BR[idx] = 0.5 * (-d / 3.0 + (d4 ? b / 4.0 : 0.0)) * Ap + k2 * Bp - a / 6.0 * Cp - b / 3.0 * Dp;
+    }
+}
+
+// colsum[i] += sum_r BR[r][i]
+__global__ void vjp_colsum_kernel(long long M, int N, const double *__restrict__ BR, double *__restrict__ colsum) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double s = 0.0;
+    for (long long r = 0; r < M; ++r) s += BR[r * N + i];
+    colsum[i] += s;
+}
+
+// gbar_i += d/dg_i sum_p Vbar[i][p] V[N+i][p] with V[N+i][(mu nu)] = x_mu g_nu + x_nu g_mu off the
+// diagonal and x_mu g_mu on it; one CTA per i, one warp per row mu of the packed triangle
+__global__ void vjp_matvec_kernel(int N, int n, long long Kp, long long np, const double *__restrict__ Vbar,
+                                  const double *__restrict__ X, double *__restrict__ gbar) {
+    extern __shared__ double gs[];
+    const int i = blockIdx.x;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const double *x = X + (long long)i * n;
+    const double *vb = Vbar + (long long)i * Kp;
+    for (int m = threadIdx.x; m < n; m += blockDim.x) gs[m] = 0.0;
+    __syncthreads();
+    for (int mu = warp; mu < n; mu += nw) {
+        const long long row = (long long)mu * n - ((long long)mu * (mu - 1)) / 2 - mu;   // + nu gives pair(mu, nu)
+        const double xm = x[mu];
+        double own = 0.0;
+        for (int nu = mu + lane; nu < n; nu += 32) {
+            const double v = vb[row + nu];
+            if (nu == mu) {
+                own += v * xm;   // V[N+i, (mu mu)] = x_mu g_mu
+            } else {
+                own += v * x[nu];
+                atomicAdd(&gs[nu], v * xm);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1) own += __shfl_down_sync(0xffffffffu, own, o);
+        if (lane == 0) atomicAdd(&gs[mu], own);
+    }
+    __syncthreads();
+    for (int m = threadIdx.x; m < n; m += blockDim.x) gbar[(long long)i * np + m] += gs[m];
+}
+
+__global__ void vjp_final_kernel(int N, int n, long long np, double norm, const double *__restrict__ rho,
+                                 const double *__restrict__ psi, const double *__restrict__ gbar, const double *__restrict__ ypart,
+                                 double *__restrict__ Ybar) {
+    const long long total = (long long)N * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+         idx += (long long)gridDim.x * blockDim.x) {
+        const long long i = idx / n, m = idx % n;
+        Ybar[idx] = norm * rho[i] * (psi[m] * gbar[i * np + m] + ypart[i * np + m]);
+    }
+}
+
+// Phi = norm sum_i rho_i colsum_i (one CTA, deterministic), rhobar_i = norm colsum_i - Phi / N_eff
+__global__ void vjp_rho_kernel(int N, double norm, double N_eff, const double *__restrict__ rho,
+                               const double *__restrict__ colsum, double *__restrict__ rhobar) {
+    __shared__ double red[256];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s += rho[i] * colsum[i];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if ((int)threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+        __syncthreads();
+    }
+    const double Phi = norm * red[0];
+    for (int i = threadIdx.x; i < N; i += blockDim.x) rhobar[i] = norm * colsum[i] - Phi / N_eff;
+}
+
+// row-major C (N x K) (+)= A^T B with A (M x N), B (M x K) row-major
+static int gemm_atb(tdscha_ensemble *e, const double *A, long long lda, const double *B, long long ldb, long long M, long long N,
+                    long long K, double *C, long long ldc, bool accumulate, cudaStream_t st) {
+    const double one = 1.0, beta = accumulate ? 1.0 : 0.0;
+    cublasSetStream(e->cublas, st);
+    cublasStatus_t s = cublasDgemm(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, (int)K, (int)N, (int)M, &one, B, (int)ldb, A, (int)lda,
+                                   &beta, C, (int)ldc);
+    TD_CHECK(s == CUBLAS_STATUS_SUCCESS, TDSCHA_ECUDA, "cublasDgemm failed (%d)", (int)s);
+    return 0;
+}
+
+int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+    TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);
+    TD_CHECK(R1 && Ys && fbar && Dbar && Ybar && rhobar, TDSCHA_EINVAL, "NULL argument");
+    TD_TRY(ensure_operands(e, FMT_F64, false, st));
+    OperandSet &o = e->ops[FMT_F64];
+    const int N = e->N, n = e->n;
+    if (!e->YX) {
+        TD_CUDA(cudaMalloc(&e->YX, (size_t)e->N2 * e->np * sizeof(double)));
+        build_YX_kernel<<<grid_for(e->N2 * e->np), 256, 0, st>>>(e->Y, e->Xt, N, n, e->np, e->YX);
+        TD_CUDA(cudaGetLastError());
+    }
+    const long long ld1 = round_up(e->N2, 4);
+    // persistent buffers, then per-chunk rows (M = nb * Jc)
+    const size_t fixed = 8 * ((size_t)N * e->Kp + 2 * (size_t)N * e->np + N + (size_t)nb * n + (size_t)nb * n * n) + 8 * 256;
+    const size_t per_row = 8 * (2 * (size_t)e->Kp + 2 * (size_t)e->np + 4 * (size_t)ld1 + 5 * (size_t)N);
+    size_t free_b = 0, tot_b = 0;
+    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    const size_t budget = std::max<size_t>((size_t)1 << 30, (size_t)((free_b + e->vjp_ws.bytes) * 0.5));
+    TD_CHECK(budget > fixed + per_row * nb, TDSCHA_ENOMEM, "not enough device memory for the averages' VJP");
+    int Jc = std::min<long long>(e->N_sym, (long long)((budget - fixed) / (per_row * nb)));
+    Jc = std::max(1, Jc);
+    const size_t need = fixed + per_row * (size_t)nb * Jc + 16 * 256;
+    if (e->vjp_ws.bytes < need) {
+        if (e->vjp_ws.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->vjp_ws.base); e->vjp_ws = Workspace(); }
+        TD_CUDA(cudaMalloc(&e->vjp_ws.base, need));
+        e->vjp_ws.bytes = need;
+    }
+    uint8_t *W = static_cast<uint8_t *>(e->vjp_ws.base);
+    size_t off = 0;
+    auto take = [&](size_t count) { double *p = reinterpret_cast<double *>(W + off); off += (count * 8 + 255) / 256 * 256; return p; };
+    double *Vbar = take((size_t)N * e->Kp), *gbar = take((size_t)N * e->np), *ypart = take((size_t)N * e->np);
+    double *colsum = take(N), *Rq = take((size_t)nb * n), *Dq = take((size_t)nb * n * n);
+    const long long Mmax = (long long)nb * Jc;
+    double *B1 = take(Mmax * e->Kp), *Q = take(Mmax * e->Kp), *r1 = take(Mmax * e->np), *phi = take(Mmax * e->np);
+    double *D1 = take(Mmax * ld1), *Dcd = take(Mmax * ld1), *DA = take(Mmax * ld1), *DC = take(Mmax * ld1);
+    double *K1 = take(Mmax * N), *K2 = take(Mmax * N), *K3 = take(Mmax * N), *K4 = take(Mmax * N), *BR = take(Mmax * N);
+    TD_CUDA(cudaMemsetAsync(gbar, 0, (size_t)N * e->np * 8, st));
+    TD_CUDA(cudaMemsetAsync(ypart, 0, (size_t)N * e->np * 8, st));
+    TD_CUDA(cudaMemsetAsync(colsum, 0, (size_t)N * 8, st));
+    vjp_cotangent_kernel<<<grid_for((long long)nb * n * n), 256, 0, st>>>(nb, n, fbar, Dbar, e->ups, Rq, Dq);
+    TD_CUDA(cudaGetLastError());
+
+    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->symP, e->symPT, e->d_offP};
+    bool first = true;
+    for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
+        const int nj = std::min(Jc, e->N_sym - j0);
+        const long long M = (long long)nb * nj;
+        TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, e->Kp, e->np, FMT_F64, B1, nullptr, r1, nullptr,
+                             false, st));
+        TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Dq, Rq, e->ups, e->P, e->Kp, e->np, FMT_F64, Q, nullptr, phi, nullptr,
+                             false, st));
+        TD_TRY(gemm_abt(e, FMT_F64, 1, B1, nullptr, e->Kp, M, o.V_hi, nullptr, e->Kp, e->N2, e->Kp, D1, ld1, st));
+        TD_TRY(gemm_abt(e, FMT_F64, 1, r1, nullptr, e->np, M, o.XG_hi, nullptr, e->np, e->N2, e->np, Dcd, ld1, st));
+        TD_TRY(gemm_abt(e, FMT_F64, 1, Q, nullptr, e->Kp, M, o.V_hi, nullptr, e->Kp, e->N2, e->Kp, DA, ld1, st));
+        TD_TRY(gemm_abt(e, FMT_F64, 1, phi, nullptr, e->np, M, e->YX, nullptr, e->np, e->N2, e->np, DC, ld1, st));
+        vjp_coef_kernel<<<grid_for(M * N), 256, 0, st>>>(M, N, ld1, D1, Dcd, DA, DC, apply_d4, K1, K2, K3, K4, BR);
+        TD_CUDA(cudaGetLastError());
+        TD_TRY(gemm_atb(e, K1, N, B1, e->Kp, M, N, e->Kp, Vbar, e->Kp, !first, st));
+        TD_TRY(gemm_atb(e, K2, N, Q, e->Kp, M, N, e->Kp, Vbar, e->Kp, true, st));
+        TD_TRY(gemm_atb(e, K3, N, r1, e->np, M, N, e->np, gbar, e->np, true, st));
+        TD_TRY(gemm_atb(e, K4, N, phi, e->np, M, N, e->np, ypart, e->np, true, st));
+        vjp_colsum_kernel<<<ceil_div(N, 256), 256, 0, st>>>(M, N, BR, colsum);
+        TD_CUDA(cudaGetLastError());
+        first = false;
+    }
+    const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
+    vjp_matvec_kernel<<<N, 256, (size_t)n * sizeof(double), st>>>(N, n, e->Kp, e->np, Vbar, e->X, gbar);
+    vjp_final_kernel<<<grid_for((long long)N * n), 256, 0, st>>>(N, n, e->np, norm, e->rho, e->psi, gbar, ypart, Ybar);
+    vjp_rho_kernel<<<1, 256, 0, st>>>(N, norm, e->N_eff, e->rho, colsum, rhobar);
     TD_CUDA(cudaGetLastError());
     return 0;
 }

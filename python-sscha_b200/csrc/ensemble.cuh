@@ -82,6 +82,8 @@ struct tdscha_ensemble {
     unsigned *d_err = nullptr;
     tdscha::OperandSet ops[3];                     // indexed by Format
     tdscha::Workspace ws;
+    tdscha::Workspace vjp_ws;                      // workspace of the averages' VJP
+    double *YX = nullptr;                          // [Y; X~] (2N x np), FP64, built by the first VJP
     cublasHandle_t cublas = nullptr;
     size_t base_bytes = 0;
     tdscha::Profile prof;
@@ -98,6 +100,13 @@ int ensemble_destroy(tdscha_ensemble *e);
 // nb perturbations, device pointers.  Ys: (nb, n, n) SYMMETRIC upsilon; R1: (nb, n).
 int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
                            int precision, double *f_out, double *d_out, cudaStream_t st);
+
+// Vector-Jacobian product of the averages with respect to the ensemble's forces Y and weights rho:
+// for cotangents (fbar, Dbar) of (f_av, D_av) at the perturbations (R1, Ys), writes
+//   Ybar (N, n) = d<fbar, f_av> + <Dbar, D_av> / dY,   rhobar (N) = same / drho   (summed over nb)
+// FP64 throughout.  Dbar must be symmetric (the Frobenius product is used).
+int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st);
 
 // (nb, n, n) -> (Y + Y^T)/2 on the device
 int symmetrize_device(int nb, int n, const double *Y, double *Ys, cudaStream_t st);

@@ -67,6 +67,7 @@ def load():
                                                      ctypes.c_int, ctypes.c_double, ctypes.c_double, vp, vp]
     lib.tdscha_tc_contract.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_longlong,
                                        vp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, vp]
+    lib.tdscha_perturb_average_vjp_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, vp, vp, vp]
     lib.tdscha_project_ensemble.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
     lib.tdscha_symmetries_on_modes.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, dp, ctypes.c_int, ip,
                                                ctypes.POINTER(ip), ctypes.POINTER(dp)]
@@ -165,6 +166,14 @@ class DeviceEnsemble:
         check(self._lib.tdscha_perturb_average_sym_device(self.handle, nb, R1.data_ptr(), Y1.data_ptr(), int(apply_d4),
                                                           PREC[precision], f_out.data_ptr(), d_out.data_ptr(),
                                                           _stream_ptr(stream)))
+
+    def perturb_average_vjp(self, R1, Ys, fbar, Dbar, Ybar, rhobar, apply_d4=1, stream=None):
+        """d[sum_k <fbar_k, f_k> + <Dbar_k, D_k>] / d(Y, rho) into Ybar (N, n), rhobar (N); all float64
+        CUDA tensors, Ys and Dbar symmetric (nb, n, n)."""
+        nb = R1.shape[0]
+        check(self._lib.tdscha_perturb_average_vjp_device(self.handle, nb, R1.data_ptr(), Ys.data_ptr(), int(apply_d4),
+                                                          fbar.data_ptr(), Dbar.data_ptr(), Ybar.data_ptr(),
+                                                          rhobar.data_ptr(), _stream_ptr(stream)))
 
     def apply_full_L(self, psi, out, transpose, opts, precision="fp64", stream=None):
         """psi, out: (nb, len) float64 CUDA tensors; transpose: sequence of nb ints."""

@@ -237,6 +237,19 @@ def sample_ensemble(sys_: RockSaltSystem, N, seed=0, chunk=2000):
     return np.ascontiguousarray(X), np.ascontiguousarray(Y), rho
 
 
+def sample_force_components(sys_: RockSaltSystem, N, seed=0):
+    """The ensemble of sample_ensemble (same seed, same X) with its forces split by coupling:
+    Y = k3 Y3 + k4 Y4 (internal Ry/Bohr units of k3, k4).  Returns X, Y3, Y4, rho."""
+    import dataclasses
+    X, _, rho = sample_ensemble(sys_, N, seed=seed)
+    out = []
+    for k3, k4 in ((1.0, 0.0), (0.0, 1.0)):
+        part = dataclasses.replace(sys_, k3=k3, k4=k4)
+        _, Yk, _ = sample_ensemble(part, N, seed=seed)
+        out.append(Yk)
+    return X, out[0], out[1], rho
+
+
 def random_born_charges(nat_uc=2, seed=0):
     """Z*[atom, field, cart] ~ N(0, 1), seeded."""
     return np.random.default_rng(seed).standard_normal((nat_uc, 3, 3))
