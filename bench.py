@@ -47,6 +47,8 @@ def parse():
     ap.add_argument("--accuracy-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--precision-study", action="store_true",
+                    help="only the 200-step G(w) / a_n / b_n errors of every mixed precision against FP64")
     return ap.parse_args()
 
 
@@ -181,10 +183,12 @@ def run_reference_arm(a, rank):
 FP64_CHAIN = os.path.join(REPO, "tests", "golden", "c2_fp64_chain.npz")
 
 
-def precision_check(a, s, X, Y, rho, ens):
-    """G(w) of the seeded chain after `accuracy_steps` steps in the benchmark precision against the
-    same chain in FP64: the stored FP64 chain when it was made from these inputs, else a live run."""
+def precision_check(a, s, X, Y, rho, ens, precision=None):
+    """G(w) of the seeded chain after `accuracy_steps` steps in `precision` (default the benchmark's)
+    against the same chain in FP64: the stored FP64 chain when it was made from these inputs, else
+    a live run."""
     from tdscha_b200 import rocksalt as RS
+    precision = precision or a.precision
     steps = a.accuracy_steps
     ref = None
     if os.path.exists(FP64_CHAIN):
@@ -195,7 +199,7 @@ def precision_check(a, s, X, Y, rho, ens):
             ref = {"a": d["a"][:steps], "b": d["b"][:steps], "c": d["c"][:steps], "source": "stored FP64 chain "
                    f"(tests/golden/c2_fp64_chain.npz, {int(d['steps'])} steps, same ensemble checksum)"}
     t0 = time.perf_counter()
-    mixed = RS.seeded_chain(s, X, Y, rho, ens, a.precision, steps)
+    mixed = RS.seeded_chain(s, X, Y, rho, ens, precision, steps)
     t_mixed = time.perf_counter() - t0
     if ref is None:
         c64 = RS.seeded_chain(s, X, Y, rho, ens, "fp64", steps)
@@ -205,18 +209,28 @@ def precision_check(a, s, X, Y, rho, ens):
     k = min(len(ref["a"]), len(mixed.a_coeffs))
     amx, bmx, cmx = (np.array(x) for x in (mixed.a_coeffs, mixed.b_coeffs, mixed.c_coeffs))
 
-    def gf(av, bv, cv):   # k steps: a_0..a_{k-1}, b/c_0..b/c_{k-2}
-        mixed.a_coeffs, mixed.b_coeffs, mixed.c_coeffs = list(av[:k]), list(bv[:k - 1]), list(cv[:k - 1])
+    def gf(av, bv, cv, ns):   # ns steps: a_0..a_{ns-1}, b/c_0..b/c_{ns-2}
+        mixed.a_coeffs, mixed.b_coeffs, mixed.c_coeffs = list(av[:ns]), list(bv[:ns - 1]), list(cv[:ns - 1])
         return mixed.get_green_function_continued_fraction(w, use_terminator=False, smearing=eta)
 
-    gmx = gf(amx, bmx, cmx)
-    g64 = gf(ref["a"], ref["b"], ref["c"])
-    return {"steps": k, "omega": "500 points 0-400 cm^-1, smearing 5 cm^-1, no terminator",
-            "reference": ref["source"], "mixed_chain_s": round(t_mixed, 1),
-            "g_rel_err_max": float(np.abs(gmx - g64).max() / np.abs(g64).max()),
-            "g_rel_err_pointwise_median": float(np.median(np.abs(gmx - g64) / np.abs(g64))),
-            "a_err_max_over_max_a": float(np.max(np.abs(amx[:k] - ref["a"][:k])) / np.max(np.abs(ref["a"][:k]))),
-            "bound": 1e-5}
+    gmx = gf(amx, bmx, cmx, k)
+    g64 = gf(ref["a"], ref["b"], ref["c"], k)
+    kk = min(20, k - 1)
+    out = {"precision": precision, "steps": k, "omega": "500 points 0-400 cm^-1, smearing 5 cm^-1, no terminator",
+           "reference": ref["source"], "mixed_chain_s": round(t_mixed, 1),
+           "g_rel_err_max": float(np.abs(gmx - g64).max() / np.abs(g64).max()),
+           "g_rel_err_pointwise_median": float(np.median(np.abs(gmx - g64) / np.abs(g64))),
+           "a_rel_err_first20_max": float(np.max(np.abs(amx[:kk] - ref["a"][:kk]) / np.abs(ref["a"][:kk]))),
+           "b_rel_err_first20_max": float(np.max(np.abs(bmx[:kk] - ref["b"][:kk]) / np.abs(ref["b"][:kk]))),
+           "bound": 1e-5}
+    # G(w) error of the truncated chains (the chains resolve new poles at different steps)
+    by_steps = {}
+    for ns in (25, 50, 100, 150, 200):
+        if ns <= k:
+            g_ref = gf(ref["a"], ref["b"], ref["c"], ns)
+            by_steps[ns] = float(np.abs(gf(amx, bmx, cmx, ns) - g_ref).max() / np.abs(g_ref).max())
+    out["g_rel_err_max_by_steps"] = by_steps
+    return out
 
 
 # ------------------------------------------------------------------------------------------------
@@ -255,6 +269,11 @@ def main():
         dist.init_process_group("nccl", timeout=timedelta(seconds=600))
 
     ens = _native.DeviceEnsemble(X, Y, s.w, rho, s.T, s.symmetries, s.deg_space, s.blocks_ids)
+    if a.precision_study:
+        if rank == 0:
+            res = [precision_check(a, s, X, Y, rho, ens, p) for p in ("bf16x3", "tf32x3", "tf32", "bf16")]
+            print(json.dumps({"precision_study": workload_name(a), "results": res}))
+        return
     n = s.n_modes
     ln = n + n * (n + 1)
     nc = a.chains
