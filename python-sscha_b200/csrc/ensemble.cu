@@ -382,7 +382,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaDeviceSynchronize();
     void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->symP, e->symPT, e->d_offP, e->d_blk_start, e->d_blk_dim,
                   e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base,
-                  e->vjp_ws.base, e->YX};
+                  e->vjp_ws.base, e->YX, e->chunk_ops.base};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);
@@ -428,12 +428,13 @@ struct WsLayout {
     long long ld1, ldz, ldf;
 };
 
-static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, Format fmt, bool lo) {
+static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, Format fmt, bool lo, long long Nc) {
     WsLayout L{};
     const size_t es = format_bytes(fmt);
     const size_t as = (fmt == FMT_F64) ? 8 : 4;
     const long long M = (long long)nb * Jc;
-    L.ld1 = round_up(e->N2, 4);
+    const long long N2pc = round_up(2 * Nc, 64);
+    L.ld1 = round_up(2 * Nc, 4);
     L.ldz = round_up(e->P, 4);
     L.ldf = round_up(e->n, 4);
     size_t off = 0;
@@ -444,10 +445,10 @@ static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, F
     L.r1_lo = lo ? take(M * e->np * es) : 0;
     L.D1 = take(M * L.ld1 * as);
     L.Dcd = take(M * L.ld1 * as);
-    L.Cw_hi = take(M * e->N2p * es);
-    L.Cw_lo = lo ? take(M * e->N2p * es) : 0;
-    L.AB_hi = take(M * e->N2p * es);
-    L.AB_lo = lo ? take(M * e->N2p * es) : 0;
+    L.Cw_hi = take(M * N2pc * es);
+    L.Cw_lo = lo ? take(M * N2pc * es) : 0;
+    L.AB_hi = take(M * N2pc * es);
+    L.AB_lo = lo ? take(M * N2pc * es) : 0;
     L.Z = take(M * L.ldz * as);
     L.F = take(M * L.ldf * as);
     L.partD = take((size_t)nb * nf_total * e->n * e->n * 8);
@@ -467,9 +468,9 @@ static int ensure_ws(tdscha_ensemble *e, size_t bytes) {
 // C (M x N) row-major = A (M x K) . B (N x K)^T
 static int gemm_abt(tdscha_ensemble *e, Format fmt, int nprod, const void *A_hi, const void *A_lo, long long lda, long long M,
                     const void *B_hi, const void *B_lo, long long ldb, long long N, long long K, void *Cout, long long ldc,
-                    cudaStream_t st) {
+                    cudaStream_t st, bool accumulate = false) {
     if (fmt == FMT_F64) {
-        const double one = 1.0, zero = 0.0;
+        const double one = 1.0, zero = accumulate ? 1.0 : 0.0;
         cublasSetStream(e->cublas, st);
         cublasStatus_t s = cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, (int)N, (int)M, (int)K, &one,
                                        static_cast<const double *>(B_hi), (int)ldb, static_cast<const double *>(A_hi), (int)lda,
@@ -478,7 +479,47 @@ static int gemm_abt(tdscha_ensemble *e, Format fmt, int nprod, const void *A_hi,
         return 0;
     }
     tc::GemmOperands op{fmt, nprod, A_hi, A_lo, lda, B_hi, B_lo, ldb};
+    op.accumulate = accumulate;
     return tc::gemm(op, (int)M, (int)N, (int)K, static_cast<float *>(Cout), ldc, st, e->d_err);
+}
+
+// Bytes of the V / VT / XG / YXt operands for Nc configurations in format fmt.
+static size_t operand_bytes(const tdscha_ensemble *e, long long Nc, Format fmt, bool lo) {
+    const long long N2pc = round_up(2 * Nc, 64);
+    const size_t per = (size_t)(2 * Nc * e->Kp + e->P * N2pc + 2 * Nc * e->np + (long long)e->n * N2pc);
+    return per * format_bytes(fmt) * (lo ? 2 : 1) + 8 * 256;
+}
+
+// Operands of configurations [c0, c0 + Nc) built into `buf` (the configuration-chunked path).
+static int build_chunk_operands(tdscha_ensemble *e, long long c0, long long Nc, Format fmt, bool lo, void *buf, OperandSet &o,
+                                cudaStream_t st) {
+    const size_t es = format_bytes(fmt);
+    const long long N2pc = round_up(2 * Nc, 64);
+    const long long nV = 2 * Nc * e->Kp, nVT = e->P * N2pc, nXG = 2 * Nc * e->np, nYX = (long long)e->n * N2pc;
+    uint8_t *b = static_cast<uint8_t *>(buf);
+    size_t off = 0;
+    auto take = [&](long long count) { void *p = b + off; off += ((size_t)count * es + 255) / 256 * 256; return p; };
+    o = OperandSet();
+    o.V_hi = take(nV);
+    o.VT_hi = take(nVT);
+    o.XG_hi = take(nXG);
+    o.YXt_hi = take(nYX);
+    if (lo) {
+        o.V_lo = take(nV);
+        o.VT_lo = take(nVT);
+        o.XG_lo = take(nXG);
+        o.YXt_lo = take(nYX);
+    }
+    const int n = e->n, Ni = (int)Nc;
+    const double *X = e->X + c0 * n, *G = e->G + c0 * n, *Y = e->Y + c0 * n, *Xt = e->Xt + c0 * n;
+    build_V_kernel<<<grid_for(nV), 256, 0, st>>>(X, G, e->d_pair_mu, e->d_pair_nu, Ni, n, e->P, e->Kp, fmt, o.V_hi, o.V_lo);
+    build_VT_kernel<<<grid_for(nVT), 256, 0, st>>>(X, G, e->d_pair_mu, e->d_pair_nu, Ni, n, e->P, N2pc, fmt, o.VT_hi, o.VT_lo);
+    build_XG_kernel<<<grid_for(nXG), 256, 0, st>>>(X, G, Ni, n, e->np, fmt, o.XG_hi, o.XG_lo);
+    build_YXt_kernel<<<grid_for(nYX), 256, 0, st>>>(Y, Xt, Ni, n, N2pc, fmt, o.YXt_hi, o.YXt_lo);
+    TD_CUDA(cudaGetLastError());
+    o.built = true;
+    o.has_lo = lo;
+    return 0;
 }
 
 int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4, int precision,
@@ -490,19 +531,44 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     const Format fmt = format_of(precision);
     const int nprod = products_of(precision);
     const bool lo = needs_lo(precision);
-    TD_TRY(ensure_operands(e, fmt, lo, st));
-    OperandSet &o = e->ops[fmt];
+    // Configuration chunk: all configurations when their operands fit in half of the free memory
+    // (then they stay resident between calls), else chunks of Nc whose operands are rebuilt from
+    // the resident X, G, Y per (symmetry chunk, configuration chunk).  TDSCHA_CONFIG_CHUNK forces a
+    // chunk size (tuning and tests).
+    size_t free_b = 0, tot_b = 0;
+    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    long long Nc = e->N;
+    const char *env_chunk = getenv("TDSCHA_CONFIG_CHUNK");
+    if (env_chunk && atoll(env_chunk) > 0 && atoll(env_chunk) < e->N) {
+        Nc = atoll(env_chunk);
+    } else if (!e->ops[fmt].built && operand_bytes(e, e->N, fmt, lo) > (free_b + e->ws.bytes) / 2) {
+        const long long per_conf = 2 * (e->Kp + e->P + e->np + e->n) * (long long)format_bytes(fmt) * (lo ? 2 : 1);
+        const long long fit = (long long)((free_b + e->ws.bytes) * 0.4) / per_conf;
+        Nc = std::min<long long>(e->N, std::max<long long>(32, fit / 32 * 32));
+    }
+    const bool chunked = Nc < e->N;
+    OperandSet co;
+    if (chunked) {
+        const size_t need = operand_bytes(e, Nc, fmt, lo);
+        if (e->chunk_ops.bytes < need) {
+            if (e->chunk_ops.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->chunk_ops.base); e->chunk_ops = Workspace(); }
+            TD_CUDA(cudaMalloc(&e->chunk_ops.base, need));
+            e->chunk_ops.bytes = need;
+        }
+        TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    } else {
+        TD_TRY(ensure_operands(e, fmt, lo, st));
+        co = e->ops[fmt];
+    }
 
     // fold chunking over symmetries: Jf symmetries per partial, at most 64 partials
     const int Jf = std::max(16, ceil_div(e->N_sym, 64));
     const int nf_total = ceil_div(e->N_sym, Jf);
     // GEMM chunk over symmetries: a multiple of Jf whose workspace fits in the budget
-    size_t free_b = 0, tot_b = 0;
-    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
     const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
     int Jc = (int)round_up(e->N_sym, Jf);
-    while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo).total > budget) Jc = (int)round_up(Jc / 2, Jf);
-    const WsLayout L = layout(e, nb, Jc, nf_total, fmt, lo);
+    while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo, Nc).total > budget) Jc = (int)round_up(Jc / 2, Jf);
+    const WsLayout L = layout(e, nb, Jc, nf_total, fmt, lo, Nc);
     TD_TRY(ensure_ws(e, L.total));
     uint8_t *W = static_cast<uint8_t *>(e->ws.base);
     void *B1_hi = W + L.B1_hi, *B1_lo = lo ? W + L.B1_lo : nullptr;
@@ -524,38 +590,48 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
             TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo,
                                  fmt != FMT_F64, st));
         }
-        // GEMM1: [a | b] = B1 . V^T      (M x 2N, K = Kp)
-        {
-            StageScope sc(e, ST_GEMM_AB, st);
-            TD_TRY(gemm_abt(e, fmt, nprod, B1_hi, B1_lo, e->Kp, M, o.V_hi, o.V_lo, e->Kp, e->N2, e->Kp, D1, L.ld1, st));
-        }
-        // [c | d] = r1 . [X; G]^T         (M x 2N, K = np)
-        {
-            StageScope sc(e, ST_GEMM_CD, st);
-            TD_TRY(gemm_abt(e, fmt, nprod, r1_hi, r1_lo, e->np, M, o.XG_hi, o.XG_lo, e->np, e->N2, e->np, Dcd, L.ld1, st));
-        }
-        // weights
-        {
-            StageScope sc(e, ST_WEIGHTS, st);
-            if (fmt == FMT_F64)
-                weights_kernel<double><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
-                    (const double *)D1, (const double *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo,
-                    AB_hi, AB_lo);
-            else
-                weights_kernel<float><<<grid_for(M * (e->N + e->N2p - e->N2)), 256, 0, st>>>(
-                    (const float *)D1, (const float *)Dcd, L.ld1, e->rho, e->N, (int)M, e->N2p, apply_d4, fmt, Cw_hi, Cw_lo,
-                    AB_hi, AB_lo);
-            TD_CUDA(cudaGetLastError());
-        }
-        // GEMM2: Z = Cw . VT^T            (M x P, K = N2p)
-        {
-            StageScope sc(e, ST_GEMM_Z, st);
-            TD_TRY(gemm_abt(e, fmt, nprod, Cw_hi, Cw_lo, e->N2p, M, o.VT_hi, o.VT_lo, e->N2p, e->P, e->N2p, Z, L.ldz, st));
-        }
-        // F = AB . YXt^T                  (M x n, K = N2p)
-        {
-            StageScope sc(e, ST_GEMM_F, st);
-            TD_TRY(gemm_abt(e, fmt, nprod, AB_hi, AB_lo, e->N2p, M, o.YXt_hi, o.YXt_lo, e->N2p, e->n, e->N2p, F, L.ldf, st));
+        for (long long c0 = 0; c0 < e->N; c0 += Nc) {
+            const long long Ncur = std::min(Nc, e->N - c0);
+            const long long N2c = 2 * Ncur, N2pc = round_up(N2c, 64);
+            const bool acc = c0 > 0;
+            if (chunked) {
+                StageScope sc(e, ST_OTHER, st);
+                TD_TRY(build_chunk_operands(e, c0, Ncur, fmt, lo, e->chunk_ops.base, co, st));
+            }
+            // GEMM1: [a | b] = B1 . V^T      (M x 2Nc, K = Kp)
+            {
+                StageScope sc(e, ST_GEMM_AB, st);
+                TD_TRY(gemm_abt(e, fmt, nprod, B1_hi, B1_lo, e->Kp, M, co.V_hi, co.V_lo, e->Kp, N2c, e->Kp, D1, L.ld1, st));
+            }
+            // [c | d] = r1 . [X; G]^T         (M x 2Nc, K = np)
+            {
+                StageScope sc(e, ST_GEMM_CD, st);
+                TD_TRY(gemm_abt(e, fmt, nprod, r1_hi, r1_lo, e->np, M, co.XG_hi, co.XG_lo, e->np, N2c, e->np, Dcd, L.ld1, st));
+            }
+            // weights
+            {
+                StageScope sc(e, ST_WEIGHTS, st);
+                const int Ni = (int)Ncur;
+                if (fmt == FMT_F64)
+                    weights_kernel<double><<<grid_for(M * (Ncur + N2pc - N2c)), 256, 0, st>>>(
+                        (const double *)D1, (const double *)Dcd, L.ld1, e->rho + c0, Ni, (int)M, N2pc, apply_d4, fmt, Cw_hi,
+                        Cw_lo, AB_hi, AB_lo);
+                else
+                    weights_kernel<float><<<grid_for(M * (Ncur + N2pc - N2c)), 256, 0, st>>>(
+                        (const float *)D1, (const float *)Dcd, L.ld1, e->rho + c0, Ni, (int)M, N2pc, apply_d4, fmt, Cw_hi,
+                        Cw_lo, AB_hi, AB_lo);
+                TD_CUDA(cudaGetLastError());
+            }
+            // GEMM2: Z (+)= Cw . VT^T          (M x P, K = N2pc)
+            {
+                StageScope sc(e, ST_GEMM_Z, st);
+                TD_TRY(gemm_abt(e, fmt, nprod, Cw_hi, Cw_lo, N2pc, M, co.VT_hi, co.VT_lo, N2pc, e->P, N2pc, Z, L.ldz, st, acc));
+            }
+            // F (+)= AB . YXt^T                (M x n, K = N2pc)
+            {
+                StageScope sc(e, ST_GEMM_F, st);
+                TD_TRY(gemm_abt(e, fmt, nprod, AB_hi, AB_lo, N2pc, M, co.YXt_hi, co.YXt_lo, N2pc, e->n, N2pc, F, L.ldf, st, acc));
+            }
         }
         // fold this chunk into the partials
         {

@@ -83,6 +83,7 @@ struct tdscha_ensemble {
     tdscha::OperandSet ops[3];                     // indexed by Format
     tdscha::Workspace ws;
     tdscha::Workspace vjp_ws;                      // workspace of the averages' VJP
+    tdscha::Workspace chunk_ops;                   // operands of one configuration chunk (large ensembles)
     double *YX = nullptr;                          // [Y; X~] (2N x np), FP64, built by the first VJP
     cublasHandle_t cublas = nullptr;
     size_t base_bytes = 0;

@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
                int M, int N, int K, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err,
-               unsigned *tile_sync, unsigned sync_ns) {
+               unsigned *tile_sync, unsigned sync_ns, int accumulate) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -343,12 +343,16 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
                 for (int v = 0; v < C::EPI_COLS / 4; ++v) {
                     const int cb = cb0 + 4 * v;
                     if (cb + 4 <= N && ((ldd & 3) == 0)) {
-                        *reinterpret_cast<float4 *>(drow + cb) =
-                            make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
+                        float4 o = make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
+                        if (accumulate) {
+                            const float4 old = *reinterpret_cast<const float4 *>(drow + cb);
+                            o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
+                        }
+                        *reinterpret_cast<float4 *>(drow + cb) = o;
                     } else {
 #pragma unroll
                         for (int e = 0; e < 4; ++e)
-                            if (cb + e < N) drow[cb + e] = acc[4 * v + e];
+                            if (cb + e < N) drow[cb + e] = accumulate ? drow[cb + e] + acc[4 * v + e] : acc[4 * v + e];
                     }
                 }
             }
@@ -442,7 +446,7 @@ static std::map<TuneKey, int> g_tune;
 
 template <typename Launch>
 static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long long tiles, int sms, cudaStream_t st,
-                       Launch &launch, int *gm_out) {
+                       Launch &launch, bool allow_trials, int *gm_out) {
     int dev = 0;
     TD_CUDA(cudaGetDevice(&dev));
     const TuneKey key{tf32, nprod, M, N, K, dev};
@@ -452,7 +456,7 @@ static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long
         if (it != g_tune.end()) { *gm_out = it->second; return 0; }
     }
     const char *env = getenv("TDSCHA_AUTOTUNE");
-    const bool enabled = !(env && atoi(env) == 0);
+    const bool enabled = allow_trials && !(env && atoi(env) == 0);
     int best = num_m;
     if (enabled && tiles >= 8LL * sms) {
         const int cand_all[] = {num_m, 48, 24, 12, 6};
@@ -482,7 +486,7 @@ static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long
         cudaEventDestroy(e1);
     }
     std::lock_guard<std::mutex> lock(g_tune_mutex);
-    g_tune[key] = best;
+    if (allow_trials) g_tune[key] = best;
     *gm_out = best;
     return 0;
 }
@@ -533,18 +537,20 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     dim3 grid((unsigned)std::min<long long>(tiles, sms));
     const int num_m = ceil_div(M, BM);
     const unsigned sync_ns = tile_sync_budget_ns();
+    const int accumulate = op.accumulate ? 1 : 0;
     unsigned *counter = nullptr;
     if (sync_ns > 0 && tiles > grid.x) TD_TRY(tile_sync_counter(dev, &counter));
     auto launch = [&](int gm) {
         if (counter) cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
         kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err,
-                                                        counter, sync_ns);
+                                                        counter, sync_ns, accumulate);
     };
     if (const char *env = getenv("TDSCHA_GROUP_M")) {   // tuning knob: fixed tile-group size
         launch(std::max(1, std::min(num_m, atoi(env))));
     } else {
         int gm = 0;
-        TD_TRY(tuned_group(TF32 ? 1 : 0, NPROD, M, N, K, num_m, tiles, sms, st, launch, &gm));
+        // trial runs write D, so an accumulating launch only reuses a group size tuned earlier
+        TD_TRY(tuned_group(TF32 ? 1 : 0, NPROD, M, N, K, num_m, tiles, sms, st, launch, !accumulate, &gm));
         launch(gm);
     }
     TD_CUDA(cudaGetLastError());

@@ -17,6 +17,7 @@ struct GemmOperands {
     const void *B_hi, *B_lo;
     long long ldb;
     int drain_kb = 0;   // k-blocks per TMEM chunk drained to fp32 registers (0 = library default)
+    bool accumulate = false;   // D += A . B^T instead of D = A . B^T
 };
 
 // K must be a multiple of 64 (bf16) or 32 (tf32); operands must be readable up to K columns.
