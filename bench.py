@@ -44,6 +44,10 @@ def parse():
     ap.add_argument("--L", type=int, default=4)
     ap.add_argument("--N", type=int, default=10000)
     ap.add_argument("--T", type=float, default=300.0)
+    ap.add_argument("--k3", type=float, default=-3.0, help="cubic bond coupling, eV/A^3")
+    ap.add_argument("--k4", type=float, default=6.0, help="quartic bond coupling, eV/A^4")
+    ap.add_argument("--sym-on-gpu", action="store_true",
+                    help="project the symmetry operations onto the modes on the GPU (large supercells)")
     ap.add_argument("--accuracy-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
@@ -55,6 +59,7 @@ def parse():
 def workload_name(a):
     nat = 2 * a.L ** 3
     return (f"rock-salt {a.L}x{a.L}x{a.L} ({nat} atoms, n={3 * nat - 3}), N={a.N}, T={a.T:g} K, "
+            f"k3={a.k3:g} eV/A^3, k4={a.k4:g} eV/A^4, "
             f"O_h x {a.L ** 3} = {48 * a.L ** 3} symmetries, {a.chains} bi-conjugate chains "
             f"(2 x {a.chains} applies per step)")
 
@@ -155,7 +160,7 @@ def run_reference_arm(a, rank):
     if rank != 0:
         return None
     from tdscha_b200 import rocksalt as RS
-    s = RS.build_system(a.L, T=a.T)
+    s = RS.build_system(a.L, T=a.T, k3=a.k3, k4=a.k4)   # host cores only: the pool forks
     X, Y, rho = RS.sample_ensemble(s, a.N, seed=0)
     vals = []
     for _ in range(max(1, a.warmup // 3)):      # untimed warm-up (import + page-in)
@@ -249,10 +254,14 @@ def main():
     from tdscha_b200 import rocksalt as RS
 
     # CPU baseline first (spawned processes, before any CUDA context): rank 0 at N = 1 only
-    s = RS.build_system(a.L, T=a.T)
+    s = RS.build_system(a.L, T=a.T, k3=a.k3, k4=a.k4, symmetries_on_gpu=a.sym_on_gpu)
     X, Y, rho = RS.sample_ensemble(s, a.N, seed=0)
     cpu_base = None
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+    if a.sym_on_gpu and not a.no_cpu_baseline:
+        # the baseline's process pool forks, which is unsafe once the symmetry build opened a CUDA context
+        cpu_base = {"value": None, "unit": "apply_L/s", "cores": 0, "kind": "reference",
+                    "sample": "skipped: --sym-on-gpu opens a CUDA context before the forking process pool"}
+    elif rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
             v, cores, sample = cpu_reference_timing(s, X, Y, rho)
             cpu_base = {"value": v, "unit": "apply_L/s", "cores": cores, "kind": "reference", "sample": sample}

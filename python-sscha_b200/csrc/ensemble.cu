@@ -17,50 +17,75 @@ namespace tdscha {
 // ------------------------------------------------------------------------------------------------
 // operand builders (once per ensemble and storage format)
 // ------------------------------------------------------------------------------------------------
-// V (2N x Kp): rows < N -> c_p x_mu x_nu ; rows >= N -> x_mu g_nu + x_nu g_mu (x g on the diagonal)
+// V (2N x Kp): rows < N -> c_p x_mu x_nu ; rows >= N -> x_mu g_nu + x_nu g_mu (x g on the diagonal).
+// One CTA row per operand row (blockIdx.y strides over rows), threads over the packed pairs p: the
+// pair tables are read coalesced and x, g come from one row of X / G (L1).
 __global__ void build_V_kernel(const double *__restrict__ X, const double *__restrict__ G,
                                const int *__restrict__ pmu, const int *__restrict__ pnu, int N, int n,
                                long long P, long long Kp, Format fmt, void *hi, void *lo) {
-    const long long total = 2LL * N * Kp;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const long long k = idx / Kp, p = idx % Kp;
-        double v = 0.0;
-        if (p < P) {
-            const int mu = pmu[p], nu = pnu[p];
-            if (k < N) {
-                const double *x = X + k * n;
-                v = (mu == nu ? 1.0 : 2.0) * x[mu] * x[nu];
-            } else {
-                const double *x = X + (k - N) * n;
-                const double *g = G + (k - N) * n;
-                v = (mu == nu) ? x[mu] * g[mu] : x[mu] * g[nu] + x[nu] * g[mu];
+    for (long long k = blockIdx.y; k < 2LL * N; k += gridDim.y) {
+        const bool second = k >= N;
+        const double *x = X + (second ? k - N : k) * n;
+        const double *g = G + (second ? k - N : k) * n;
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < Kp; p += (long long)gridDim.x * blockDim.x) {
+            double v = 0.0;
+            if (p < P) {
+                const int mu = pmu[p], nu = pnu[p];
+                if (!second) v = (mu == nu ? 1.0 : 2.0) * x[mu] * x[nu];
+                else v = (mu == nu) ? x[mu] * g[mu] : x[mu] * g[nu] + x[nu] * g[mu];
             }
+            store_split(fmt, hi, lo, k * Kp + p, v);
         }
-        store_split(fmt, hi, lo, idx, v);
     }
 }
 
-// VT (P x N2p) = V^T with zero columns beyond 2N
-__global__ void build_VT_kernel(const double *__restrict__ X, const double *__restrict__ G,
-                                const int *__restrict__ pmu, const int *__restrict__ pnu, int N, int n,
-                                long long P, long long N2p, Format fmt, void *hi, void *lo) {
-    const long long total = P * N2p;
-    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
-         idx += (long long)gridDim.x * blockDim.x) {
-        const long long p = idx / N2p, k = idx % N2p;
+// VT (P x N2p) = V^T with zero columns beyond 2N, from the transposed ensemble XGT = [X^T ; G^T]
+// (2n x ldT, configuration-contiguous): one CTA row per pair p, threads over configurations, so
+// every read and write is coalesced.
+__global__ void build_VT_kernel(const double *__restrict__ XGT, long long ldT, const int *__restrict__ pmu,
+                                const int *__restrict__ pnu, int N, int n, long long P, long long N2p, Format fmt, void *hi,
+                                void *lo) {
+    for (long long p = blockIdx.y; p < P; p += gridDim.y) {
         const int mu = pmu[p], nu = pnu[p];
-        double v = 0.0;
-        if (k < N) {
-            const double *x = X + k * n;
-            v = (mu == nu ? 1.0 : 2.0) * x[mu] * x[nu];
-        } else if (k < 2LL * N) {
-            const double *x = X + (k - N) * n;
-            const double *g = G + (k - N) * n;
-            v = (mu == nu) ? x[mu] * g[mu] : x[mu] * g[nu] + x[nu] * g[mu];
+        const double *xm = XGT + (long long)mu * ldT, *xn = XGT + (long long)nu * ldT;
+        const double *gm = XGT + (long long)(n + mu) * ldT, *gn = XGT + (long long)(n + nu) * ldT;
+        const double c = mu == nu ? 1.0 : 2.0;
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N2p; k += (long long)gridDim.x * blockDim.x) {
+            double v = 0.0;
+            if (k < N) {
+                v = c * xm[k] * xn[k];
+            } else if (k < 2LL * N) {
+                const long long i = k - N;
+                v = (mu == nu) ? xm[i] * gm[i] : xm[i] * gn[i] + xn[i] * gm[i];
+            }
+            store_split(fmt, hi, lo, p * N2p + k, v);
         }
-        store_split(fmt, hi, lo, idx, v);
     }
+}
+
+// XGT (2n x N) = [X^T ; G^T], tiled transpose through shared memory
+__global__ void transpose_XG_kernel(const double *__restrict__ X, const double *__restrict__ G, int N, int n,
+                                    double *__restrict__ XGT) {
+    __shared__ double tile[32][33];
+    const int which = blockIdx.z;                       // 0: X, 1: G
+    const double *src = which ? G : X;
+    const int i0 = blockIdx.y * 32, m0 = blockIdx.x * 32;
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int i = i0 + r, m = m0 + threadIdx.x;
+        tile[r][threadIdx.x] = (i < N && m < n) ? src[(long long)i * n + m] : 0.0;
+    }
+    __syncthreads();
+    for (int r = threadIdx.y; r < 32; r += blockDim.y) {
+        const int m = m0 + r, i = i0 + threadIdx.x;
+        if (m < n && i < N) XGT[((long long)which * n + m) * N + i] = tile[threadIdx.x][r];
+    }
+}
+
+// grid of the row-wise builders: x over a row's columns (256 threads a CTA), y over rows
+static dim3 rows_grid(long long cols, long long rows) {
+    const long long gx = std::min<long long>(ceil_div(cols, 256), 64);
+    const long long gy = std::min<long long>(std::max<long long>(rows, 1), 65535);
+    return dim3((unsigned)std::max<long long>(gx, 1), (unsigned)gy);
 }
 
 // XG (2N x np) = [X ; G] ; YXt (n x N2p) = [Y^T | X~^T]
@@ -382,7 +407,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaDeviceSynchronize();
     void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->symP, e->symPT, e->d_offP, e->d_blk_start, e->d_blk_dim,
                   e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base,
-                  e->vjp_ws.base, e->YX, e->chunk_ops.base};
+                  e->vjp_ws.base, e->YX, e->chunk_ops.base, e->XGT};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);
@@ -390,6 +415,17 @@ int ensemble_destroy(tdscha_ensemble *e) {
     if (e->cublas) cublasDestroy(e->cublas);
     delete e;
     cudaSetDevice(prev);
+    return 0;
+}
+
+// The transposed ensemble [X^T ; G^T] (2n x N) of the VT builder, built once.
+static int ensure_XGT(tdscha_ensemble *e, cudaStream_t st) {
+    if (e->XGT) return 0;
+    TD_CHECK(ceil_div(e->N, 32) <= 65535, TDSCHA_EINVAL, "ensemble of %d configurations exceeds the transpose grid", e->N);
+    TD_CUDA(cudaMalloc(&e->XGT, (size_t)2 * e->n * e->N * sizeof(double)));
+    dim3 grid((unsigned)ceil_div(e->n, 32), (unsigned)ceil_div(e->N, 32), 2);
+    transpose_XG_kernel<<<grid, dim3(32, 8), 0, st>>>(e->X, e->G, e->N, e->n, e->XGT);
+    TD_CUDA(cudaGetLastError());
     return 0;
 }
 
@@ -411,8 +447,11 @@ static int ensure_operands(tdscha_ensemble *e, Format fmt, bool with_lo, cudaStr
         TD_TRY(dev_alloc(&o.XG_lo, nXG * es, &acc));
         TD_TRY(dev_alloc(&o.YXt_lo, nYX * es, &acc));
     }
-    build_V_kernel<<<grid_for(nV), 256, 0, st>>>(e->X, e->G, e->d_pair_mu, e->d_pair_nu, e->N, e->n, e->P, e->Kp, fmt, o.V_hi, o.V_lo);
-    build_VT_kernel<<<grid_for(nVT), 256, 0, st>>>(e->X, e->G, e->d_pair_mu, e->d_pair_nu, e->N, e->n, e->P, e->N2p, fmt, o.VT_hi, o.VT_lo);
+    TD_TRY(ensure_XGT(e, st));
+    build_V_kernel<<<rows_grid(e->Kp, e->N2), 256, 0, st>>>(e->X, e->G, e->d_pair_mu, e->d_pair_nu, e->N, e->n, e->P, e->Kp, fmt,
+                                                           o.V_hi, o.V_lo);
+    build_VT_kernel<<<rows_grid(e->N2p, e->P), 256, 0, st>>>(e->XGT, e->N, e->d_pair_mu, e->d_pair_nu, e->N, e->n, e->P, e->N2p,
+                                                            fmt, o.VT_hi, o.VT_lo);
     build_XG_kernel<<<grid_for(nXG), 256, 0, st>>>(e->X, e->G, e->N, e->n, e->np, fmt, o.XG_hi, o.XG_lo);
     build_YXt_kernel<<<grid_for(nYX), 256, 0, st>>>(e->Y, e->Xt, e->N, e->n, e->N2p, fmt, o.YXt_hi, o.YXt_lo);
     TD_CUDA(cudaGetLastError());
@@ -478,9 +517,26 @@ static int gemm_abt(tdscha_ensemble *e, Format fmt, int nprod, const void *A_hi,
         TD_CHECK(s == CUBLAS_STATUS_SUCCESS, TDSCHA_ECUDA, "cublasDgemm failed (%d)", (int)s);
         return 0;
     }
-    tc::GemmOperands op{fmt, nprod, A_hi, A_lo, lda, B_hi, B_lo, ldb};
-    op.accumulate = accumulate;
-    return tc::gemm(op, (int)M, (int)N, (int)K, static_cast<float *>(Cout), ldc, st, e->d_err);
+    // Split K: a contraction over a K longer than about 72k runs as launches over K slices, the
+    // later ones accumulating into the output.  Within one launch the co-resident tiles walk K in
+    // near-lockstep and share the operand slices through L2; over a very long K they drift apart
+    // (the L2 holds only a few thousand K of the tiles' panels), so the slices bound the drift.
+    // TDSCHA_KSPLIT sets the slice length (elements; 0 disables).
+    const char *kv = getenv("TDSCHA_KSPLIT");
+    const long long kslice = kv ? atoll(kv) : 73728LL;
+    const size_t es = format_bytes(fmt);
+    long long chunk = K;
+    if (kslice > 0 && K > kslice) chunk = round_up(ceil_div(K, ceil_div(K, kslice)), 64);
+    for (long long k0 = 0; k0 < K; k0 += chunk) {
+        const long long kc = std::min(chunk, K - k0);
+        auto off = [&](const void *p) -> const void * {
+            return p ? static_cast<const uint8_t *>(p) + k0 * es : nullptr;
+        };
+        tc::GemmOperands op{fmt, nprod, off(A_hi), off(A_lo), lda, off(B_hi), off(B_lo), ldb};
+        op.accumulate = accumulate || k0 > 0;
+        TD_TRY(tc::gemm(op, (int)M, (int)N, (int)kc, static_cast<float *>(Cout), ldc, st, e->d_err));
+    }
+    return 0;
 }
 
 // Bytes of the V / VT / XG / YXt operands for Nc configurations in format fmt.
@@ -512,8 +568,11 @@ static int build_chunk_operands(tdscha_ensemble *e, long long c0, long long Nc, 
     }
     const int n = e->n, Ni = (int)Nc;
     const double *X = e->X + c0 * n, *G = e->G + c0 * n, *Y = e->Y + c0 * n, *Xt = e->Xt + c0 * n;
-    build_V_kernel<<<grid_for(nV), 256, 0, st>>>(X, G, e->d_pair_mu, e->d_pair_nu, Ni, n, e->P, e->Kp, fmt, o.V_hi, o.V_lo);
-    build_VT_kernel<<<grid_for(nVT), 256, 0, st>>>(X, G, e->d_pair_mu, e->d_pair_nu, Ni, n, e->P, N2pc, fmt, o.VT_hi, o.VT_lo);
+    TD_TRY(ensure_XGT(e, st));
+    build_V_kernel<<<rows_grid(e->Kp, 2 * Nc), 256, 0, st>>>(X, G, e->d_pair_mu, e->d_pair_nu, Ni, n, e->P, e->Kp, fmt, o.V_hi,
+                                                            o.V_lo);
+    build_VT_kernel<<<rows_grid(N2pc, e->P), 256, 0, st>>>(e->XGT + c0, e->N, e->d_pair_mu, e->d_pair_nu, Ni, n, e->P, N2pc, fmt,
+                                                          o.VT_hi, o.VT_lo);
     build_XG_kernel<<<grid_for(nXG), 256, 0, st>>>(X, G, Ni, n, e->np, fmt, o.XG_hi, o.XG_lo);
     build_YXt_kernel<<<grid_for(nYX), 256, 0, st>>>(Y, Xt, Ni, n, N2pc, fmt, o.YXt_hi, o.YXt_lo);
     TD_CUDA(cudaGetLastError());

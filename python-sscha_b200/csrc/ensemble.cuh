@@ -85,6 +85,7 @@ struct tdscha_ensemble {
     tdscha::Workspace vjp_ws;                      // workspace of the averages' VJP
     tdscha::Workspace chunk_ops;                   // operands of one configuration chunk (large ensembles)
     double *YX = nullptr;                          // [Y; X~] (2N x np), FP64, built by the first VJP
+    double *XGT = nullptr;                         // [X^T; G^T] (2n x N), FP64, built by the first operand build
     cublasHandle_t cublas = nullptr;
     size_t base_bytes = 0;
     tdscha::Profile prof;

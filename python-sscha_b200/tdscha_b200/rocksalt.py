@@ -84,8 +84,10 @@ def _oh_rotations():
 
 
 def build_system(L, T=300.0, a_ang=5.6, masses_amu=(23.0, 35.45), k2=2.0, k3=-3.0, k4=6.0,
-                 deg_tol=1e-7, with_symmetries=True):
-    """Supercell geometry, harmonic modes and mode-space symmetry blocks.  k2/k3/k4 in eV/A^n."""
+                 deg_tol=1e-7, with_symmetries=True, symmetries_on_gpu=False):
+    """Supercell geometry, harmonic modes and mode-space symmetry blocks.  k2/k3/k4 in eV/A^n.
+    symmetries_on_gpu: project the symmetry operations onto the modes with the device kernel
+    (tdscha_symmetries_on_modes) instead of numpy (large supercells)."""
     a = a_ang / BOHR_TO_ANG
     prim = 0.5 * a * np.array([[0, 1, 1], [1, 0, 1], [1, 1, 0]], dtype=np.float64)
     basis = np.array([[0.0, 0.0, 0.0], [0.5 * a, 0.0, 0.0]])
@@ -172,25 +174,38 @@ def build_system(L, T=300.0, a_ang=5.6, masses_amu=(23.0, 35.45), k2=2.0, k3=-3.
         return sys_
 
     rots = _oh_rotations()
-    trans = [n1 * prim[0] + n2 * prim[1] + n3 * prim[2] for n1, n2, n3 in itertools.product(range(L), repeat=3)]
+    trans = np.array([n1 * prim[0] + n2 * prim[1] + n3 * prim[2] for n1, n2, n3 in itertools.product(range(L), repeat=3)])
+    # image atoms of every (rotation, translation): lattice keys of the images looked up in a table
+    q = 4 * L
+    lut = np.full(q ** 3, -1, dtype=np.int64)
+    for kk, i in key.items():
+        lut[(kk[0] * q + kk[1]) * q + kk[2]] = i
     perms, rmats = [], []
     for R in rots:
-        rp = pos @ R.T
-        for t in trans:
-            perms.append([find(r + t) for r in rp])
-            rmats.append(R)
+        img = (pos @ R.T)[None, :, :] + trans[:, None, :]          # (n_trans, nat, 3)
+        f = wrap_frac(img.reshape(-1, 3))
+        k = np.round(f * q).astype(np.int64) % q
+        p = lut[(k[:, 0] * q + k[:, 1]) * q + k[:, 2]].reshape(len(trans), nat)
+        if (p < 0).any():
+            raise RuntimeError("symmetry image off the lattice")
+        perms.extend(p)
+        rmats.extend([R] * len(trans))
     perms = np.array(perms, dtype=np.int64)
     rmats = np.array(rmats)
     N_sym = len(perms)
-    # P_j acting on (3 nat) mass-weighted displacement: (P v)[pi(a)] = R v[a]
-    sym_blocks = [np.zeros((N_sym, len(blk), len(blk))) for blk in blocks]
-    E3 = vec.reshape(nat, 3, -1)
-    for j in range(N_sym):
-        PE = np.zeros_like(E3)
-        PE[perms[j]] = np.einsum("ab,nbm->nam", rmats[j], E3)
-        PE = PE.reshape(3 * nat, -1)
-        for b, blk in enumerate(blocks):
-            sym_blocks[b][j] = vec[:, blk].T @ PE[:, blk]
+    if symmetries_on_gpu:
+        from . import _native
+        sym_blocks = _native.symmetries_on_modes(vec, perms, rmats, sys_.deg_space)
+    else:
+        # P_j acting on (3 nat) mass-weighted displacement: (P v)[pi(a)] = R v[a]
+        sym_blocks = [np.zeros((N_sym, len(blk), len(blk))) for blk in blocks]
+        E3 = vec.reshape(nat, 3, -1)
+        for j in range(N_sym):
+            PE = np.zeros_like(E3)
+            PE[perms[j]] = np.einsum("ab,nbm->nam", rmats[j], E3)
+            PE = PE.reshape(3 * nat, -1)
+            for b, blk in enumerate(blocks):
+                sym_blocks[b][j] = vec[:, blk].T @ PE[:, blk]
     sys_.symmetries = sym_blocks
     sys_.n_syms = N_sym
     sys_.perm = perms

@@ -65,3 +65,22 @@ def test_chunked_equals_resident(cuda, chunk_env, precision):
     tol = 1e-12 if precision == "fp64" else TOL[precision]
     assert _rel(out[128][0], out[None][0]) < tol
     assert _rel(out[128][1], out[None][1]) < tol
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3", "bf16"])
+def test_split_k_equals_single_launch(cuda, rocksalt_l2, monkeypatch, precision):
+    """The projection contraction split over K slices (TDSCHA_KSPLIT, accumulate epilogue) against
+    one launch over the whole K: slices of 384, 384, 320 for K = 1088."""
+    from tdscha_b200 import _native
+    d = rocksalt_l2
+    ens = _native.DeviceEnsemble(d["X"], d["Y"], d["w"], d["rho"], d["T"], d["syms"], d["blocks"], d["blocks_ids"])
+    out = {}
+    for ks in ("0", "400"):
+        monkeypatch.setenv("TDSCHA_KSPLIT", ks)
+        out[ks] = ens.perturb_average(d["case1_R1"], d["case1_Y1"], 1, precision)
+        assert _rel(out[ks][1], d["case1_d2v"]) < TOL[precision]
+    monkeypatch.delenv("TDSCHA_KSPLIT")
+    ens.close()
+    tol = 1e-5 if precision != "bf16" else 1e-2
+    assert _rel(out["400"][0], out["0"][0]) < tol
+    assert _rel(out["400"][1], out["0"][1]) < tol

@@ -26,6 +26,16 @@ def test_symmetries_on_modes_match_numpy(cuda, system):
         assert np.abs(eye - np.eye(S.shape[1])).max() <= 1e-10
 
 
+def test_generator_gpu_symmetries_match_numpy(cuda):
+    """build_system(symmetries_on_gpu=True), the path of the large-supercell benchmark, on 3x3x3."""
+    from tdscha_b200 import rocksalt as RS
+    ref = RS.build_system(3)
+    got = RS.build_system(3, symmetries_on_gpu=True)
+    assert np.array_equal(ref.perm, got.perm)
+    for a, b in zip(got.symmetries, ref.symmetries):
+        assert np.abs(a - b).max() <= 1e-12
+
+
 def test_ensemble_projection_matches_numpy(cuda, system):
     from tdscha_b200 import modes
     s = system
