@@ -600,9 +600,11 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     const char *env_chunk = getenv("TDSCHA_CONFIG_CHUNK");
     if (env_chunk && atoll(env_chunk) > 0 && atoll(env_chunk) < e->N) {
         Nc = atoll(env_chunk);
-    } else if (!e->ops[fmt].built && operand_bytes(e, e->N, fmt, lo) > (free_b + e->ws.bytes) / 2) {
+    } else if (!e->ops[fmt].built &&
+               operand_bytes(e, e->N, fmt, lo) > (free_b + e->ws.bytes + e->chunk_ops.bytes) / 2) {
+        // memory this call may use: free + its own workspace and chunk buffer (so every call plans alike)
         const long long per_conf = 2 * (e->Kp + e->P + e->np + e->n) * (long long)format_bytes(fmt) * (lo ? 2 : 1);
-        const long long fit = (long long)((free_b + e->ws.bytes) * 0.4) / per_conf;
+        const long long fit = (long long)((free_b + e->ws.bytes + e->chunk_ops.bytes) * 0.4) / per_conf;
         Nc = std::min<long long>(e->N, std::max<long long>(32, fit / 32 * 32));
     }
     const bool chunked = Nc < e->N;
