@@ -51,6 +51,10 @@ def parse():
     ap.add_argument("--accuracy-steps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--batch-systems", action="store_true",
+                    help="16 chains (3 IR, 6 Raman, 7 random) on each of three uneven rock-salt systems "
+                         "(2x2x2 N=2000, 3x3x3 N=5000, 4x4x4 N=10000) in one graph-captured multi-system run")
+    ap.add_argument("--batch-steps", type=int, default=150)
     ap.add_argument("--precision-study", action="store_true",
                     help="only the 200-step G(w) / a_n / b_n errors of every mixed precision against FP64")
     return ap.parse_args()
@@ -239,6 +243,115 @@ def precision_check(a, s, X, Y, rho, ens, precision=None):
 
 
 # ------------------------------------------------------------------------------------------------
+BATCH_SYSTEMS = ((2, 2000, 31), (3, 5000, 32), (4, 10000, 33))   # (L, N, seed), T = 300 K
+
+
+def batch_chains(base):
+    """The 16 chains of one system: IR along x, y, z (seeded Born charges), Raman for the six
+    (in, out) polarisation pairs xx yy zz xy yz xz (seeded Raman tensors), 7 seeded random unit
+    vectors on R^(1)."""
+    e = np.eye(3)
+    chains = []
+    for pol in e:
+        L = base.new_chain()
+        L.prepare_ir(pol_vec=pol)
+        chains.append(L)
+    for i, j in ((0, 0), (1, 1), (2, 2), (0, 1), (1, 2), (0, 2)):
+        L = base.new_chain()
+        L.prepare_raman(pol_vec_in=e[i], pol_vec_out=e[j])
+        chains.append(L)
+    for sd in range(7):
+        L = base.new_chain()
+        L.prepare_random(seed=100 + sd, sector="R")
+        chains.append(L)
+    return chains
+
+
+def run_batch_systems(a):
+    """Throughput of 48 chains (16 per system) over three uneven systems advanced together by
+    tdscha_lanczos_run_device (one CUDA graph launch per step after two eager steps), against the
+    host-driven per-system loop; G(w) error of the mixed chains against FP64 on the two small
+    systems."""
+    import torch
+    from tdscha_b200 import DynamicalLanczos as DL
+    from tdscha_b200 import rocksalt as RS
+    bases, names = [], []
+    for L_, N_, seed in BATCH_SYSTEMS:
+        ens = RS.make_ensemble(L_, N_, T=300.0, seed=seed)
+        b = DL.Lanczos(ens)
+        b.init()
+        bases.append(b)
+        names.append(f"{L_}x{L_}x{L_} (n={b.n_modes}) N={N_} N_sym={b.n_syms}")
+    steps = a.batch_steps
+    prec = a.precision
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # warm-up (untimed): tunes the contraction tiles, allocates the workspaces
+    DL.run_FT_multi([batch_chains(b) for b in bases], max(a.warmup, 3), precision=prec, use_graph=True)
+    groups = [batch_chains(b) for b in bases]
+    smi_path = os.path.join(REPO, ".bench_clocks_batch.csv")
+    sp, sf = clocks_sampler_start(smi_path)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    DL.run_FT_multi(groups, steps, precision=prec, use_graph=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = clocks_sampler_stop(sp, sf, smi_path, 0)
+    try:
+        os.remove(smi_path)
+    except OSError:
+        pass
+    ms = e0.elapsed_time(e1)
+    n_chains = sum(len(g) for g in groups)
+    applies = 2 * n_chains * steps
+    lengths = {names[i]: [len(L.a_coeffs) for L in g] for i, g in enumerate(groups)}
+    # comparisons on a short run: the same run without the graph, and the host-driven loop
+    cmp_steps = 20
+    cmp = {}
+    for label, fn in (("multi_no_graph", lambda gs: DL.run_FT_multi(gs, cmp_steps, precision=prec, use_graph=False)),
+                      ("multi_graph", lambda gs: DL.run_FT_multi(gs, cmp_steps, precision=prec, use_graph=True)),
+                      ("host_loop_per_system", lambda gs: [DL.run_FT_batched(g, cmp_steps, precision=prec) for g in gs])):
+        gs = [batch_chains(b) for b in bases]
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn(gs)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t = e0.elapsed_time(e1)
+        cmp[label] = {"ms": round(t, 1), "apply_L_per_s": 2 * n_chains * cmp_steps / (t / 1e3)}
+    # accuracy of the mixed chains (first `steps` steps) against FP64 chains, small systems
+    w, eta = RS.gf_grid()
+    acc = {}
+    for i in range(2):
+        ref = batch_chains(bases[i])
+        DL.run_FT_multi([ref], steps, precision="fp64", use_graph=True)
+        errs = []
+        for Lm, Lr in zip(groups[i], ref):
+            k = min(len(Lm.a_coeffs), len(Lr.a_coeffs))
+            gm = _gf_truncated(Lm, k, w, eta)
+            gr = _gf_truncated(Lr, k, w, eta)
+            errs.append(float(np.abs(gm - gr).max() / np.abs(gr).max()))
+        acc[names[i]] = {"g_rel_err_max_over_chains": max(errs), "g_rel_err_median_over_chains": float(np.median(errs))}
+    acc[names[2]] = "the 4x4x4 benchmark system: see the default run's accuracy_vs_fp64 (same kernels and precision)"
+    line = {"metric": "apply_L/s, 48 chains over three uneven systems, one graph-captured run", "value": applies / (ms / 1e3),
+            "unit": "apply_L/s", "n_gpus": 1, "steps": steps, "warmup": max(a.warmup, 3), "ms_total": ms,
+            "higher_is_better": True, "dtype": f"{prec} contractions (f32 accumulate) + f64 recurrence",
+            "data": "synthetic (seeded rock-salt ensembles, T = 300 K)",
+            "config": {"workload": "16 chains (3 IR, 6 Raman, 7 random R1) on each of " + "; ".join(names),
+                       "graph": "2 eager steps, then one CUDA graph launch per step for all systems",
+                       "streams": "one per system, forked from and joined into the run's stream"},
+            "chain_lengths": lengths, "comparison_20_steps": cmp, "accuracy_vs_fp64": acc, "clocks": clocks}
+    print(json.dumps(line))
+
+
+def _gf_truncated(L, k, w, eta):
+    a, b, c = list(L.a_coeffs), list(L.b_coeffs), list(L.c_coeffs)
+    L.a_coeffs, L.b_coeffs, L.c_coeffs = a[:k], b[:k - 1], c[:k - 1]
+    g = L.get_green_function_continued_fraction(w, use_terminator=False, smearing=eta)
+    L.a_coeffs, L.b_coeffs, L.c_coeffs = a, b, c
+    return g
+
+
 def main():
     a = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -249,6 +362,13 @@ def main():
         line = run_reference_arm(a, rank)
         if line is not None:
             print(json.dumps(line))
+        return
+
+    if a.batch_systems:
+        import torch
+        torch.cuda.set_device(local_rank)
+        if rank == 0:
+            run_batch_systems(a)
         return
 
     from tdscha_b200 import rocksalt as RS

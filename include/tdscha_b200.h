@@ -171,6 +171,37 @@ int tdscha_lanczos_step_device_noalloc(int nc, long long len, const double *Lq, 
                                        double *q_next, double *p_next, double *sc_out, void *stream);
 
 /*
+ * Many bi-conjugate steps of many chains over several systems, without returning to the host:
+ * the step loop of Lanczos.run_FT (Modules/DynamicalLanczos.py:5843-6374, n_rep_orth = 0) for
+ * every chain of every system, advanced in lockstep.  The reference runs one chain per call; this
+ * entry point has no single counterpart (run_FT per chain is the reference-side equivalent).
+ *
+ * Per system (one resident ensemble, nc = n_chains <= 32 chains, len = n + n(n+1)):
+ *   qp    device (4, nc, len): q_k, p_k, q_{k-1}, p_{k-1} of every chain (in, advanced in place)
+ *   sc    device (nc, 6): the recurrence history of tdscha_lanczos_step_device's sc_in (in/out)
+ *   coef  device (n_steps, nc, 4): [a_k, b_k, c_k, s_norm_{k+1}] of every step (out)
+ * Each step is one batched apply of the 2 nc vectors [q; p] (transpose 0 for q, 1 for p), one
+ * batched recurrence and the history update.  Systems run on their own streams forked from and
+ * joined into `stream`.  With use_graph != 0 the first two steps run eagerly and one step of all
+ * systems is captured into a CUDA graph launched once per remaining step.  A chain whose |b| or
+ * |c| falls below 1e-12 ends there as in run_FT (:6129-6141): its last coef row is that step's,
+ * later rows are left untouched, its qp and sc stay at that step (its vectors still go through
+ * the batched apply, whose other chains are unaffected).  Returns after the last step completed.
+ */
+typedef struct tdscha_run_system {
+    tdscha_ensemble *ens;
+    int n_chains;
+    double *qp;
+    double *sc;
+    double *coef;
+    tdscha_apply_opts opts;
+    int precision;
+} tdscha_run_system;
+
+int tdscha_lanczos_run_device(int n_systems, const tdscha_run_system *systems, int n_steps, int use_graph,
+                              void *stream);
+
+/*
  * Continued-fraction Green function (DynamicalLanczos.py:4951-5047) on the device.
  * a (n_iter), b (n_iter-1 or more), c (same as b or NULL = symmetric) FP64 device arrays;
  * omega (n_w) device; gf_out (2 * n_w) interleaved re, im.

@@ -13,6 +13,7 @@
 #include <cuComplex.h>
 #include <mutex>
 
+#include "apply.cuh"
 #include "common.cuh"
 #include "ensemble.cuh"
 
@@ -161,24 +162,33 @@ static int grid_for(long long total, int threads = 256) {
 
 int apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose_h, const tdscha_apply_opts *opts,
                         int precision, double *out, cudaStream_t st, void *scratch, size_t scratch_bytes) {
-    TD_CHECK(e && psi && out && transpose_h, TDSCHA_EINVAL, "NULL argument");
-    TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+    TD_CHECK(e && psi && out && transpose_h && scratch, TDSCHA_EINVAL, "NULL argument");
+    TD_CHECK(nb > 0 && nb <= 64, TDSCHA_EINVAL, "1..64 vectors per apply call (got %d)", nb);
+    TD_CHECK(scratch_bytes > 256, TDSCHA_EINVAL, "apply scratch too small");
+    // scratch: transpose flags (nb ints, 256 bytes), then the work of apply_full_L_device_flags
+    uint8_t *s = static_cast<uint8_t *>(scratch);
+    int *tr_d = reinterpret_cast<int *>(s);
+    TD_CUDA(cudaMemcpyAsync(tr_d, transpose_h, nb * sizeof(int), cudaMemcpyHostToDevice, st));
+    return apply_full_L_device_flags(e, nb, psi, tr_d, opts, precision, out, st, reinterpret_cast<double *>(s + 256),
+                                     scratch_bytes - 256);
+}
+
+// apply_full_L with the transpose flags already on the device (no host transfer: graph-capturable);
+// work: R (nb n), Ys (nb n^2), f (nb n), D (nb n^2) doubles.
+int apply_full_L_device_flags(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
+                              int precision, double *out, cudaStream_t st, double *work, size_t work_bytes) {
+    TD_CHECK(e && psi && out && tr_d && work, TDSCHA_EINVAL, "NULL argument");
+    TD_CHECK(nb > 0 && nb <= 64, TDSCHA_EINVAL, "1..64 vectors per apply call (got %d)", nb);
     tdscha_apply_opts o{0, 0, 0, 0, 0, 0.0};
     if (opts) o = *opts;
     const int n = e->n;
     const long long P = (long long)n * (n + 1) / 2;
     const long long len = n + 2 * P;
-    // scratch: transpose flags (nb ints), R (nb n), Ys (nb n^2), f (nb n), D (nb n^2)
-    const size_t need = 256 + (size_t)nb * (2 * n + 2 * (size_t)n * n) * sizeof(double);
-    TD_CHECK(scratch_bytes >= need, TDSCHA_EINVAL, "apply scratch too small");
-    uint8_t *s = static_cast<uint8_t *>(scratch);
-    int *tr_d = reinterpret_cast<int *>(s);
-    double *R = reinterpret_cast<double *>(s + 256);
+    TD_CHECK(work_bytes >= (size_t)nb * (2 * n + 2 * (size_t)n * n) * sizeof(double), TDSCHA_EINVAL, "apply work too small");
+    double *R = work;
     double *Ys = R + (size_t)nb * n;
     double *fav = Ys + (size_t)nb * n * n;
     double *dav = fav + (size_t)nb * n;
-    TD_CHECK(nb <= 64, TDSCHA_EINVAL, "at most 64 vectors per apply call");
-    TD_CUDA(cudaMemcpyAsync(tr_d, transpose_h, nb * sizeof(int), cudaMemcpyHostToDevice, st));
     e->prof.launches[ST_OTHER] += o.ignore_v3 ? 1 : 2;
     if (!o.ignore_v3) {
         prologue_kernel<<<grid_for((long long)nb * P), 256, 0, st>>>(nb, n, len, psi, tr_d, e->w, e->T, o.use_wigner, R, Ys);

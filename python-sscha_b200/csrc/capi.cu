@@ -4,6 +4,7 @@
 #include <cstring>
 #include <vector>
 
+#include "apply.cuh"
 #include "common.cuh"
 #include "ensemble.cuh"
 #include "modes.cuh"
@@ -20,21 +21,6 @@ void set_error(const char *fmt, ...) {
     va_end(ap);
 }
 void clear_error() { g_err[0] = 0; }
-
-int apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, const int *transpose_h, const tdscha_apply_opts *opts,
-                        int precision, double *out, cudaStream_t st, void *scratch, size_t scratch_bytes);
-size_t apply_scratch_bytes(const tdscha_ensemble *e, int nb);
-int apply_prologue_device(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
-                          double *R, double *Ys, cudaStream_t st);
-int apply_epilogue_device(tdscha_ensemble *e, int nb, const double *psi, const int *tr_d, const tdscha_apply_opts *opts,
-                          const double *fav, const double *dav, double *out, cudaStream_t st);
-int lanczos_step_device(int nc, long long len, const double *Lq, const double *pL, const double *q, const double *p,
-                        const double *q_prev, const double *p_prev, const double *sc_in, const double *mask, double *q_next,
-                        double *p_next, double *sc_out, cudaStream_t st, double *scratch, size_t scratch_bytes);
-size_t lanczos_scratch_bytes(int nc);
-int continued_fraction_device(int n_iter, const double *a, const double *b, const double *c, int n_b, int n_c, int n_w,
-                              const double *omega, int use_terminator, int last_average, double smearing, int use_wigner,
-                              int reverse_L, double shift_value, double modulus, double *gf_out, cudaStream_t st);
 
 // Scratch owned by the library for the calls that need temporaries (grown on demand, per device).
 struct Scratch {
@@ -202,6 +188,11 @@ int tdscha_apply_epilogue_device(tdscha_ensemble *e, int nb, const double *psi, 
     int *tr_d = nullptr;
     TD_TRY(upload_flags(nb, transpose, st, &tr_d));
     return apply_epilogue_device(e, nb, psi, tr_d, opts, f_av, d2v_av, out, st);
+}
+
+int tdscha_lanczos_run_device(int n_systems, const tdscha_run_system *systems, int n_steps, int use_graph, void *stream) {
+    clear_error();
+    return lanczos_run_device(n_systems, systems, n_steps, use_graph, static_cast<cudaStream_t>(stream));
 }
 
 int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const double *pL, const double *q, const double *p,

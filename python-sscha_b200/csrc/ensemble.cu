@@ -590,47 +590,73 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     const Format fmt = format_of(precision);
     const int nprod = products_of(precision);
     const bool lo = needs_lo(precision);
-    // Configuration chunk: all configurations when their operands fit in half of the free memory
-    // (then they stay resident between calls), else chunks of Nc whose operands are rebuilt from
-    // the resident X, G, Y per (symmetry chunk, configuration chunk).  TDSCHA_CONFIG_CHUNK forces a
-    // chunk size (tuning and tests).
-    size_t free_b = 0, tot_b = 0;
-    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
-    long long Nc = e->N;
-    const char *env_chunk = getenv("TDSCHA_CONFIG_CHUNK");
-    if (env_chunk && atoll(env_chunk) > 0 && atoll(env_chunk) < e->N) {
-        Nc = atoll(env_chunk);
-    } else if (!e->ops[fmt].built &&
-               operand_bytes(e, e->N, fmt, lo) > (free_b + e->ws.bytes + e->chunk_ops.bytes) / 2) {
-        // memory this call may use: free + its own workspace and chunk buffer (so every call plans alike)
-        const long long per_conf = 2 * (e->Kp + e->P + e->np + e->n) * (long long)format_bytes(fmt) * (lo ? 2 : 1);
-        const long long fit = (long long)((free_b + e->ws.bytes + e->chunk_ops.bytes) * 0.4) / per_conf;
-        Nc = std::min<long long>(e->N, std::max<long long>(32, fit / 32 * 32));
-    }
-    const bool chunked = Nc < e->N;
-    OperandSet co;
-    if (chunked) {
-        const size_t need = operand_bytes(e, Nc, fmt, lo);
-        if (e->chunk_ops.bytes < need) {
-            if (e->chunk_ops.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->chunk_ops.base); e->chunk_ops = Workspace(); }
-            TD_CUDA(cudaMalloc(&e->chunk_ops.base, need));
-            e->chunk_ops.bytes = need;
-        }
-        TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
-    } else {
-        TD_TRY(ensure_operands(e, fmt, lo, st));
-        co = e->ops[fmt];
-    }
-
     // fold chunking over symmetries: Jf symmetries per partial, at most 64 partials
     const int Jf = std::max(16, ceil_div(e->N_sym, 64));
     const int nf_total = ceil_div(e->N_sym, Jf);
-    // GEMM chunk over symmetries: a multiple of Jf whose workspace fits in the budget
-    const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
-    int Jc = (int)round_up(e->N_sym, Jf);
-    while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo, Nc).total > budget) Jc = (int)round_up(Jc / 2, Jf);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    TD_CUDA(cudaStreamIsCapturing(st, &cap));
+    long long Nc = e->N;
+    int Jc = 0;
+    OperandSet co;
+    if (cap != cudaStreamCaptureStatusNone) {
+        // inside a CUDA graph capture: the plan and buffers of the previous (eager) call, unchanged
+        const AvgPlan &pl = e->plan;
+        TD_CHECK(pl.valid && pl.nb == nb && pl.fmt == (int)fmt && pl.lo == lo, TDSCHA_EINVAL,
+                 "graph capture of the averages needs an earlier call with the same batch (%d) and precision", nb);
+        Nc = pl.Nc;
+        Jc = pl.Jc;
+        if (Nc < e->N) {
+            TD_CHECK(e->chunk_ops.bytes >= operand_bytes(e, Nc, fmt, lo), TDSCHA_EINVAL, "chunk buffer changed since the plan");
+        } else {
+            TD_CHECK(e->ops[fmt].built && (e->ops[fmt].has_lo || !lo), TDSCHA_EINVAL, "operands released since the plan");
+            co = e->ops[fmt];
+        }
+    } else {
+        // Configuration chunk: all configurations when their operands fit in half of the free memory
+        // (then they stay resident between calls), else chunks of Nc whose operands are rebuilt from
+        // the resident X, G, Y per (symmetry chunk, configuration chunk).  TDSCHA_CONFIG_CHUNK forces a
+        // chunk size (tuning and tests).
+        size_t free_b = 0, tot_b = 0;
+        TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+        const char *env_chunk = getenv("TDSCHA_CONFIG_CHUNK");
+        if (env_chunk && atoll(env_chunk) > 0 && atoll(env_chunk) < e->N) {
+            Nc = atoll(env_chunk);
+        } else if (!e->ops[fmt].built &&
+                   operand_bytes(e, e->N, fmt, lo) > (free_b + e->ws.bytes + e->chunk_ops.bytes) / 2) {
+            // memory this call may use: free + its own workspace and chunk buffer (so every call plans alike)
+            const long long per_conf = 2 * (e->Kp + e->P + e->np + e->n) * (long long)format_bytes(fmt) * (lo ? 2 : 1);
+            const long long fit = (long long)((free_b + e->ws.bytes + e->chunk_ops.bytes) * 0.4) / per_conf;
+            Nc = std::min<long long>(e->N, std::max<long long>(32, fit / 32 * 32));
+        }
+        if (Nc < e->N) {
+            const size_t need = operand_bytes(e, Nc, fmt, lo);
+            if (e->chunk_ops.bytes < need) {
+                if (e->chunk_ops.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->chunk_ops.base); e->chunk_ops = Workspace(); }
+                TD_CUDA(cudaMalloc(&e->chunk_ops.base, need));
+                e->chunk_ops.bytes = need;
+            }
+            TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+        } else {
+            TD_TRY(ensure_operands(e, fmt, lo, st));
+            co = e->ops[fmt];
+        }
+        // GEMM chunk over symmetries: a multiple of Jf whose workspace fits in the budget
+        const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
+        Jc = (int)round_up(e->N_sym, Jf);
+        while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo, Nc).total > budget) Jc = (int)round_up(Jc / 2, Jf);
+        e->plan.valid = true;
+        e->plan.nb = nb;
+        e->plan.fmt = (int)fmt;
+        e->plan.lo = lo;
+        e->plan.Nc = Nc;
+        e->plan.Jc = Jc;
+    }
+    const bool chunked = Nc < e->N;
     const WsLayout L = layout(e, nb, Jc, nf_total, fmt, lo, Nc);
-    TD_TRY(ensure_ws(e, L.total));
+    if (cap != cudaStreamCaptureStatusNone)
+        TD_CHECK(e->ws.bytes >= L.total, TDSCHA_EINVAL, "workspace changed since the plan");
+    else
+        TD_TRY(ensure_ws(e, L.total));
     uint8_t *W = static_cast<uint8_t *>(e->ws.base);
     void *B1_hi = W + L.B1_hi, *B1_lo = lo ? W + L.B1_lo : nullptr;
     void *r1_hi = W + L.r1_hi, *r1_lo = lo ? W + L.r1_lo : nullptr;

@@ -44,6 +44,16 @@ struct Workspace {
     size_t bytes = 0;
 };
 
+// Chunking plan of the last averages call (reused verbatim while a CUDA graph is being captured,
+// when neither device memory queries nor allocations may happen).
+struct AvgPlan {
+    bool valid = false;
+    int nb = 0, fmt = -1;
+    bool lo = false;
+    long long Nc = 0;
+    int Jc = 0;
+};
+
 // Stages of one averages call, for the optional CUDA-event profile.
 enum Stage : int { ST_TRANSFORM = 0, ST_GEMM_AB, ST_GEMM_CD, ST_WEIGHTS, ST_GEMM_Z, ST_GEMM_F, ST_FOLD, ST_OTHER, ST_COUNT };
 
@@ -84,6 +94,7 @@ struct tdscha_ensemble {
     tdscha::Workspace ws;
     tdscha::Workspace vjp_ws;                      // workspace of the averages' VJP
     tdscha::Workspace chunk_ops;                   // operands of one configuration chunk (large ensembles)
+    tdscha::AvgPlan plan;                          // chunking plan of the last averages call
     double *YX = nullptr;                          // [Y; X~] (2N x np), FP64, built by the first VJP
     double *XGT = nullptr;                         // [X^T; G^T] (2n x N), FP64, built by the first operand build
     cublasHandle_t cublas = nullptr;

@@ -23,6 +23,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <utility>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -491,15 +492,22 @@ static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long
     return 0;
 }
 
-// One tile-start counter per device (zeroed on the stream before every launch).
+// One tile-start counter per (device, stream), zeroed on the stream before every launch, so that
+// contractions running concurrently on different streams never share one.  A counter (256 bytes)
+// is allocated on a stream's first launch outside graph capture and kept for the process.
 static std::mutex g_sync_mutex;
-static unsigned *g_sync_counter[64] = {nullptr};
+static std::map<std::pair<int, cudaStream_t>, unsigned *> g_sync_counter;
 
-static int tile_sync_counter(int dev, unsigned **out) {
+static int tile_sync_counter(int dev, cudaStream_t st, bool capturing, unsigned **out) {
     std::lock_guard<std::mutex> lock(g_sync_mutex);
     TD_CHECK(dev >= 0 && dev < 64, TDSCHA_EINVAL, "device index %d out of range", dev);
-    if (!g_sync_counter[dev]) TD_CUDA(cudaMalloc(&g_sync_counter[dev], 256));
-    *out = g_sync_counter[dev];
+    auto it = g_sync_counter.find({dev, st});
+    if (it != g_sync_counter.end()) { *out = it->second; return 0; }
+    if (capturing) { *out = nullptr; return 0; }   // no allocation inside a capture: no alignment
+    void *slab = nullptr;
+    TD_CUDA(cudaMalloc(&slab, 256));
+    g_sync_counter[{dev, st}] = static_cast<unsigned *>(slab);
+    *out = static_cast<unsigned *>(slab);
     return 0;
 }
 
@@ -538,8 +546,11 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     const int num_m = ceil_div(M, BM);
     const unsigned sync_ns = tile_sync_budget_ns();
     const int accumulate = op.accumulate ? 1 : 0;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    TD_CUDA(cudaStreamIsCapturing(st, &cap));
+    const bool capturing = cap != cudaStreamCaptureStatusNone;
     unsigned *counter = nullptr;
-    if (sync_ns > 0 && tiles > grid.x) TD_TRY(tile_sync_counter(dev, &counter));
+    if (sync_ns > 0 && tiles > grid.x) TD_TRY(tile_sync_counter(dev, st, capturing, &counter));
     auto launch = [&](int gm) {
         if (counter) cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
         kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err,
@@ -550,7 +561,8 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     } else {
         int gm = 0;
         // trial runs write D, so an accumulating launch only reuses a group size tuned earlier
-        TD_TRY(tuned_group(TF32 ? 1 : 0, NPROD, M, N, K, num_m, tiles, sms, st, launch, !accumulate, &gm));
+        // (and a launch being captured into a CUDA graph runs nothing, so it cannot time trials)
+        TD_TRY(tuned_group(TF32 ? 1 : 0, NPROD, M, N, K, num_m, tiles, sms, st, launch, !accumulate && !capturing, &gm));
         launch(gm);
     }
     TD_CUDA(cudaGetLastError());

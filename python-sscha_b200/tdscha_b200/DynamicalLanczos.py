@@ -163,6 +163,16 @@ class Lanczos(object):
         self.krilov_basis = []
         self.arnoldi_matrix = []
 
+    def new_chain(self):
+        """Another chain on this initialised object's device ensemble: same ensemble, symmetries and
+        flags, fresh Lanczos state (for run_FT_batched / run_FT_multi, whose chains share an ensemble)."""
+        import copy
+        self._check_init()
+        L = copy.copy(self)
+        L.reset()
+        L.perturbation_modulus = 1
+        return L
+
     def init(self, use_symmetries=True):
         self.prepare_symmetrization(no_sym=not use_symmetries)
         self.initialized = True
@@ -880,3 +890,77 @@ def run_FT_batched(lanczos_list, n_iter, save_dir=None, save_each=5, verbose=Fal
             sys.stdout.flush()
     for s in state:
         s["L"].psi = s["q"].cpu().numpy()
+
+
+def run_FT_multi(groups, n_iter, precision=None, use_graph=True):
+    """Advance the bi-conjugate chains of several systems together for n_iter steps without returning
+    to the host (tdscha_lanczos_run_device): ``groups`` has one entry per system, a list of at most
+    32 Lanczos objects sharing that system's initialised device ensemble.  Every step is one batched
+    apply per system (all its chains' L q and L^T p), one batched recurrence and the history update;
+    systems run on their own streams and, with use_graph, one step of all systems is a single CUDA
+    graph launch after two eager steps.
+
+    Afterwards every chain holds its coefficients up to its first breakdown (|b| or |c| < 1e-12, where
+    run_FT stops, DynamicalLanczos.py:6129-6141) and psi = its last q.  Unlike run_FT the basis is not
+    kept: basis_Q / basis_P end with the last two vectors only (the full basis is only needed for
+    Gram-Schmidt re-orthogonalisation, n_rep_orth > 0, which MODE_B200 does not provide)."""
+    torch = _torch()
+    from . import _native
+    dev = "cuda"
+    systems, meta = [], []
+    for g, chains in enumerate(groups):
+        if not chains or len(chains) > 32:
+            raise ValueError(f"system {g}: 1..32 chains per system (got {len(chains)})")
+        L0 = chains[0]
+        for L in chains:
+            L._check_init()
+            if L.device_ensemble is not L0.device_ensemble:
+                raise ValueError(f"system {g}: the chains of one system must share its device ensemble")
+            flags = lambda o: (o.use_wigner, o.ignore_harmonic, o.ignore_v3, o.ignore_v4, o.reverse_L, o.shift_value)  # noqa: E731
+            if flags(L._opts()) != flags(L0._opts()):
+                raise ValueError(f"system {g}: the chains of one system must share the apply flags")
+            psi = np.asarray(L.psi)
+            if np.isnan(np.sum(psi ** 2)) or np.sum(psi ** 2) == 0:
+                raise ValueError("Error, you must initialize a perturbation to start the Lanczos.")
+        nc = len(chains)
+        ln = len(L0.psi)
+        qp = torch.zeros((4, nc, ln), dtype=torch.float64, device=dev)
+        sc = torch.zeros((nc, 6), dtype=torch.float64, device=dev)
+        for ci, L in enumerate(chains):
+            if len(L.a_coeffs) == 0:
+                v = np.asarray(L.psi, dtype=np.float64)
+                first = v / np.sqrt(np.sum(v * v))
+                L.basis_Q, L.basis_P, L.s_norm = [first], [first], [1]
+            L.basis_Q, L.basis_P, L.s_norm = list(L.basis_Q), list(L.basis_P), list(L.s_norm)
+            L.a_coeffs, L.b_coeffs, L.c_coeffs = list(L.a_coeffs), list(L.b_coeffs), list(L.c_coeffs)
+            qp[0, ci] = torch.as_tensor(np.asarray(L.basis_Q[-1]), device=dev)
+            qp[1, ci] = torch.as_tensor(np.asarray(L.basis_P[-1]), device=dev)
+            if len(L.basis_Q) > 1:
+                qp[2, ci] = torch.as_tensor(np.asarray(L.basis_Q[-2]), device=dev)
+                qp[3, ci] = torch.as_tensor(np.asarray(L.basis_P[-2]), device=dev)
+            sc[ci] = torch.tensor([L.c_coeffs[-1] if L.c_coeffs else 0.0, L.b_coeffs[-1] if L.b_coeffs else 0.0,
+                                   L.s_norm[-1], L.s_norm[-2] if len(L.s_norm) > 1 else 0.0,
+                                   L.c_coeffs[-2] if len(L.c_coeffs) > 1 else 1.0, float(len(L.a_coeffs))],
+                                  dtype=torch.float64)
+        coef = torch.zeros((n_iter, nc, 4), dtype=torch.float64, device=dev)
+        systems.append((L0.device_ensemble, qp, sc, coef, L0._opts(), precision or L0.precision))
+        meta.append(chains)
+    _native.lanczos_run(systems, n_iter, use_graph=use_graph)
+    torch.cuda.synchronize()
+    for (ens, qp, sc, coef, _, _), chains in zip(systems, meta):
+        cf = coef.cpu().numpy()
+        q_host = qp.cpu().numpy()
+        for ci, L in enumerate(chains):
+            for k in range(n_iter):
+                a, b, c, snew = (float(x) for x in cf[k, ci])
+                if np.isnan(a):
+                    raise ValueError("Invalid value encountered during the Lanczos.")
+                L.a_coeffs.append(a)
+                if abs(b) < __EPSILON__ or abs(c) < __EPSILON__:
+                    break
+                L.b_coeffs.append(b)
+                L.c_coeffs.append(c)
+                L.s_norm.append(snew)
+            L.basis_Q = [q_host[2, ci], q_host[0, ci]]
+            L.basis_P = [q_host[3, ci], q_host[1, ci]]
+            L.psi = q_host[0, ci]

@@ -27,6 +27,12 @@ class ApplyOpts(ctypes.Structure):
                 ("ignore_v4", ctypes.c_int), ("reverse_L", ctypes.c_int), ("shift_value", ctypes.c_double)]
 
 
+class RunSystem(ctypes.Structure):
+    """tdscha_run_system: one system of tdscha_lanczos_run_device."""
+    _fields_ = [("ens", vp), ("n_chains", ctypes.c_int), ("qp", vp), ("sc", vp), ("coef", vp), ("opts", ApplyOpts),
+                ("precision", ctypes.c_int)]
+
+
 class TdschaError(RuntimeError):
     pass
 
@@ -73,9 +79,10 @@ def load():
                                                ctypes.POINTER(ip), ctypes.POINTER(dp)]
     lib.tdscha_apply_prologue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp]
     lib.tdscha_apply_epilogue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp, vp]
+    lib.tdscha_lanczos_run_device.argtypes = [ctypes.c_int, ctypes.POINTER(RunSystem), ctypes.c_int, ctypes.c_int, vp]
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
-    for name in ("tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    for name in ("tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -211,6 +218,22 @@ def lanczos_step(Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_o
     check(lib.tdscha_lanczos_step_device(nc, length, ptr(Lq), ptr(pL), ptr(q), ptr(p), ptr(q_prev), ptr(p_prev),
                                          ptr(sc_in), ptr(mask), ptr(q_next), ptr(p_next), ptr(sc_out),
                                          _stream_ptr(stream)))
+
+
+def lanczos_run(systems, n_steps, use_graph=True, stream=None):
+    """tdscha_lanczos_run_device.  systems: list of (DeviceEnsemble, qp, sc, coef, ApplyOpts, precision)
+    with qp (4, nc, len), sc (nc, 6), coef (n_steps, nc, 4) contiguous float64 CUDA tensors."""
+    lib = load()
+    arr = (RunSystem * len(systems))()
+    for i, (ens, qp, sc, coef, opts, prec) in enumerate(systems):
+        nc = qp.shape[1]
+        if qp.shape[0] != 4 or tuple(sc.shape) != (nc, 6) or tuple(coef.shape) != (n_steps, nc, 4):
+            raise ValueError(f"system {i}: shapes qp {tuple(qp.shape)}, sc {tuple(sc.shape)}, coef {tuple(coef.shape)}")
+        for t in (qp, sc, coef):
+            if not t.is_contiguous() or str(t.dtype) != "torch.float64" or not t.is_cuda:
+                raise ValueError(f"system {i}: state tensors must be contiguous float64 CUDA tensors")
+        arr[i] = RunSystem(ens.handle.value, nc, qp.data_ptr(), sc.data_ptr(), coef.data_ptr(), opts, PREC[prec])
+    check(lib.tdscha_lanczos_run_device(len(systems), arr, int(n_steps), int(bool(use_graph)), _stream_ptr(stream)))
 
 
 def lanczos_step_noalloc(Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_out, stream=None):
