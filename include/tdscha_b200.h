@@ -171,6 +171,23 @@ int tdscha_lanczos_step_device_noalloc(int nc, long long len, const double *Lq, 
                                        double *q_next, double *p_next, double *sc_out, void *stream);
 
 /*
+ * The static (zero-frequency) L operator of the free-energy Hessian on nb static vectors
+ * psi (nb, n + n(n+1)/2) = (R, Upsilon packed upper row-major), FP64 device arrays:
+ *   tdscha_apply_L1_static_device  Lanczos.apply_L1_static(psi, inverse, power)
+ *                                  (Modules/DynamicalLanczos.py:2502-2565) with the exponent
+ *                                  already signed: power = -p for inverse = True
+ *   tdscha_apply_static_L_device   apply_anharmonic_static() (:3287-3354), plus apply_L1_static(psi)
+ *                                  when include_L1: the matvec of run_hessian_calculation
+ *                                  (:3973-4235) and of StaticHessian.apply_L
+ *                                  (Modules/StaticHessian.py:561-623); nb <= 64; averages in
+ *                                  `precision`, D4 term unless ignore_v4
+ */
+int tdscha_apply_L1_static_device(tdscha_ensemble *ens, int nb, const double *psi, double power, double *out,
+                                  void *stream);
+int tdscha_apply_static_L_device(tdscha_ensemble *ens, int nb, const double *psi, int ignore_v4, int include_L1,
+                                 int precision, double *out, void *stream);
+
+/*
  * Many bi-conjugate steps of many chains over several systems, without returning to the host:
  * the step loop of Lanczos.run_FT (Modules/DynamicalLanczos.py:5843-6374, n_rep_orth = 0) for
  * every chain of every system, advanced in lockstep.  The reference runs one chain per call; this

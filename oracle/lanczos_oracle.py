@@ -18,6 +18,10 @@ around the C kernel, following these reference lines (Modules/DynamicalLanczos.p
   run_FT (bi-conjugate Lanczos, GS off)    :5843-6374
   get_green_function_continued_fraction    :4951-5047
   prepare_perturbation / prepare_mode      :1963-2031
+  apply_L1_static / apply_anharmonic_static :2502-2565, 3287-3354
+  run_hessian_calculation ("cg")           :3973-4235
+and Modules/Tools.py:265-471 (minimum_residual_algorithm[_precond]), Modules/StaticHessian.py:561-690
+(the system matrix of StaticHessian).
 
 The symmetrised averages (the reference's ``sscha_HP_odd.GetPerturbAverageSym``,
 CModules/odd_corr_module.c:491-634) come from one of two C back ends:
@@ -332,6 +336,83 @@ class OracleLanczos:
                                    self.symmetries, self.N_degeneracy, self.degenerate_space,
                                    self.sym_block_id, backend=self.backend, n_threads=self.n_threads)
 
+    # ---- static operator of the free-energy Hessian (DynamicalLanczos.py:2502-2565, 3287-3354) ----
+    def apply_L1_static(self, psi, inverse=False, power=1):
+        """apply_L1_static: w^(2 power) on R, 1/Lambda^power on the packed Upsilon, with the
+        reference's quirks (both Bose factors masked by w_a; the equal-frequency branch multiplies
+        by an all-zero array taken before the factors are filled)."""
+        n = self.n_modes
+        assert len(psi) == n + n * (n + 1) // 2
+        out = np.zeros(psi.shape, dtype=np.float64)
+        if inverse:
+            power *= -1
+        out[:n] = psi[:n] * (self.w ** (2 * power))
+        b, a = upper_pairs(n)                  # i_b = row, i_a = col >= row
+        w_a, w_b = self.w[a], self.w[b]
+        n_a = np.zeros(w_a.shape)
+        n_b = np.zeros(w_a.shape)
+        mask_a = 0.01 * w_a * RY_TO_K > self.T
+        mask_b = 0.01 * w_a * RY_TO_K > self.T
+        diff = np.zeros(w_a.shape)
+        equal = np.abs(w_a - w_b) < 1e-8
+        w_equal = w_a[equal]
+        n_equal = n_a[equal]
+        if self.T > 0:
+            beta = RY_TO_K / self.T
+            with np.errstate(over="ignore", divide="ignore", invalid="ignore"):
+                n_a = 1 / (np.exp(w_a * beta) - 1)
+                n_b = 1 / (np.exp(w_b * beta) - 1)
+                n_a[mask_a] = 0
+                n_b[mask_b] = 0
+                diff[:] = (n_a - n_b) / (w_a - w_b)
+                diff[equal] = -beta * np.exp(w_equal * beta) * n_equal ** 2
+        lam = (n_a + n_b + 1) / (w_a + w_b) - diff
+        lam /= 4 * w_a * w_b
+        out[n:] = psi[n:] / lam ** power
+        return out
+
+    def apply_anharmonic_static(self):
+        """apply_anharmonic_static on the static vector self.psi = (R, packed Upsilon)."""
+        n = self.n_modes
+        Y1 = unpack_sym(self.psi[n:n + n * (n + 1) // 2], n)
+        R1 = self.psi[:n].copy()
+        n_mu = bose(self.w, self.T) if self.T > 1e-12 else np.zeros(n)
+        Y_w = 2 * self.w / (2 * n_mu + 1)
+        Y1 = -2 * np.einsum("ab, a, b -> ab", Y1, Y_w, Y_w)
+        f, d = self.averages(R1, Y1, 0 if self.ignore_v4 else 1)
+        out = np.zeros(self.psi.shape, dtype=np.float64)
+        out[:n] = -f
+        out[n:] = pack_upper(d)
+        return out
+
+    def apply_static_L(self, psi, eigen_shift=1.0):
+        """The matvec of run_hessian_calculation (DynamicalLanczos.py:4041-4051)."""
+        n = self.n_modes
+        self.psi = psi.copy()
+        self.psi[n:] *= eigen_shift
+        ret = self.apply_L1_static(self.psi)
+        ret += self.apply_anharmonic_static()
+        ret[n:] *= eigen_shift
+        return ret
+
+    def static_green_function(self, eigen_shift=1, max_iters=1000, use_preconditioning=True):
+        """The rows of the one-phonon static Green function of run_hessian_calculation with
+        algorithm "cg" (DynamicalLanczos.py:3973-4218): one minimum-residual solve per mode."""
+        n = self.n_modes
+        ln = n + n * (n + 1) // 2
+        A = lambda x: self.apply_static_L(x, eigen_shift)                         # noqa: E731
+        M = lambda x: self.apply_L1_static(x, inverse=True, power=0.5)             # noqa: E731
+        G = np.zeros((n, n))
+        for i in range(n):
+            b = np.zeros(ln)
+            b[i] = 1
+            if not use_preconditioning:
+                res = minimum_residual_algorithm(A, b.copy(), b.copy(), max_iters=max_iters)
+            else:
+                res = minimum_residual_algorithm_precond(A, b.copy(), M, max_iters=max_iters)
+            G[i, :] = res[:n]
+        return G
+
     # ---- anharmonic part (DynamicalLanczos.py:2891-3281) ----
     def apply_anharmonic_FT(self, transpose=False):
         n = self.n_modes
@@ -493,3 +574,106 @@ class OracleLanczos:
         if not self.use_wigner:
             return gf * self.perturbation_modulus
         return (-np.real(gf) + 1j * np.imag(gf)) * self.perturbation_modulus
+
+
+# ----------------------------------------------------------------------------------------------
+# the reference's minimum residual solver (Modules/Tools.py:265-471), on plain callables
+# ----------------------------------------------------------------------------------------------
+def minimum_residual_algorithm(A, b, x0, max_iters=100, conv_thr=1e-6, callback=None):
+    """Tools.minimum_residual_algorithm with precond = None (the only form its callers use)."""
+    r1 = b - A(x0)
+    b_prec = b.copy()
+    r1_bar = A(r1)
+    z1 = r1.copy()
+    p1 = r1.copy()
+    p1_bar = r1_bar.copy()
+    x = x0.copy()
+    iters = 1
+    converged = False
+    while iters < max_iters and not converged:
+        Ap = p1_bar
+        Ap_bar = A(p1_bar)
+        alpha = r1_bar.dot(z1) / (p1_bar.dot(Ap))
+        x[:] += alpha * p1
+        if callback is not None:
+            callback(x, iters)
+        r = r1 - alpha * Ap
+        rbar = r1_bar - alpha * Ap_bar
+        r_norm = np.sqrt(r.dot(r)) / np.sqrt(b_prec.dot(b_prec))
+        z = r.copy()
+        zbar = rbar.copy()
+        beta = rbar.dot(z) / (r1_bar.dot(z1))
+        p1[:] = z + beta * p1
+        p1_bar[:] = zbar + beta * p1_bar
+        r1[:] = r
+        r1_bar[:] = rbar
+        z1[:] = z
+        converged = r_norm < conv_thr
+        iters += 1
+    return x
+
+
+def minimum_residual_algorithm_precond(A, b, precond_half, x0=None, **kwargs):
+    """Tools.minimum_residual_algorithm_precond: the solve of M A M x~ = M b, x = M x~."""
+    A_tilde = lambda x: precond_half(A(precond_half(x)))     # noqa: E731
+    b_tilde = precond_half(b)
+    if x0 is None:
+        x0 = b_tilde.copy()
+    x_tilde = minimum_residual_algorithm(A_tilde, b_tilde, x0, **kwargs)
+    return precond_half(x_tilde)
+
+
+# ----------------------------------------------------------------------------------------------
+# StaticHessian's system matrix (Modules/StaticHessian.py:561-690), plain loops, small n only
+# ----------------------------------------------------------------------------------------------
+def static_hessian_get_G_W(vector, n, ignore_W=False):
+    G = np.zeros((n, n))
+    counter = 0
+    for i in range(n):
+        for j in range(i, n):
+            G[i, j] = vector[counter]
+            G[j, i] = vector[counter]
+            counter += 1
+    if ignore_W:
+        return G
+    W = np.zeros((n, n, n))
+    for i in range(n):
+        for j in range(i, n):
+            for k in range(j, n):
+                v = vector[counter]
+                W[i, j, k] = W[i, k, j] = W[j, i, k] = W[j, k, i] = W[k, i, j] = W[k, j, i] = v
+                counter += 1
+    return G, W
+
+
+def static_hessian_get_vector(G, W):
+    n = G.shape[0]
+    out = []
+    for i in range(n):
+        for j in range(i, n):
+            out.append(G[i, j])
+    for i in range(n):
+        for j in range(i, n):
+            for k in range(j, n):
+                out.append(W[i, j, k])
+    return np.array(out)
+
+
+def static_hessian_apply_L(oracle, vect, preconditioner=False, inverse_preconditioner=False):
+    """StaticHessian.apply_L: the static L on each row (G^-1[i, :], W[i] packed)."""
+    n = oracle.n_modes
+    Ginv, W = static_hessian_get_G_W(vect, n)
+    for i in range(n):
+        vector = np.zeros(n + n * (n + 1) // 2)
+        vector[:n] = Ginv[i, :]
+        vector[n:] = pack_upper(W[i])
+        oracle.psi = vector
+        if not preconditioner and not inverse_preconditioner:
+            outv = oracle.apply_L1_static(vector)
+            outv += oracle.apply_anharmonic_static()
+        else:
+            power = 0.5 if preconditioner else -0.5
+            outv = oracle.apply_L1_static(vector, inverse=True, power=power)
+        Ginv[i, :] = outv[:n]
+        W[i] = unpack_sym(outv[n:], n)
+    return static_hessian_get_vector(Ginv, W)

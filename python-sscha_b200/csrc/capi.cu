@@ -190,6 +190,27 @@ int tdscha_apply_epilogue_device(tdscha_ensemble *e, int nb, const double *psi, 
     return apply_epilogue_device(e, nb, psi, tr_d, opts, f_av, d2v_av, out, st);
 }
 
+int tdscha_apply_L1_static_device(tdscha_ensemble *e, int nb, const double *psi, double power, double *out, void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    return apply_L1_static_device(e, nb, psi, power, out, static_cast<cudaStream_t>(stream));
+}
+
+int tdscha_apply_static_L_device(tdscha_ensemble *e, int nb, const double *psi, int ignore_v4, int include_L1, int precision,
+                                 double *out, void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CHECK(nb > 0 && nb <= 64, TDSCHA_EINVAL, "1..64 vectors per static apply (got %d)", nb);
+    TD_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t need = static_work_bytes(e, nb);
+    void *buf = nullptr;
+    TD_TRY(scratch_get(0, need, &buf));
+    TD_TRY(apply_static_L_device(e, nb, psi, ignore_v4, include_L1, precision, out, st, static_cast<double *>(buf), need));
+    return check_err_word(e, st);
+}
+
 int tdscha_lanczos_run_device(int n_systems, const tdscha_run_system *systems, int n_steps, int use_graph, void *stream) {
     clear_error();
     return lanczos_run_device(n_systems, systems, n_steps, use_graph, static_cast<cudaStream_t>(stream));

@@ -407,7 +407,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaDeviceSynchronize();
     void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->symP, e->symPT, e->d_offP, e->d_blk_start, e->d_blk_dim,
                   e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base,
-                  e->vjp_ws.base, e->YX, e->chunk_ops.base, e->XGT};
+                  e->vjp_ws.base, e->YX, e->chunk_ops.base, e->XGT, e->d_static_lam};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);

@@ -97,6 +97,7 @@ struct tdscha_ensemble {
     tdscha::AvgPlan plan;                          // chunking plan of the last averages call
     double *YX = nullptr;                          // [Y; X~] (2N x np), FP64, built by the first VJP
     double *XGT = nullptr;                         // [X^T; G^T] (2n x N), FP64, built by the first operand build
+    double *d_static_lam = nullptr;                // Lambda of the static L1 per packed pair (P), built on first use
     cublasHandle_t cublas = nullptr;
     size_t base_bytes = 0;
     tdscha::Profile prof;

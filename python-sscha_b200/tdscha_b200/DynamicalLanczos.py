@@ -652,6 +652,130 @@ class Lanczos(object):
         sign = -1 if self.reverse_L else 1
         return sign * matrix - sign * np.eye(N_size) * self.shift_value
 
+    # ---- static response: the free-energy Hessian (DynamicalLanczos.py:2502-2565, 3287-3354,
+    #      3973-4235) --------------------------------------------------------------------------
+    def _static_len(self):
+        n = self.n_modes
+        return n + n * (n + 1) // 2
+
+    def apply_L1_static(self, psi, inverse=False, power=1):
+        """Harmonic part of the static L: w^(2 power) on R, 1/Lambda^power on the packed Upsilon
+        (tdscha_apply_L1_static_device, with the reference's Bose-mask quirks)."""
+        torch = _torch()
+        self._check_init()
+        psi = np.asarray(psi, dtype=TYPE_DP)
+        expected_dim = self._static_len()
+        assert len(psi) == expected_dim, f"\nError, for the static calculation the vector must be of dimension {expected_dim}, got {len(psi)}\n"
+        if inverse:
+            power *= -1
+        x = torch.as_tensor(psi, device="cuda").reshape(1, -1).contiguous()
+        out = torch.empty_like(x)
+        _native.apply_L1_static(self.device_ensemble, x, out, power)
+        return out.cpu().numpy().ravel()
+
+    def apply_anharmonic_static(self):
+        """Anharmonic part of the static L on the static vector self.psi = (R, packed Upsilon):
+        (-f_av, packed D_av) of R1 = R, Upsilon1 = -2 Yw Upsilon Yw."""
+        torch = _torch()
+        self._check_init()
+        x = torch.as_tensor(np.asarray(self.psi[:self._static_len()], dtype=TYPE_DP), device="cuda").reshape(1, -1).contiguous()
+        out = torch.empty_like(x)
+        _native.apply_static_L(self.device_ensemble, x, out, ignore_v4=self.ignore_v4, include_L1=False,
+                               precision=self.precision)
+        res = np.zeros(self.psi.shape, dtype=TYPE_DP)
+        res[:x.shape[1]] = out.cpu().numpy().ravel()
+        return res
+
+    def _static_apply_batched(self, X, eigen_shift=1.0, with_L1=True):
+        """The matvec of run_hessian_calculation on a (k, len) device batch."""
+        torch = _torch()
+        n = self.n_modes
+        Xs = X.clone()
+        Xs[:, n:] *= eigen_shift
+        out = torch.empty_like(Xs)
+        _native.apply_static_L(self.device_ensemble, Xs, out, ignore_v4=self.ignore_v4, include_L1=with_L1,
+                               precision=self.precision)
+        out[:, n:] *= eigen_shift
+        return out
+
+    def _static_precond_batched(self, X, power=0.5):
+        torch = _torch()
+        out = torch.empty_like(X)
+        _native.apply_L1_static(self.device_ensemble, X.contiguous(), out, -power)
+        return out
+
+    def run_hessian_calculation(self, verbose=True, eigen_shift=1, tol=5e-4, max_iters=1000, save_g=None, save_each=1,
+                                use_preconditioning=True, algorithm="cg"):
+        """Static susceptibility by one linear solve per mode, then its inverse: the mass-rescaled
+        free-energy Hessian (DynamicalLanczos.py:3973-4235).  With algorithm "cg" (the reference's
+        minimum-residual method, Tools.py:265-471) the n solves advance together: every iteration
+        applies the static L to all still-unconverged right-hand sides in batches of 64 on the
+        device.  "minimize" / "minimize-quad" run scipy's BFGS per mode on the device matvec, as
+        the reference does."""
+        G_one_phonon = self.static_green_function(verbose, eigen_shift, tol, max_iters, save_g, save_each,
+                                                  use_preconditioning, algorithm)
+        disp = np.max(np.abs(G_one_phonon - G_one_phonon.T))
+        assert disp < 1e-4, "Error, the resulting one-phonon Green function is not Hermitian."
+        G = 0.5 * (G_one_phonon + G_one_phonon.T)
+        return np.linalg.inv(G)
+
+    def static_green_function(self, verbose=True, eigen_shift=1, tol=5e-4, max_iters=1000, save_g=None, save_each=1,
+                              use_preconditioning=True, algorithm="cg"):
+        """The rows G[i, :] = (L_static^-1 e_i)[:n] that run_hessian_calculation symmetrises and
+        inverts (DynamicalLanczos.py:4024-4218), before its absolute hermiticity check (1e-4, which
+        trips on Green functions of order 1/w^2 in Rydberg units)."""
+        torch = _torch()
+        self._check_init()
+        n = self.n_modes
+        ln = self._static_len()
+        if verbose:
+            print("\n=====================\n HESSIAN CALCULATION \n=====================\n")
+        G_one_phonon = np.zeros((n, n), dtype=np.double)
+        alg = algorithm.lower()
+        if alg == "cg":
+            B = torch.zeros((n, ln), dtype=torch.float64, device="cuda")
+            B[torch.arange(n), torch.arange(n)] = 1.0
+            A = lambda X: self._static_apply_batched(X, eigen_shift)                  # noqa: E731
+            if not use_preconditioning:
+                res = minimum_residual_batched(A, B, B.clone(), max_iters=max_iters, verbose=verbose)
+            else:
+                M = self._static_precond_batched
+                res = minimum_residual_batched_precond(A, B, M, max_iters=max_iters, verbose=verbose)
+            G_one_phonon[:, :] = res[:, :n].cpu().numpy()
+        elif alg in ("minimize", "minimize-quad"):
+            import scipy.optimize
+
+            def matvec(x):
+                X = torch.as_tensor(x, device="cuda").reshape(1, -1).contiguous()
+                return self._static_apply_batched(X, eigen_shift).cpu().numpy().ravel()
+
+            for i in range(n):
+                b = np.zeros(ln)
+                b[i] = 1
+
+                def func_standard(x, b):
+                    Lx = matvec(x)
+                    return 0.5 * x.dot(Lx) - b.dot(x), Lx - b
+
+                def func_quad(x, b):
+                    r = matvec(x) - b
+                    return 0.5 * np.sum(r ** 2), matvec(r)
+
+                options = {"gtol": tol, "maxiter": max_iters, "disp": verbose, "norm": 2}
+                fn = func_standard if alg == "minimize" else func_quad
+                results = scipy.optimize.minimize(fn, b.copy(), args=(b,), method="bfgs", jac=True, options=options)
+                G_one_phonon[i, :] = results.x[:n]
+                if save_g is not None and i % save_each == 0:
+                    np.save(save_g, G_one_phonon)
+        else:
+            raise ValueError(f"""
+Error, algorithm type '{algorithm}' in subroutine run_biconjugate_gradient not implemented.
+       the only supported algorithms are ['bicgstab', 'bicg']
+""")
+        if save_g is not None:
+            np.save(save_g, G_one_phonon)
+        return G_one_phonon
+
     def get_static_frequency(self, smearing=0):
         """sqrt(1 / Re G(omega -> 0 + i eta)), negative when imaginary (DynamicalLanczos.py:5273-5307)."""
         gf = self.get_green_function_continued_fraction(np.array([0]), False, smearing=smearing)
@@ -964,3 +1088,57 @@ def run_FT_multi(groups, n_iter, precision=None, use_graph=True):
             L.basis_Q = [q_host[2, ci], q_host[0, ci]]
             L.basis_P = [q_host[3, ci], q_host[1, ci]]
             L.psi = q_host[0, ci]
+
+
+# ---- the reference's minimum-residual solver (Modules/Tools.py:265-471), batched over rows ----
+def minimum_residual_batched(A, B, X0, max_iters=100, conv_thr=1e-6, verbose=False, callback=None):
+    """Tools.minimum_residual_algorithm (precond = None) for every row of B at once: A maps a
+    (k, len) device batch to A applied to each row.  Each row runs the reference's iteration and
+    stops when its residual |r| / |b| falls below conv_thr (or at max_iters); the apply of one
+    iteration covers only the rows still running."""
+    torch = _torch()
+    r1 = B - A(X0)
+    b_norm = torch.sqrt((B * B).sum(1))
+    r1_bar = A(r1)
+    z1 = r1.clone()
+    p1 = r1.clone()
+    p1_bar = r1_bar.clone()
+    x = X0.clone()
+    active = torch.ones(B.shape[0], dtype=torch.bool, device=B.device)
+    iters = 1
+    while iters < max_iters:
+        idx = torch.nonzero(active).ravel()
+        if idx.numel() == 0:
+            break
+        Ap = p1_bar[idx]
+        Ap_bar = A(Ap.contiguous())
+        alpha = (r1_bar[idx] * z1[idx]).sum(1) / (Ap * Ap).sum(1)
+        x[idx] += alpha[:, None] * p1[idx]
+        if callback is not None:
+            callback(x, iters)
+        r = r1[idx] - alpha[:, None] * Ap
+        rbar = r1_bar[idx] - alpha[:, None] * Ap_bar
+        r_norm = torch.sqrt((r * r).sum(1)) / b_norm[idx]
+        beta = (rbar * r).sum(1) / (r1_bar[idx] * z1[idx]).sum(1)
+        p1[idx] = r + beta[:, None] * p1[idx]
+        p1_bar[idx] = rbar + beta[:, None] * p1_bar[idx]
+        r1[idx] = r
+        r1_bar[idx] = rbar
+        z1[idx] = r
+        active[idx[r_norm < conv_thr]] = False
+        if verbose:
+            print(f"Iteration {iters}: {int(active.sum())} of {B.shape[0]} still running, max residual "
+                  f"{float(r_norm.max()):.3e}")
+        iters += 1
+    if bool(active.any()):
+        print(f"WARNING: cg did not converge after {max_iters} iterations for {int(active.sum())} right-hand sides.")
+    return x
+
+
+def minimum_residual_batched_precond(A, B, precond_half, X0=None, **kwargs):
+    """Tools.minimum_residual_algorithm_precond, batched: solve M A M x~ = M b, x = M x~."""
+    A_tilde = lambda X: precond_half(A(precond_half(X)))     # noqa: E731
+    B_tilde = precond_half(B)
+    if X0 is None:
+        X0 = B_tilde.clone()
+    return precond_half(minimum_residual_batched(A_tilde, B_tilde, X0, **kwargs))

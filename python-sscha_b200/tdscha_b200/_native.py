@@ -79,10 +79,12 @@ def load():
                                                ctypes.POINTER(ip), ctypes.POINTER(dp)]
     lib.tdscha_apply_prologue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp]
     lib.tdscha_apply_epilogue_device.argtypes = [vp, ctypes.c_int, vp, ip, ctypes.POINTER(ApplyOpts), vp, vp, vp, vp]
+    lib.tdscha_apply_L1_static_device.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, vp]
+    lib.tdscha_apply_static_L_device.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.tdscha_lanczos_run_device.argtypes = [ctypes.c_int, ctypes.POINTER(RunSystem), ctypes.c_int, ctypes.c_int, vp]
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
-    for name in ("tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    for name in ("tdscha_apply_L1_static_device", "tdscha_apply_static_L_device", "tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -202,6 +204,33 @@ class DeviceEnsemble:
         check(self._lib.tdscha_apply_epilogue_device(self.handle, nb, psi.data_ptr(), _i(tr), ctypes.byref(opts),
                                                      f_av.data_ptr(), d_av.data_ptr(), out.data_ptr(),
                                                      _stream_ptr(stream)))
+
+
+def _static_check(ens, psi, out):
+    n = ens.n
+    ln = n + n * (n + 1) // 2
+    if psi.dim() != 2 or psi.shape[1] != ln or tuple(out.shape) != tuple(psi.shape):
+        raise ValueError(f"static vectors must be (nb, {ln}); got {tuple(psi.shape)} -> {tuple(out.shape)}")
+    for t in (psi, out):
+        if not t.is_contiguous() or str(t.dtype) != "torch.float64" or not t.is_cuda:
+            raise ValueError("static vectors must be contiguous float64 CUDA tensors")
+
+
+def apply_L1_static(ens, psi, out, power=1.0, stream=None):
+    """tdscha_apply_L1_static_device on (nb, n + n(n+1)/2) tensors (power already signed)."""
+    _static_check(ens, psi, out)
+    check(ens._lib.tdscha_apply_L1_static_device(ens.handle, psi.shape[0], psi.data_ptr(), float(power), out.data_ptr(),
+                                                 _stream_ptr(stream)))
+
+
+def apply_static_L(ens, psi, out, ignore_v4=False, include_L1=True, precision="fp64", stream=None):
+    """tdscha_apply_static_L_device on (nb, n + n(n+1)/2) tensors, in batches of 64 vectors."""
+    _static_check(ens, psi, out)
+    for k0 in range(0, psi.shape[0], 64):
+        k1 = min(psi.shape[0], k0 + 64)
+        check(ens._lib.tdscha_apply_static_L_device(ens.handle, k1 - k0, psi[k0:k1].data_ptr(), int(bool(ignore_v4)),
+                                                    int(bool(include_L1)), PREC[precision], out[k0:k1].data_ptr(),
+                                                    _stream_ptr(stream)))
 
 
 def _stream_ptr(stream):
