@@ -21,7 +21,8 @@ around the C kernel, following these reference lines (Modules/DynamicalLanczos.p
   apply_L1_static / apply_anharmonic_static :2502-2565, 3287-3354
   run_hessian_calculation ("cg")           :3973-4235
 and Modules/Tools.py:265-471 (minimum_residual_algorithm[_precond]), Modules/StaticHessian.py:561-690
-(the system matrix of StaticHessian).
+(the system matrix of StaticHessian), and the analytic L operator from explicit d3 / d4 tensors
+(get_full_L_operator_FT, :5454-5789).
 
 The symmetrised averages (the reference's ``sscha_HP_odd.GetPerturbAverageSym``,
 CModules/odd_corr_module.c:491-634) come from one of two C back ends:
@@ -677,3 +678,88 @@ def static_hessian_apply_L(oracle, vect, preconditioner=False, inverse_precondit
         Ginv[i, :] = outv[:n]
         W[i] = unpack_sym(outv[n:], n)
     return static_hessian_get_vector(Ginv, W)
+
+
+# ----------------------------------------------------------------------------------------------
+# the reference's analytic L operator from explicit d3 / d4 tensors (DynamicalLanczos.py:5454-5789)
+# ----------------------------------------------------------------------------------------------
+def explicit_L_operator_FT(o, debug_d3=None):
+    """get_full_L_operator_FT(symmetrize=False) of the reference, with its full n^3 / n^4 einsums
+    (small n only).  `o` carries X, Y, rho, w, T, n_modes and the flags use_wigner,
+    ignore_harmonic, ignore_v3, ignore_v4."""
+    n = o.n_modes
+    i_a = np.tile(np.arange(n), (n, 1)).ravel()
+    i_b = np.tile(np.arange(n), (n, 1)).T.ravel()
+    new_i_a = np.array([i_a[i] for i in range(len(i_a)) if i_a[i] >= i_b[i]])
+    new_i_b = np.array([i_b[i] for i in range(len(i_a)) if i_a[i] >= i_b[i]])
+    w_a, w_b = o.w[new_i_a], o.w[new_i_b]
+    N_w2 = len(w_a)
+    L = np.zeros((n + 2 * N_w2, n + 2 * N_w2))
+    if not o.ignore_harmonic:
+        L[:n, :n] = np.diag(o.w ** 2) if not o.use_wigner else -np.diag(o.w ** 2)
+    n_a = np.zeros(w_a.shape)
+    n_b = np.zeros(w_a.shape)
+    if o.T > 0:
+        n_a = 1 / (np.exp(w_a * 157887.32400374097 / o.T) - 1)
+        n_b = 1 / (np.exp(w_b * 157887.32400374097 / o.T) - 1)
+    sY, sA = n, n + N_w2
+    if not o.ignore_harmonic:
+        if not o.use_wigner:
+            L[sY:sA, sY:sA] = -np.diag(-w_a ** 2 - w_b ** 2 - (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1)))
+            L[sY:sA, sA:] = -np.diag(-(8 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1)))
+            L[sA:, sY:sA] = -np.diag(-(2 * n_a * n_b + n_a + n_b) * (2 * n_a * n_b + n_a + n_b + 1) * (2 * w_a * w_b)
+                                     / ((2 * n_a + 1) * (2 * n_b + 1)))
+            L[sA:, sA:] = -np.diag(-w_a ** 2 - w_b ** 2 + (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1)))
+        else:
+            L[sY:sA, sY:sA] = np.diag(-(w_a ** 2 + w_b ** 2 - 2 * w_a * w_b))
+            L[sA:, sA:] = np.diag(-(w_a ** 2 + w_b ** 2 + 2. * w_a * w_b))
+    N_eff = np.sum(o.rho)
+    Y_weighted = np.einsum("ia, i -> ia", o.Y, o.rho)
+    n_w = bose(o.w, o.T)
+    X_ups = np.einsum("ia, a -> ia", o.X, 2 * o.w / (1 + 2 * n_w))
+    ec = np.ones(N_w2)
+    ec[new_i_a != new_i_b] = 2
+    if not o.ignore_v3:
+        if debug_d3 is not None:
+            d3 = debug_d3
+        else:
+            d3n = np.einsum("ia, ib, ic -> abc", X_ups, X_ups, Y_weighted) / -N_eff
+            d3 = (d3n + np.einsum("abc->acb", d3n) + np.einsum("abc->bac", d3n) + np.einsum("abc->bca", d3n)
+                  + np.einsum("abc->cab", d3n) + np.einsum("abc->cba", d3n)) / 6
+        d3s = d3[new_i_a, new_i_b, :]
+        if not o.use_wigner:
+            L[sY:sA, :sY] = -np.einsum("ab, a -> ab", d3s, 2 * ((2 * n_a + 1) * w_b + (2 * n_b + 1) * w_a)
+                                       / ((2 * n_a + 1) * (2 * n_b + 1)))
+            L[sA:, :sY] = -np.einsum("ab, a -> ab", d3s, 2 * ((2 * n_a + 1) * w_b * n_b * (n_b + 1) + (2 * n_b + 1) * w_a
+                                                             * n_a * (n_a + 1)) / ((2 * n_a + 1) * (2 * n_b + 1)))
+            L[:sY, sY:sA] = -np.einsum("ab, a -> ba", d3s, (2 * n_b + 1) * (2 * n_a + 1) / (8 * w_a * w_b) * ec)
+        else:
+            chi_minus = (n_a - n_b) * (w_a - w_b) / (2 * w_a * w_b)
+            chi_plus = (1 + n_a + n_b) * (w_a + w_b) / (2 * w_a * w_b)
+            L[:sY, sY:sA] = np.einsum("ab, a -> ab", d3s, np.sqrt(-0.5 * chi_minus) * ec).T
+            L[:sY, sA:] = -np.einsum("ab, a -> ab", d3s, np.sqrt(0.5 * chi_plus) * ec).T
+            L[sY:sA, :sY] = np.einsum("ab, a -> ab", d3s, np.sqrt(-0.5 * chi_minus))
+            L[sA:, :sY] = -np.einsum("ab, a -> ab", d3s, np.sqrt(0.5 * chi_plus))
+    if not o.ignore_v4:
+        d4 = np.einsum("ia, ib, ic, id -> abcd", X_ups, X_ups, X_ups, Y_weighted)
+        d4 += np.einsum("ia, ib, ic, id -> abcd", X_ups, X_ups, Y_weighted, X_ups)
+        d4 += np.einsum("ia, ib, ic, id -> abcd", X_ups, Y_weighted, X_ups, X_ups)
+        d4 += np.einsum("ia, ib, ic, id -> abcd", Y_weighted, X_ups, X_ups, X_ups)
+        d4 /= -4 * N_eff
+        d4s = d4[new_i_a, new_i_b, :, :][:, new_i_a, new_i_b]
+        if not o.use_wigner:
+            left = -(2 * w_a * n_b + 2 * w_b * n_a + w_a + w_b) / (4 * (2 * n_a + 1) * (2 * n_b + 1))
+            right = (2 * n_a + 1) * (2 * n_b + 1) / (w_a * w_b)
+            L[sY:sA, sY:sA] += -np.einsum("a, ab, b -> ab", left, d4s, right * ec)
+            left1 = -(w_a * n_a * (n_a + 1) * (2 * n_b + 1) + w_b * n_b * (n_b + 1) * (2 * n_a + 1)) / (
+                4 * (2 * n_a + 1) * (2 * n_b + 1))
+            L[sA:, sY:sA] += -np.einsum("a, ab, b -> ab", left1, d4s, right * ec)
+        else:
+            chi_plus = (1 + n_a + n_b) * (w_a + w_b) / (2 * w_a * w_b)
+            chi_minus = (n_a - n_b) * (w_a - w_b) / (2 * w_a * w_b)
+            sp, sm = np.sqrt(0.5 * chi_plus), np.sqrt(-0.5 * chi_minus)
+            L[sY:sA, sY:sA] += -np.einsum("a, ab, b -> ab", sm, d4s, sm * ec)
+            L[sA:, sA:] += -np.einsum("a, ab, b -> ab", sp, d4s, sp * ec)
+            L[sY:sA, sA:] += np.einsum("a, ab, b -> ab", sm, d4s, sp * ec)
+            L[sA:, sY:sA] += np.einsum("a, ab, b -> ab", sp, d4s, sm * ec)
+    return L

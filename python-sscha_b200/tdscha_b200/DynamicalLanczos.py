@@ -593,16 +593,25 @@ class Lanczos(object):
 
     def get_full_L_operator_FT(self, verbose=False, debug_d3=None, symmetrize=True, overwrite_L_operator=True,
                                batch=64, max_bytes=16 << 30):
-        """The full L matrix (DynamicalLanczos.py:5454-5789), built column by column from batched
-        device applies of unit vectors, so it is exactly the operator that apply_full_L applies
-        (symmetrised averages, current flags).  Memory |psi|^2 x 8 B on the host."""
-        if debug_d3 is not None:
-            raise NotImplementedError("debug_d3: the explicit third-order tensor path is not part of the B200 mode")
+        """The full L matrix (DynamicalLanczos.py:5454-5789).  Memory |psi|^2 x 8 B on the host.
+
+        * symmetrize=False, or a debug_d3 tensor: the reference's analytic operator from the explicit
+          d3 / d4 tensors of the ensemble, unsymmetrised (explicit_L_operator_FT).
+        * symmetrize=True without debug_d3: the reference raises NotImplementedError unless
+          ignore_v3 and ignore_v4 (it cannot symmetrise d3 / d4); here the symmetrised operator is
+          built column by column from batched device applies of unit vectors, i.e. exactly the
+          operator that apply_full_L applies (current flags)."""
         torch = _torch()
         self._check_init()
         ln = len(self.psi)
         if ln * ln * 8 > max_bytes:
             raise MemoryError(f"the full L operator needs {ln * ln * 8 / 2**30:.1f} GiB (limit {max_bytes / 2**30:.1f} GiB)")
+        if debug_d3 is not None or not symmetrize:
+            L = self.explicit_L_operator_FT(debug_d3=debug_d3, symmetrize=symmetrize, verbose=verbose)
+            if overwrite_L_operator:
+                import scipy.sparse.linalg as sla
+                self.L_linop = sla.LinearOperator(L.shape, matvec=L.dot, rmatvec=lambda x: x.dot(L))
+            return L
         L = np.zeros((ln, ln), dtype=TYPE_DP)
         opts = self._opts()
         for c0 in range(0, ln, batch):
@@ -615,6 +624,111 @@ class Lanczos(object):
         if overwrite_L_operator:
             import scipy.sparse.linalg as sla
             self.L_linop = sla.LinearOperator(L.shape, matvec=L.dot, rmatvec=L.T.dot, dtype=TYPE_DP)
+        return L
+
+    def explicit_tensors_FT(self, debug_d3=None, need_d3=True, need_d4=True):
+        """The pair-space third- and fourth-order tensors of the reference's analytic operator
+        (DynamicalLanczos.py:5578-5700), with x = X o ups, y = rho Y, N_eff = sum rho and the packed
+        pairs p = (a_p, b_p) = (col, row) of the upper triangle:
+          d3[p, c] = -(1 / 3 N_eff) sum_i (x_a x_b y_c + x_a x_c y_b + x_b x_c y_a)
+                     (the six-permutation average of -x_a x_b y_c / N_eff)
+          d4[p, q] = -(1 / 4 N_eff) sum_i [ (x_a x_b)_p (x y + y x)_q + (x y + y x)_p (x_a x_b)_q ]
+        Both are FP64 GEMMs over the configurations on the device (O(P N n) and O(P^2 N)).
+        debug_d3 (n, n, n), when given, replaces d3 as in the reference."""
+        torch = _torch()
+        n = self.n_modes
+        r, c = np.triu_indices(n)
+        dev = "cuda"
+        n_w = 1 / (np.exp(self.w * __RyToK__ / self.T) - 1) if self.T > 0 else 0    # f_ups, :144-163
+        ups = 2 * self.w / (1 + 2 * n_w)
+        x = torch.as_tensor(np.asarray(self.X) * ups[None, :], device=dev)
+        y = torch.as_tensor(np.asarray(self.Y) * np.asarray(self.rho)[:, None], device=dev)
+        N_eff = float(np.sum(self.rho))
+        ra, cb = torch.as_tensor(c, device=dev), torch.as_tensor(r, device=dev)   # a = col, b = row
+        XX = (x[:, ra] * x[:, cb]).T.contiguous()                       # (P, N)
+        XY = (x[:, ra] * y[:, cb] + y[:, ra] * x[:, cb]).T.contiguous()   # (P, N)
+        d3 = d4 = None
+        if need_d3:
+            if debug_d3 is not None:
+                d3 = np.asarray(debug_d3)[c, r, :].copy()
+            else:
+                d3 = (-(XX @ y + XY @ x) / (3.0 * N_eff)).cpu().numpy()
+        if need_d4:
+            d4 = (-(XX @ XY.T + XY @ XX.T) / (4.0 * N_eff)).cpu().numpy()
+        return d3, d4
+
+    def explicit_L_operator_FT(self, debug_d3=None, symmetrize=False, verbose=False):
+        """The reference's analytic L operator (DynamicalLanczos.py:5454-5789) from the explicit,
+        unsymmetrised d3 / d4 tensors: harmonic blocks, d3 couplings between R and the pair
+        sectors, d4 couplings within the pair sectors, standard or Wigner representation, with the
+        reference's double-counting factors.  As in the reference, symmetrize=True raises for the
+        tensors it needs (no symmetrisation of d3 / d4 exists there)."""
+        n = self.n_modes
+        r, c = np.triu_indices(n)
+        w_a, w_b = self.w[c], self.w[r]
+        N_w2 = len(w_a)
+        start_Y, start_A = n, n + N_w2
+        L = np.zeros((n + 2 * N_w2, n + 2 * N_w2), dtype=TYPE_DP)
+        if not self.ignore_harmonic:
+            L[:n, :n] = np.diag(self.w ** 2) if not self.use_wigner else -np.diag(self.w ** 2)
+        n_a = np.zeros(w_a.shape, dtype=TYPE_DP)
+        n_b = np.zeros(w_a.shape, dtype=TYPE_DP)
+        if self.T > 0:
+            n_a = 1 / (np.exp(w_a * 157887.32400374097 / self.T) - 1)
+            n_b = 1 / (np.exp(w_b * 157887.32400374097 / self.T) - 1)
+        if not self.ignore_harmonic:
+            if not self.use_wigner:
+                X_ab_NI = -w_a ** 2 - w_b ** 2 - (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+                L[start_Y:start_A, start_Y:start_A] = -np.diag(X_ab_NI)
+                Y_ab_NI = -(8 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+                L[start_Y:start_A, start_A:] = -np.diag(Y_ab_NI)
+                X1_ab_NI = -(2 * n_a * n_b + n_a + n_b) * (2 * n_a * n_b + n_a + n_b + 1) * (2 * w_a * w_b) / (
+                    (2 * n_a + 1) * (2 * n_b + 1))
+                L[start_A:, start_Y:start_A] = -np.diag(X1_ab_NI)
+                Y1_ab_NI = -w_a ** 2 - w_b ** 2 + (2 * w_a * w_b) / ((2 * n_a + 1) * (2 * n_b + 1))
+                L[start_A:, start_A:] = -np.diag(Y1_ab_NI)
+            else:
+                L[start_Y:start_A, start_Y:start_A] = np.diag(-(w_a ** 2 + w_b ** 2 - 2 * w_a * w_b))
+                L[start_A:, start_A:] = np.diag(-(w_a ** 2 + w_b ** 2 + 2. * w_a * w_b))
+        need_d3, need_d4 = not self.ignore_v3, not self.ignore_v4
+        if need_d3 and symmetrize and debug_d3 is None:
+            raise NotImplementedError('The symmetrizaiton on d3 is not implemented')
+        if need_d4 and symmetrize:
+            raise NotImplementedError('The symmetrizaiton on d4 is not implemented')
+        d3, d4 = self.explicit_tensors_FT(debug_d3, need_d3, need_d4)
+        double = np.where(c != r, 2, 1)
+        if need_d3:
+            if not self.use_wigner:
+                Z_coeff = 2 * ((2 * n_a + 1) * w_b + (2 * n_b + 1) * w_a) / ((2 * n_a + 1) * (2 * n_b + 1))
+                L[start_Y:start_A, :start_Y] = -d3 * Z_coeff[:, None]
+                Z1_coeff = 2 * ((2 * n_a + 1) * w_b * n_b * (n_b + 1) + (2 * n_b + 1) * w_a * n_a * (n_a + 1)) / (
+                    (2 * n_a + 1) * (2 * n_b + 1))
+                L[start_A:, :start_Y] = -d3 * Z1_coeff[:, None]
+                X2_coeff = (2 * n_b + 1) * (2 * n_a + 1) / (8 * w_a * w_b)
+                L[:start_Y, start_Y:start_A] = -(d3 * (X2_coeff * double)[:, None]).T
+            else:
+                chi_minus = (n_a - n_b) * (w_a - w_b) / (2 * w_a * w_b)
+                chi_plus = (1 + n_a + n_b) * (w_a + w_b) / (2 * w_a * w_b)
+                L[:start_Y, start_Y:start_A] = (d3 * (np.sqrt(-0.5 * chi_minus) * double)[:, None]).T
+                L[:start_Y, start_A:] = -(d3 * (np.sqrt(0.5 * chi_plus) * double)[:, None]).T
+                L[start_Y:start_A, :start_Y] = d3 * np.sqrt(-0.5 * chi_minus)[:, None]
+                L[start_A:, :start_Y] = -d3 * np.sqrt(0.5 * chi_plus)[:, None]
+        if need_d4:
+            if not self.use_wigner:
+                X_left = -(2 * w_a * n_b + 2 * w_b * n_a + w_a + w_b) / (4 * (2 * n_a + 1) * (2 * n_b + 1))
+                right = (2 * n_a + 1) * (2 * n_b + 1) / (w_a * w_b) * double
+                L[start_Y:start_A, start_Y:start_A] += -(X_left[:, None] * d4 * right[None, :])
+                X1_left = -(w_a * n_a * (n_a + 1) * (2 * n_b + 1) + w_b * n_b * (n_b + 1) * (2 * n_a + 1)) / (
+                    4 * (2 * n_a + 1) * (2 * n_b + 1))
+                L[start_A:, start_Y:start_A] += -(X1_left[:, None] * d4 * right[None, :])
+            else:
+                chi_plus = (1 + n_a + n_b) * (w_a + w_b) / (2 * w_a * w_b)
+                chi_minus = (n_a - n_b) * (w_a - w_b) / (2 * w_a * w_b)
+                sp, sm = np.sqrt(0.5 * chi_plus), np.sqrt(-0.5 * chi_minus)
+                L[start_Y:start_A, start_Y:start_A] += -(sm[:, None] * d4 * (sm * double)[None, :])
+                L[start_A:, start_A:] += -(sp[:, None] * d4 * (sp * double)[None, :])
+                L[start_Y:start_A, start_A:] += sm[:, None] * d4 * (sp * double)[None, :]
+                L[start_A:, start_Y:start_A] += sp[:, None] * d4 * (sm * double)[None, :]
         return L
 
     def run_full_diag(self, number, discard_dyn=True, n_iter=100):
