@@ -29,8 +29,9 @@
 namespace tdscha {
 namespace {
 
-constexpr int THREADS = 512;
-constexpr int NW = THREADS / 32;
+// threads of a CTA per block class: small classes get small CTAs (several per SM) so that the
+// fixed per-symmetry cost (table copy, barriers) of their many small block pairs overlaps
+__host__ __device__ constexpr int threads_for(int MT) { return MT <= 2 ? 128 : (MT == 3 ? 256 : 512); }
 
 __host__ __device__ constexpr int ld_for(int d) { return d + ((4 - d % 8) + 8) % 8; }   // ld = 4 (mod 8)
 
@@ -76,7 +77,7 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 // rows x cols (cols a multiple of 4) of a (dp x dp) zero-padded fp32 table into shared memory with
 // leading dimension ld; rows / chunks beyond the table are zero filled
-template <int LD>
+template <int LD, int THREADS>
 __device__ __forceinline__ void copy_table(float *dst, const float *src, int dp, int rows, int cols) {
     const int cpr = cols >> 2;
     for (int e = threadIdx.x; e < rows * cpr; e += THREADS) {
@@ -159,6 +160,8 @@ struct TcShape {
     static constexpr int LD = ld_for(DM);
     static constexpr int ARR = DM * LD;   // floats per shared array
     static constexpr size_t SMEM = (size_t)8 * ARR * sizeof(float);
+    static constexpr int THREADS = threads_for(MT);
+    static constexpr int NW = THREADS / 32;
     // fold step-2 tiles per warp (16 x 8 tiles of the largest block pair of the class)
     static constexpr int TILES_PER_WARP = ((DM / 16) * (DM / 8) + NW - 1) / NW;
 };
@@ -170,12 +173,12 @@ struct TcShape {
 // T is staged in shared memory and written row by row to B1 (packed pairs, format fmt) for
 // global modes mu <= nu.
 template <int MT>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(threads_for(MT))
 transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__ pc, int nj, int j0, int JT,
                     const double *__restrict__ Ys, const double *__restrict__ R1, const double *__restrict__ ups, long long Kp,
                     long long np, Format fmt, void *B1_hi, void *B1_lo, void *r1_hi, void *r1_lo) {
     using S = TcShape<MT>;
-    constexpr int LD = S::LD, ARR = S::ARR;
+    constexpr int LD = S::LD, ARR = S::ARR, NW = S::NW;
     extern __shared__ __align__(16) float smf[];
     float *Yhi = smf, *Ylo = smf + ARR;               // Ys_k[b, c] (mu, nu)
     float *MThi = smf + 2 * ARR, *MTlo = smf + 3 * ARR;   // M1^T (nu', mu')
@@ -191,8 +194,8 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
     const float *Tb_base = tb.symPT + tb.offP[b], *Tc_base = tb.symPT + tb.offP[c];
     auto issue = [&](int j, int buf) {
         float *stb = Tab + buf * 2 * ARR, *stc = stb + ARR;
-        copy_table<LD>(stb, Tb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
-        copy_table<LD>(stc, Tc_base + (long long)j * dpc * dpc, dpc, DC, DC);
+        copy_table<LD, S::THREADS>(stb, Tb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
+        copy_table<LD, S::THREADS>(stc, Tc_base + (long long)j * dpc * dpc, dpc, DC, DC);
         cp_async_commit();
     };
     if (ja < jb) issue(ja, 0);
@@ -259,12 +262,12 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
 //   step 2  D += S_b . U           A = S_b (table as given), B[n][k] = U^T (split); fp32 per
 //                                  symmetry, summed over symmetries in fp64
 template <int MT>
-__global__ void __launch_bounds__(THREADS)
+__global__ void __launch_bounds__(threads_for(MT))
 fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__ pc, const float *__restrict__ Z, long long ldz,
                const float *__restrict__ F, long long ldf, const double *__restrict__ ups, int nj, int j0, int Jf, int nf_total,
                double *__restrict__ partD, double *__restrict__ partF) {
     using S = TcShape<MT>;
-    constexpr int LD = S::LD, ARR = S::ARR;
+    constexpr int LD = S::LD, ARR = S::ARR, NW = S::NW;
     extern __shared__ __align__(16) float smf[];
     float *UThi = smf, *UTlo = smf + ARR;   // U^T (nu', mu')
     float *Buf = smf + 2 * ARR;             // buffers x {S_b (mu, p), S_c (nu', nu), W (mu, nu)}
@@ -281,8 +284,8 @@ fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__
     const float *Pb_base = tb.symP + tb.offP[b], *Pc_base = tb.symP + tb.offP[c];
     auto issue = [&](int j, int buf) {
         float *snb = Buf + buf * 3 * ARR, *snc = snb + ARR, *wd = snc + ARR;
-        copy_table<LD>(snb, Pb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
-        copy_table<LD>(snc, Pc_base + (long long)j * dpc * dpc, dpc, DC, DC);
+        copy_table<LD, S::THREADS>(snb, Pb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
+        copy_table<LD, S::THREADS>(snc, Pc_base + (long long)j * dpc * dpc, dpc, DC, DC);
         const float *Zr = Z + ((long long)k * nj + (j - j0)) * ldz;
         for (int mu = warp; mu < DB; mu += NW)
             for (int nu = lane; nu < DC; nu += 32) {
@@ -373,7 +376,7 @@ int launch_transform_tc(const SymTables &t, const PairClasses &pc, int nb, int n
     auto kern = transform_tc_kernel<MT>;
     TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, JT), (unsigned)nb);
-    kern<<<grid, THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], nj, j0, JT, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
+    kern<<<grid, S::THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], nj, j0, JT, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
     TD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -387,7 +390,7 @@ int launch_fold_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, in
     auto kern = fold_tc_kernel<MT>;
     TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, Jf), (unsigned)nb);
-    kern<<<grid, THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
+    kern<<<grid, S::THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
     TD_CUDA(cudaGetLastError());
     return 0;
 }

@@ -73,3 +73,31 @@ def test_bad_blocks_raise_not_exit(cuda, mode10):
     ens = _dev_ens(d)
     with pytest.raises(_native.TdschaError, match="apply_D4"):
         ens.perturb_average(d["case0_R1"], d["case0_Y1"], 2, "fp64")
+
+
+@pytest.mark.parametrize("L,N", [(3, 40), (4, 24)])
+@pytest.mark.parametrize("precision,tol", [("bf16x3", 2e-5), ("tf32x3", 2e-5), ("tf32", 5e-3)])
+def test_mixed_modes_against_fp64_all_block_classes(cuda, L, N, precision, tol):
+    """The tensor-core symmetry transform / fold (mixed modes) against the FP64 CUDA-core path on
+    rock-salt 3x3x3 (blocks up to 42 modes) and 4x4x4 (up to 72): every padded block class."""
+    torch = cuda
+    from tdscha_b200 import _native
+    from tdscha_b200 import rocksalt as RS
+    s = RS.make_ensemble(L, N, seed=L)
+    ens = _native.DeviceEnsemble(s.X, s.Y, s.w, s.rho, s.T, s.symmetries, s.deg_space, s.blocks_ids)
+    n = s.X.shape[1]
+    rng = np.random.default_rng(9)
+    nb = 3
+    R = torch.as_tensor(rng.standard_normal((nb, n)), device="cuda")
+    A = rng.standard_normal((nb, n, n))
+    Y1 = torch.as_tensor(A + A.transpose(0, 2, 1), device="cuda")
+    out = {}
+    for prec in ("fp64", precision):
+        f = torch.empty((nb, n), dtype=torch.float64, device="cuda")
+        dv = torch.empty((nb, n, n), dtype=torch.float64, device="cuda")
+        ens.perturb_average_device(R, Y1, f, dv, 1, prec)
+        torch.cuda.synchronize()
+        out[prec] = (f.cpu().numpy(), dv.cpu().numpy())
+    ens.close()
+    assert _rel(out[precision][0], out["fp64"][0]) < tol
+    assert _rel(out[precision][1], out["fp64"][1]) < tol
