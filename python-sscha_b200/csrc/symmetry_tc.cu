@@ -100,6 +100,7 @@ __device__ __forceinline__ void warp_tile(float (&c)[4], const float *Ahi, const
     const uint32_t b_off = (uint32_t)(((n0 + r8) * LD + 4 * (q & 1)) * 4);
     const uint32_t ah_base = smem_u32(Ahi) + a_off, bh_base = smem_u32(Bhi) + b_off;
     const uint32_t al_base = A_SPLIT ? smem_u32(Alo) + a_off : 0u, bl_base = B_SPLIT ? smem_u32(Blo) + b_off : 0u;
+    float c_lh[4] = {0.f, 0.f, 0.f, 0.f}, c_hl[4] = {0.f, 0.f, 0.f, 0.f}, c_hh[4] = {0.f, 0.f, 0.f, 0.f};
 #pragma unroll 2
     for (int ks = 0; ks < kt; ++ks) {
         uint32_t ah[4], al[4], bh[2], bl[2];
@@ -121,10 +122,12 @@ __device__ __forceinline__ void warp_tile(float (&c)[4], const float *Ahi, const
 #pragma unroll
             for (int i = 0; i < 2; ++i) split_tf32(__uint_as_float(raw[i]), bh[i], bl[i]);
         }
-        mma_tf32(c, al, bh[0], bh[1]);   // small terms first
-        mma_tf32(c, ah, bl[0], bl[1]);
-        mma_tf32(c, ah, bh[0], bh[1]);
+        mma_tf32(c_lh, al, bh[0], bh[1]);   // three independent accumulation chains: the tensor
+        mma_tf32(c_hl, ah, bl[0], bl[1]);   // pipe overlaps them instead of waiting on one chain
+        mma_tf32(c_hh, ah, bh[0], bh[1]);
     }
+#pragma unroll
+    for (int e = 0; e < 4; ++e) c[e] += (c_lh[e] + c_hl[e]) + c_hh[e];   // small terms first
 }
 
 // a warp tile's accumulators, transposed ([n][m]) and split, into hi / lo arrays
