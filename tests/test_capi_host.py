@@ -158,3 +158,23 @@ def test_checkpoint_schema_round_trip(tmp_path):
     L2.load_status(f)
     assert L2.a_coeffs == [1.0, 2.0] and L2.c_coeffs == [0.25] and L2.reverse_L and L2.shift_value == 2e-4
     assert L2.perturbation_modulus == 3.5 and np.array_equal(np.asarray(L2.basis_Q), np.asarray(L.basis_Q))
+
+
+def test_argument_errors_of_run_and_static_entry_points():
+    """Argument checks of the multi-system run and the static operator come back as error codes
+    with a message before any device call (no GPU needed)."""
+    import ctypes
+    from tdscha_b200 import _native
+    lib = _native.load()
+    EINVAL = [k for k, v in _native.ERRORS.items() if v == "EINVAL"][0]
+    rc = lib.tdscha_lanczos_run_device(0, None, 5, 1, None)
+    assert rc != 0 and b"systems per run" in lib.tdscha_last_error()
+    rc = lib.tdscha_lanczos_run_device(1, None, 5, 1, None)
+    assert rc != 0 and b"bad run arguments" in lib.tdscha_last_error()
+    sysarr = (_native.RunSystem * 1)()           # NULL ensemble and buffers
+    rc = lib.tdscha_lanczos_run_device(1, sysarr, 5, 1, None)
+    assert rc != 0 and b"NULL argument" in lib.tdscha_last_error()
+    rc = lib.tdscha_apply_static_L_device(None, 1, None, 0, 1, 0, None, None)
+    assert rc != 0 and b"NULL ensemble" in lib.tdscha_last_error()
+    rc = lib.tdscha_apply_L1_static_device(None, 1, None, ctypes.c_double(1.0), None, None)
+    assert rc == EINVAL and b"NULL ensemble" in lib.tdscha_last_error()
