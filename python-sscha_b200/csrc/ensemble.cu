@@ -640,10 +640,13 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
             TD_TRY(ensure_operands(e, fmt, lo, st));
             co = e->ops[fmt];
         }
-        // GEMM chunk over symmetries: a multiple of Jf whose workspace fits in the budget
+        // GEMM chunk over symmetries: the largest multiple of Jf whose workspace fits in the budget
+        // (fewer symmetry chunks = fewer rebuilds of chunked operands and fewer small launches)
         const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
         Jc = (int)round_up(e->N_sym, Jf);
-        while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo, Nc).total > budget) Jc = (int)round_up(Jc / 2, Jf);
+        while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo, Nc).total > budget) Jc -= Jf;
+        const char *env_sym = getenv("TDSCHA_SYM_CHUNK");   // forces a smaller chunk (tuning and tests)
+        if (env_sym && atoi(env_sym) > 0) Jc = std::min(Jc, std::max(Jf, atoi(env_sym) / Jf * Jf));
         e->plan.valid = true;
         e->plan.nb = nb;
         e->plan.fmt = (int)fmt;

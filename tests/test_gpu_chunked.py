@@ -84,3 +84,25 @@ def test_split_k_equals_single_launch(cuda, rocksalt_l2, monkeypatch, precision)
     tol = 1e-5 if precision != "bf16" else 1e-2
     assert _rel(out["400"][0], out["0"][0]) < tol
     assert _rel(out["400"][1], out["0"][1]) < tol
+
+
+@pytest.mark.parametrize("precision", ["fp64", "bf16x3"])
+def test_symmetry_chunks_equal_one_chunk(cuda, rocksalt_l2, monkeypatch, precision):
+    """The symmetry dimension in chunks (what a tight workspace budget gives): 384 operations in
+    chunks of 80 (a multiple of the 16-operation fold group; last chunk 64) against one chunk."""
+    from tdscha_b200 import _native
+    d = rocksalt_l2
+    out = {}
+    for sc in (None, "80"):
+        if sc is None:
+            monkeypatch.delenv("TDSCHA_SYM_CHUNK", raising=False)
+        else:
+            monkeypatch.setenv("TDSCHA_SYM_CHUNK", sc)
+        ens = _native.DeviceEnsemble(d["X"], d["Y"], d["w"], d["rho"], d["T"], d["syms"], d["blocks"], d["blocks_ids"])
+        out[sc] = ens.perturb_average(d["case2_R1"], d["case2_Y1"], int(d["case2_d4"]), precision)
+        ens.close()
+    monkeypatch.delenv("TDSCHA_SYM_CHUNK", raising=False)
+    tol = 1e-12 if precision == "fp64" else 1e-5
+    assert _rel(out["80"][0], out[None][0]) < tol
+    assert _rel(out["80"][1], out[None][1]) < tol
+    assert _rel(out["80"][1], d["case2_d2v"]) < (1e-12 if precision == "fp64" else TOL[precision])
