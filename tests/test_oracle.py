@@ -85,3 +85,25 @@ def test_transpose_identity_on_dense_operator(rocksalt_l2):
         e = np.zeros(ln); e[r] = 1
         LTmat[:, ri] = L.apply_full_L(e, transpose=True)[cols]
     assert np.allclose(Lmat, LTmat.T, rtol=1e-8, atol=1e-10 * np.abs(Lmat).max())
+
+
+@pytest.mark.parametrize("use_wigner", [False, True])
+def test_explicit_operator_equals_applied_operator_on_the_oracle(rocksalt_l2, use_wigner):
+    """For the trivial symmetry group, the reference's analytic operator from explicit d3 / d4
+    tensors (einsum restatement) equals the operator its apply_full_L applies (C averages), column
+    by column: the two routes of the reference agree, which pins the explicit restatement."""
+    import types
+    d = rocksalt_l2
+    O = LO.OracleLanczos(d["X"], d["Y"], d["w"], d["rho"], d["T"])          # no symmetries
+    O.use_wigner = use_wigner
+    n = O.n_modes
+    ln = n + n * (n + 1)
+    La = np.zeros((ln, ln))
+    for i in range(ln):
+        e = np.zeros(ln)
+        e[i] = 1.0
+        La[:, i] = O.apply_full_L(e)
+    o = types.SimpleNamespace(X=O.X, Y=O.Y, rho=O.rho, w=O.w, T=O.T, n_modes=n, use_wigner=use_wigner,
+                              ignore_harmonic=False, ignore_v3=False, ignore_v4=False)
+    Lx = LO.explicit_L_operator_FT(o)
+    assert np.abs(Lx - La).max() <= 1e-10 * np.abs(La).max()
