@@ -107,3 +107,27 @@ def test_explicit_operator_equals_applied_operator_on_the_oracle(rocksalt_l2, us
                               ignore_harmonic=False, ignore_v3=False, ignore_v4=False)
     Lx = LO.explicit_L_operator_FT(o)
     assert np.abs(Lx - La).max() <= 1e-10 * np.abs(La).max()
+
+
+def test_static_limit_on_the_oracle(rocksalt_l2):
+    """The oracle's static operator (apply_L1_static + apply_anharmonic_static) and its dynamical
+    operator (apply_full_L) are restated from different reference functions; the R-R block of
+    their inverses must agree (the static limit of the dynamical response)."""
+    d = rocksalt_l2
+    # with the symmetry group: without it, 6 configurations leave the dynamical operator singular
+    O = LO.OracleLanczos(d["X"], d["Y"], d["w"], d["rho"], d["T"], d["syms"], d["blocks"], d["blocks_ids"])
+    n = O.n_modes
+    ln, ls = n + n * (n + 1), n + n * (n + 1) // 2
+    Ld = np.zeros((ln, ln))
+    for i in range(ln):
+        e = np.zeros(ln)
+        e[i] = 1.0
+        Ld[:, i] = O.apply_full_L(e)
+    Ls = np.zeros((ls, ls))
+    for i in range(ls):
+        e = np.zeros(ls)
+        e[i] = 1.0
+        Ls[:, i] = O.apply_static_L(e)
+    Gd = np.linalg.inv(Ld)[:n, :n]
+    Gs = np.linalg.inv(Ls)[:n, :n]
+    assert np.abs(Gd - Gs).max() <= 1e-8 * np.abs(Gs).max()
