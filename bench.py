@@ -79,11 +79,21 @@ def _ref_worker(i):
     from oracle import lanczos_oracle as LO
     t0 = time.perf_counter()
     LO.perturb_average_sym(d["X"][i:i + 1], d["Y"][i:i + 1], d["w"], d["rho"][i:i + 1], d["R1"], d["Y1"], d["T"], 1,
-                           d["syms"], d["n_deg"], d["degs"], d["bid"], backend="reference")
+                           d["syms"], d["n_deg"], d["degs"], d["bid"], backend=d["backend"], n_threads=1)
     return time.perf_counter() - t0
 
 
-def cpu_reference_timing(system, X, Y, rho, seconds_target=20.0, max_procs=None):
+def cpu_backend():
+    """The reference's own kernel (oracle/_ref) when it was compiled here, else the C port."""
+    from oracle import lanczos_oracle as LO
+    try:
+        LO.reference_module()
+        return "reference"
+    except Exception:
+        return "port"
+
+
+def cpu_reference_timing(system, X, Y, rho, seconds_target=20.0, max_procs=None, backend=None):
     """Time the reference kernel on P host processes, one configuration each (the reference's MPI
     partition: contiguous config slices, LanczosFunctions.c:2123-2136).  Returns (apply/s for the
     full ensemble, cores, sample description).  The per-(configuration, symmetry) cost is O(n^2)
@@ -95,14 +105,15 @@ def cpu_reference_timing(system, X, Y, rho, seconds_target=20.0, max_procs=None)
     R1 = rng.standard_normal(n) * 1e-3
     Y1 = rng.standard_normal((n, n)) * 1e-3
     Y1 = Y1 + Y1.T
-    procs = max_procs or min(os.cpu_count() or 1, 64)
+    procs = min(max_procs or min(os.cpu_count() or 1, 64), X.shape[0])
+    backend = backend or cpu_backend()
     # bounded sample: a slice of the symmetry group keeps one task near seconds_target on big cells
     per_pair = 6.4e-3 * (n / 381.0) ** 2
     n_sym_sample = int(min(system.n_syms, max(48, seconds_target / per_pair)))
     _REF_DATA.update(X=X, Y=Y, w=system.w, rho=rho, R1=R1, Y1=Y1, T=system.T,
                      syms=[s[:n_sym_sample] for s in system.symmetries],
                      n_deg=np.array([len(d) for d in system.deg_space], dtype=np.intc), degs=system.deg_space,
-                     bid=system.blocks_ids)
+                     bid=system.blocks_ids, backend=backend)
     ctx = mp.get_context("fork")
     t0 = time.perf_counter()
     with ctx.Pool(procs) as pool:
@@ -111,10 +122,12 @@ def cpu_reference_timing(system, X, Y, rho, seconds_target=20.0, max_procs=None)
     pairs_sample = procs * n_sym_sample
     pairs_full = X.shape[0] * system.n_syms
     t_apply = max(per_task) * pairs_full / pairs_sample
-    sample = (f"reference GetPerturbAverageSym (oracle/_ref, gcc -O2) on {procs} processes x 1 configuration x "
+    what = ("reference GetPerturbAverageSym (oracle/_ref, gcc -O2)" if backend == "reference"
+            else "C port of GetPerturbAverageSym (oracle/tdscha_oracle.c; the reference kernel is not built here)")
+    sample = (f"{what} on {procs} processes x 1 configuration x "
               f"{n_sym_sample} symmetries ({pairs_sample} pairs, {wall:.1f} s wall); one apply = "
               f"{pairs_full} pairs, extrapolated linearly in pairs")
-    return 1.0 / t_apply, procs, sample
+    return 1.0 / t_apply, procs, sample, ("reference" if backend == "reference" else "port")
 
 
 # ------------------------------------------------------------------------------------------------
@@ -173,7 +186,7 @@ def run_reference_arm(a, rank):
     sample = ""
     t0 = time.perf_counter()
     for _ in range(a.steps):
-        v, cores, sample = cpu_reference_timing(s, X, Y, rho, seconds_target=8.0)
+        v, cores, sample, kind = cpu_reference_timing(s, X, Y, rho, seconds_target=8.0)
         vals.append(v)
     wall = time.perf_counter() - t0
     v = float(np.mean(vals))
@@ -182,7 +195,7 @@ def run_reference_arm(a, rank):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded rock-salt ensemble)",
             "config": {"workload": workload_name(a), "N": a.N, "n_modes": s.n_modes, "N_sym": s.n_syms},
             "impl": "reference",
-            "cpu_baseline": {"value": v, "unit": "apply_L/s", "cores": cores, "kind": "reference", "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "apply_L/s", "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": v, "unit": "apply_L/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall}
     return line
@@ -383,8 +396,8 @@ def main():
                     "sample": "skipped: --sym-on-gpu opens a CUDA context before the forking process pool"}
     elif rank == 0 and world == 1 and not a.no_cpu_baseline:
         try:
-            v, cores, sample = cpu_reference_timing(s, X, Y, rho)
-            cpu_base = {"value": v, "unit": "apply_L/s", "cores": cores, "kind": "reference", "sample": sample}
+            v, cores, sample, kind = cpu_reference_timing(s, X, Y, rho)
+            cpu_base = {"value": v, "unit": "apply_L/s", "cores": cores, "kind": kind, "sample": sample}
         except Exception as ex:   # reference kernel not built on this machine
             cpu_base = {"value": None, "unit": "apply_L/s", "cores": 0, "kind": "reference", "sample": f"unavailable: {ex}"}
 
