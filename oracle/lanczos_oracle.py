@@ -155,6 +155,78 @@ def perturb_average_sym(X, Y, w, rho, R1, Y1, T, apply_d4, symmetries, n_deg, de
     return f_out, d_out
 
 
+_POOL_DATA = {}
+
+
+def _pool_init(data):
+    _POOL_DATA.clear()
+    _POOL_DATA.update(data)
+
+
+def _pool_slice(args):
+    """Averages of one slice of (configuration, symmetry) pairs, scaled back to a partial sum (x the
+    slice's N_eff x its number of symmetries): what each MPI rank contributes to the reference's
+    MPI_Allreduce (LanczosFunctions.c:2123-2136, 2236-2248)."""
+    i0, i1, sym0, sym1, R1, Y1, apply_d4 = args
+    d = _POOL_DATA
+    syms = d["syms"] if sym0 is None else [s[sym0:sym1] for s in d["syms"]]
+    f, dv = perturb_average_sym(d["X"][i0:i1], d["Y"][i0:i1], d["w"], d["rho"][i0:i1], R1, Y1, d["T"], apply_d4, syms,
+                                d["n_deg"], d["degs"], d["bid"], backend=d["backend"], n_threads=1)
+    scale = float(np.sum(d["rho"][i0:i1])) * int(syms[0].shape[0])
+    return f * scale, dv * scale
+
+
+class SlicedAverages:
+    """The averages of the whole ensemble from P worker processes (``spawn``: safe after a CUDA
+    context exists; callers' scripts need an ``if __name__ == "__main__"`` guard), each running the
+    C kernel on a contiguous slice of the configurations -- the reference's MPI partition and
+    Allreduce (LanczosFunctions.c:2123-2136, 2236-2248) on the host cores.  With fewer
+    configurations than processes the symmetry group is sliced too (the averages are plain sums
+    over (configuration, symmetry) pairs divided by N_eff * N_sym).  Use as a context manager."""
+
+    def __init__(self, X, Y, w, rho, T, symmetries, n_deg, deg_space, blocks_ids, backend="reference", procs=None):
+        import multiprocessing as mp
+        self.N = X.shape[0]
+        self.N_sym = int(symmetries[0].shape[0])
+        self.rho = np.asarray(rho, dtype=np.float64)
+        self.procs = max(1, procs or (os.cpu_count() or 1))
+        data = dict(X=np.ascontiguousarray(X, dtype=np.float64), Y=np.ascontiguousarray(Y, dtype=np.float64),
+                    w=np.ascontiguousarray(w, dtype=np.float64), rho=self.rho, T=float(T),
+                    syms=[np.ascontiguousarray(s, dtype=np.float64) for s in symmetries],
+                    n_deg=np.ascontiguousarray(n_deg, dtype=np.intc),
+                    degs=[np.ascontiguousarray(d_, dtype=np.intc) for d_ in deg_space],
+                    bid=np.ascontiguousarray(blocks_ids, dtype=np.intc), backend=backend)
+        if self.N >= self.procs:
+            edges = np.linspace(0, self.N, self.procs + 1).round().astype(int)
+            self.tasks = [(int(a), int(b), None, None) for a, b in zip(edges[:-1], edges[1:]) if b > a]
+        else:
+            per = max(1, -(-self.procs // self.N))
+            sedges = np.linspace(0, self.N_sym, per + 1).round().astype(int)
+            self.tasks = [(i, i + 1, int(a), int(b)) for i in range(self.N)
+                          for a, b in zip(sedges[:-1], sedges[1:]) if b > a]
+        self._pool = mp.get_context("spawn").Pool(self.procs, initializer=_pool_init, initargs=(data,))
+
+    def __call__(self, R1, Y1, apply_d4):
+        R1 = np.ascontiguousarray(R1, dtype=np.float64)
+        Y1 = np.ascontiguousarray(Y1, dtype=np.float64)
+        parts = self._pool.map(_pool_slice, [t + (R1, Y1, int(apply_d4)) for t in self.tasks], chunksize=1)
+        norm = float(np.sum(self.rho)) * self.N_sym
+        f = sum(p[0] for p in parts) / norm
+        dv = sum(p[1] for p in parts) / norm
+        return f, dv
+
+    def close(self):
+        self._pool.close()
+        self._pool.join()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+        return False
+
+
 # ----------------------------------------------------------------------------------------------
 # helpers on the packed (R | Y-triangle | A-triangle) vector
 # ----------------------------------------------------------------------------------------------
