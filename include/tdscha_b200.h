@@ -6,6 +6,9 @@
  * failure on the calling thread.  "_device" entry points take device pointers and an optional
  * cudaStream_t passed as void* (NULL = the legacy default stream) and are asynchronous with respect
  * to the host unless stated otherwise; the other entry points take host buffers and synchronise.
+ * Temporaries of the entry points that need them live in library-owned device buffers, one per
+ * (host thread, device, stream), grown on demand: calls issued from one thread on one stream reuse
+ * them in stream order, and calls on different streams or threads never share one.
  *
  * Reference interfaces replaced (mesonepigreco/python-sscha, tdscha package):
  *   sscha_HP_odd.GetPerturbAverageSym          CModules/odd_corr_module.c:491-634
@@ -159,7 +162,8 @@ int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const do
  * that loads the library holds until the process exits.
  *   - nc must be at most 32; larger requests fail with TDSCHA_EINVAL and a message.
  *   - Runs on the current device.  The first call on each device looks up the array's device
- *     address (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     address (cudaGetSymbolAddress), and so does the first call after that device's context
+ *     changed (e.g. after cudaDeviceReset); make such a call before any stream capture.
  *   - All calls share the one array: calls that overlap on the GPU (e.g. on different streams)
  *     race and give wrong results.  Each call writes every partial it reads, so no clearing is
  *     needed between calls.
@@ -250,6 +254,20 @@ int tdscha_read_profile(tdscha_ensemble *ens, double *ms, long long *launches, i
  */
 int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, const void *A_lo, long long lda,
                        const void *B_hi, const void *B_lo, long long ldb, float *D, long long ldd, void *stream);
+
+/*
+ * Failure detection of the tensor-core kernels (no counterpart in the reference, whose kernels have
+ * no waits).  Every pipeline wait inside the tcgen05 contraction is bounded; when one runs out the
+ * kernel stops its CTA cleanly (its copies in flight drained, its MMAs retired, its tensor memory
+ * freed) and the call returns TDSCHA_ETIMEOUT, after which the library stays usable.
+ *   tdscha_set_wait_budget               budget of each wait of later launches, seconds in
+ *                                        [1e-6, 60] (default 4); process-wide
+ *   tdscha_debug_stall_next_contraction  the next contraction launch issues no operand copy, so that
+ *                                        its first wait can only end by running out (tests of the
+ *                                        abort path); one-shot, process-wide
+ */
+int tdscha_set_wait_budget(double seconds);
+int tdscha_debug_stall_next_contraction(void);
 
 /*
  * Vector-Jacobian product of the averages (the outputs of tdscha_perturb_average_sym_device)

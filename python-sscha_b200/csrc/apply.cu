@@ -11,6 +11,7 @@
 //   get_green_function_continued_fraction :4951-5047
 #include <cmath>
 #include <cuComplex.h>
+#include <cuda.h>
 #include <mutex>
 
 #include "apply.cuh"
@@ -370,21 +371,43 @@ size_t lanczos_scratch_bytes(int nc) { return (size_t)nc * LZ_BLOCKS * 4 * sizeo
 constexpr int LZ_NOALLOC_MAX_CHAINS = 32;
 static __device__ __align__(256) double g_lz_noalloc_scratch[(size_t)LZ_NOALLOC_MAX_CHAINS * LZ_BLOCKS * 4];
 
-// Device address of the array on each device, looked up once (with that device current).
+// Device address of the array, looked up once per device (with that device current) and again only
+// when the device's context changed since (after a device reset the module is loaded anew and the
+// array may sit elsewhere).  The context handle comes from the driver entry point cuCtxGetCurrent.
+typedef CUresult (*CtxGetCurrentFn)(CUcontext *);
 static std::mutex g_noalloc_mutex;
 static void *g_noalloc_addr[128] = {nullptr};
+static CUcontext g_noalloc_ctx[128] = {nullptr};
+
+static int current_context(CUcontext *ctx) {
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        TD_CHECK(cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+                     q == cudaDriverEntryPointSuccess && p != nullptr,
+                 TDSCHA_ECUDA, "cuCtxGetCurrent entry point unavailable");
+        fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    }
+    TD_CHECK(fn(ctx) == CUDA_SUCCESS, TDSCHA_ECUDA, "cuCtxGetCurrent failed");
+    return 0;
+}
 
 static int noalloc_scratch_address(double **out) {
     int dev = 0;
     TD_CUDA(cudaGetDevice(&dev));
     TD_CHECK(dev >= 0 && dev < 128, TDSCHA_EINVAL, "device index %d out of range", dev);
+    TD_CUDA(cudaSetDevice(dev));            // makes the device's primary context current (CUDA >= 12)
+    CUcontext ctx = nullptr;
+    TD_TRY(current_context(&ctx));
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_addr[dev]) {
+    if (!g_noalloc_addr[dev] || g_noalloc_ctx[dev] != ctx) {
         void *p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_lz_noalloc_scratch);
         TD_CHECK(e == cudaSuccess && p != nullptr, TDSCHA_ECUDA, "cudaGetSymbolAddress of the Lanczos scratch failed: %s",
                  cudaGetErrorString(e));
         g_noalloc_addr[dev] = p;
+        g_noalloc_ctx[dev] = ctx;
     }
     *out = static_cast<double *>(g_noalloc_addr[dev]);
     return 0;

@@ -2,6 +2,8 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <tuple>
 #include <vector>
 
 #include "apply.cuh"
@@ -22,30 +24,27 @@ void set_error(const char *fmt, ...) {
 }
 void clear_error() { g_err[0] = 0; }
 
-// Scratch owned by the library for the calls that need temporaries (grown on demand, per device).
+// Temporaries of the allocating entry points: library-owned buffers, grown on demand, one per
+// (slot, device, stream) and host thread.  Calls from one thread on one stream reuse a buffer in
+// stream order; calls on different streams or from different threads never share one.
 struct Scratch {
     void *p = nullptr;
     size_t bytes = 0;
-    int device = -1;
 };
-static thread_local Scratch g_scratch[3];
+static thread_local std::map<std::tuple<int, int, cudaStream_t>, Scratch> g_scratch;
 
-static int scratch_get(int slot, size_t bytes, void **out) {
+static int scratch_get(int slot, size_t bytes, cudaStream_t st, void **out) {
     int dev = 0;
     TD_CUDA(cudaGetDevice(&dev));
-    Scratch &s = g_scratch[slot];
-    if (s.p && (s.device != dev || s.bytes < bytes)) {
-        int prev = dev;
-        cudaSetDevice(s.device);
-        cudaDeviceSynchronize();
+    Scratch &s = g_scratch[std::make_tuple(slot, dev, st)];
+    if (s.p && s.bytes < bytes) {
+        TD_CUDA(cudaStreamSynchronize(st));   // the old buffer may still be read by this stream's work
         cudaFree(s.p);
-        cudaSetDevice(prev);
         s = Scratch();
     }
     if (!s.p) {
         TD_CUDA(cudaMalloc(&s.p, bytes));
         s.bytes = bytes;
-        s.device = dev;
     }
     *out = s.p;
     return 0;
@@ -109,7 +108,7 @@ int tdscha_perturb_average_sym_device(tdscha_ensemble *e, int nb, const double *
     TD_CUDA(cudaSetDevice(e->device));
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     void *ys = nullptr;
-    TD_TRY(scratch_get(0, (size_t)nb * e->n * e->n * sizeof(double), &ys));
+    TD_TRY(scratch_get(0, (size_t)nb * e->n * e->n * sizeof(double), st, &ys));
     TD_TRY(symmetrize_device(nb, e->n, Y1, static_cast<double *>(ys), st));
     TD_TRY(perturb_average_device(e, nb, R1, static_cast<const double *>(ys), apply_d4, precision, f_out, d2v_out, st));
     return check_err_word(e, st);
@@ -122,7 +121,7 @@ int tdscha_perturb_average_sym(tdscha_ensemble *e, const double *R1, const doubl
     TD_CUDA(cudaSetDevice(e->device));
     const size_t n = e->n;
     void *buf = nullptr;
-    TD_TRY(scratch_get(1, (2 * n + 2 * n * n) * sizeof(double), &buf));
+    TD_TRY(scratch_get(1, (2 * n + 2 * n * n) * sizeof(double), nullptr, &buf));
     double *dR = static_cast<double *>(buf), *dY = dR + n, *df = dY + n * n, *dD = df + n;
     TD_CUDA(cudaMemcpy(dR, R1, n * sizeof(double), cudaMemcpyHostToDevice));
     TD_CUDA(cudaMemcpy(dY, Y1, n * n * sizeof(double), cudaMemcpyHostToDevice));
@@ -153,7 +152,7 @@ int tdscha_apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, co
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t need = apply_scratch_bytes(e, nb);
     void *buf = nullptr;
-    TD_TRY(scratch_get(0, need, &buf));
+    TD_TRY(scratch_get(0, need, st, &buf));
     TD_TRY(apply_full_L_device(e, nb, psi, transpose, opts, precision, out, st, buf, need));
     return check_err_word(e, st);
 }
@@ -161,7 +160,7 @@ int tdscha_apply_full_L_device(tdscha_ensemble *e, int nb, const double *psi, co
 static int upload_flags(int nb, const int *transpose, cudaStream_t st, int **tr_d) {
     TD_CHECK(transpose && nb > 0 && nb <= 4096, TDSCHA_EINVAL, "bad transpose flags");
     void *buf = nullptr;
-    TD_TRY(scratch_get(2, 4096 * sizeof(int), &buf));
+    TD_TRY(scratch_get(2, 4096 * sizeof(int), st, &buf));
     TD_CUDA(cudaMemcpyAsync(buf, transpose, nb * sizeof(int), cudaMemcpyHostToDevice, st));
     *tr_d = static_cast<int *>(buf);
     return 0;
@@ -206,7 +205,7 @@ int tdscha_apply_static_L_device(tdscha_ensemble *e, int nb, const double *psi, 
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     const size_t need = static_work_bytes(e, nb);
     void *buf = nullptr;
-    TD_TRY(scratch_get(0, need, &buf));
+    TD_TRY(scratch_get(0, need, st, &buf));
     TD_TRY(apply_static_L_device(e, nb, psi, ignore_v4, include_L1, precision, out, st, static_cast<double *>(buf), need));
     return check_err_word(e, st);
 }
@@ -222,7 +221,7 @@ int tdscha_lanczos_step_device(int nc, long long len, const double *Lq, const do
     clear_error();
     const size_t need = lanczos_scratch_bytes(nc);
     void *buf = nullptr;
-    TD_TRY(scratch_get(1, need, &buf));
+    TD_TRY(scratch_get(3, need, static_cast<cudaStream_t>(stream), &buf));
     return lanczos_step_device(nc, len, Lq, pL, q, p, q_prev, p_prev, sc_in, mask, q_next, p_next, sc_out,
                                static_cast<cudaStream_t>(stream), static_cast<double *>(buf), need);
 }
@@ -259,6 +258,19 @@ int tdscha_read_profile(tdscha_ensemble *e, double *ms, long long *launches, int
     }
     e->prof.recs.clear();
     for (int s = 0; s < ST_COUNT; ++s) e->prof.launches[s] = 0;
+    return 0;
+}
+
+int tdscha_set_wait_budget(double seconds) {
+    clear_error();
+    TD_CHECK(seconds >= 1e-6 && seconds <= 60.0, TDSCHA_EINVAL, "wait budget must lie in [1e-6, 60] s (got %g)", seconds);
+    tc::set_wait_budget_ns((unsigned long long)(seconds * 1e9));
+    return 0;
+}
+
+int tdscha_debug_stall_next_contraction(void) {
+    clear_error();
+    tc::stall_next_launch();
     return 0;
 }
 

@@ -18,6 +18,7 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
 #include <cstdint>
 #include <cstdlib>
 #include <map>
@@ -33,7 +34,14 @@ namespace tc {
 
 constexpr int BM = 128;
 constexpr int NUM_THREADS = 320;   // producer, MMA, 8 epilogue warps
-constexpr unsigned long long WAIT_BUDGET_NS = 4000000000ull;   // 4 s per wait
+constexpr unsigned long long DEFAULT_WAIT_BUDGET_NS = 4000000000ull;   // 4 s per pipeline wait
+constexpr unsigned long long DRAIN_BUDGET_NS = 4000000000ull;          // 4 s per wait of the abort path
+
+// Budget of every pipeline wait of the next launches (tdscha_set_wait_budget), and a one-shot request
+// that the next launch's producers issue no copy, so that the MMA warps' first wait can only end by
+// running out (tdscha_debug_stall_next_contraction: a test of the abort path).
+static std::atomic<unsigned long long> g_wait_budget_ns{DEFAULT_WAIT_BUDGET_NS};
+static std::atomic<int> g_stall_next{0};
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -61,7 +69,8 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
     return ok != 0;
 }
 // Bounded wait: true when the phase completed, false on timeout or when another role aborted.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort_flag,
+                                          unsigned long long budget_ns) {
     unsigned long long t0 = 0;
     for (uint32_t it = 0;; ++it) {
         if (mbar_try(bar, parity)) return true;
@@ -69,7 +78,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
             if (*abort_flag) return false;
             unsigned long long t = globaltimer();
             if (t0 == 0) t0 = t;
-            else if (t - t0 > WAIT_BUDGET_NS) return false;
+            else if (t - t0 > budget_ns) return false;
         }
     }
 }
@@ -193,7 +202,7 @@ __global__ void __launch_bounds__(NUM_THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
                int M, int N, int K, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err,
-               unsigned *tile_sync, unsigned sync_ns, int accumulate) {
+               unsigned *tile_sync, unsigned sync_ns, int accumulate, unsigned long long wait_ns, int stall) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -203,6 +212,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
     uint64_t *acc_empty = bars + 2 * STAGES + 2;
     volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 4);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
+    uint64_t *done_bar = bars + 2 * STAGES + 6;   // abort path: completion of every MMA issued
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -220,6 +230,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
             mbar_init(smem_u32(&acc_full[x]), 1);
             mbar_init(smem_u32(&acc_empty[x]), C::EPI_WARPS);
         }
+        mbar_init(smem_u32(done_bar), 1);
         *abort_flag = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -234,7 +245,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
     const uint32_t tmem_base = *tmem_slot;
 
     long long issued = 0;   // k-blocks handed to TMA by the producer (for the drain on abort)
-    if (warp == 0 && lane == 0) {
+    if (warp == 0 && lane == 0 && !stall) {
         // ---------------- TMA producer ----------------
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmA_hi)) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(&tmB_hi)) : "memory");
@@ -249,7 +260,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
                 const int s = (int)(g % STAGES);
                 const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
-                if (!mbar_wait(smem_u32(&bars[STAGES + s]), ph ^ 1u, abort_flag)) { *abort_flag = 1; break; }
+                if (!mbar_wait(smem_u32(&bars[STAGES + s]), ph ^ 1u, abort_flag, wait_ns)) { *abort_flag = 1; break; }
                 uint8_t *st = smem + s * C::STAGE_BYTES;
                 const uint32_t full = smem_u32(&bars[s]);
                 mbar_expect_tx(full, C::STAGE_BYTES);
@@ -272,14 +283,14 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
             for (int c = 0; c < chunks_per_tile && ok; ++c, ++ch) {
                 const int X = (int)(ch & 1);
                 const uint32_t use = (uint32_t)(ch >> 1);
-                if (!mbar_wait(smem_u32(&acc_empty[X]), (use & 1u) ^ 1u, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(smem_u32(&acc_empty[X]), (use & 1u) ^ 1u, abort_flag, wait_ns)) { ok = false; break; }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t dtm = tmem_base + (uint32_t)(X * BN);
                 const int kb_end = min(num_kb, (c + 1) * drain);
                 for (int kb = c * drain; kb < kb_end; ++kb, ++g) {
                     const int s = (int)(g % STAGES);
                     const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
-                    if (!mbar_wait(smem_u32(&bars[s]), ph, abort_flag)) { ok = false; break; }
+                    if (!mbar_wait(smem_u32(&bars[s]), ph, abort_flag, wait_ns)) { ok = false; break; }
                     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                     uint8_t *st = smem + s * C::STAGE_BYTES;
                     const uint32_t a_hi = smem_u32(st);
@@ -321,7 +332,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
             for (int c = 0; c < chunks_per_tile; ++c, ++ch) {
                 const int X = (int)(ch & 1);
                 const uint32_t use = (uint32_t)(ch >> 1);
-                if (!mbar_wait(smem_u32(&acc_full[X]), use & 1u, abort_flag)) { ok = false; break; }
+                if (!mbar_wait(smem_u32(&acc_full[X]), use & 1u, abort_flag, wait_ns)) { ok = false; break; }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
                 const uint32_t tbase = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)(X * BN + half * C::EPI_COLS);
 #pragma unroll
@@ -366,11 +377,17 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
     __syncthreads();
     if (*abort_flag) {
         if (threadIdx.x == 0) atomicOr(err, ERR_TIMEOUT);
+        volatile int never = 0;
         if (warp == 0 && lane == 0) {
-            // drain the TMA copies this CTA still has in flight (bounded)
-            volatile int never = 0;
+            // drain the TMA copies this CTA still has in flight (bounded; copies older than the last
+            // STAGES completed before their slots were handed back)
             for (long long g = (issued > STAGES ? issued - STAGES : 0); g < issued; ++g)
-                mbar_wait(smem_u32(&bars[g % STAGES]), (uint32_t)(g / STAGES) & 1u, &never);
+                mbar_wait(smem_u32(&bars[g % STAGES]), (uint32_t)(g / STAGES) & 1u, &never, DRAIN_BUDGET_NS);
+        }
+        if (warp == 1 && lane == 0) {
+            // every MMA this thread issued has retired before the accumulator columns are released
+            umma_commit(smem_u32(done_bar));
+            mbar_wait(smem_u32(done_bar), 0u, &never, DRAIN_BUDGET_NS);
         }
         __syncthreads();
     }
@@ -551,12 +568,16 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     const bool capturing = cap != cudaStreamCaptureStatusNone;
     unsigned *counter = nullptr;
     if (sync_ns > 0 && tiles > grid.x) TD_TRY(tile_sync_counter(dev, st, capturing, &counter));
+    const unsigned long long wait_ns = g_wait_budget_ns.load();
+    const int stall = g_stall_next.exchange(0);
     auto launch = [&](int gm) {
         if (counter) cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
         kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err,
-                                                        counter, sync_ns, accumulate);
+                                                        counter, sync_ns, accumulate, wait_ns, stall);
     };
-    if (const char *env = getenv("TDSCHA_GROUP_M")) {   // tuning knob: fixed tile-group size
+    if (stall) {                                        // abort-path test: one launch, no tuning trials
+        launch(num_m);
+    } else if (const char *env = getenv("TDSCHA_GROUP_M")) {   // tuning knob: fixed tile-group size
         launch(std::max(1, std::min(num_m, atoi(env))));
     } else {
         int gm = 0;
@@ -568,6 +589,9 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     TD_CUDA(cudaGetLastError());
     return 0;
 }
+
+void set_wait_budget_ns(unsigned long long ns) { g_wait_budget_ns.store(ns); }
+void stall_next_launch() { g_stall_next.store(1); }
 
 int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
     TD_CHECK(M > 0 && N > 0 && K > 0, TDSCHA_EINVAL, "tc::gemm: empty problem %d x %d x %d", M, N, K);

@@ -23,5 +23,10 @@ struct GemmOperands {
 // K must be a multiple of 64 (bf16) or 32 (tf32); operands must be readable up to K columns.
 int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err);
 
+// Budget of every bounded wait of later launches (default 4 s), and a one-shot request that the next
+// launch's producers issue no copy (its MMA warps' first wait then runs out): the abort-path test.
+void set_wait_budget_ns(unsigned long long ns);
+void stall_next_launch();
+
 }  // namespace tc
 }  // namespace tdscha

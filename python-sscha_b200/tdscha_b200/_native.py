@@ -82,9 +82,11 @@ def load():
     lib.tdscha_apply_L1_static_device.argtypes = [vp, ctypes.c_int, vp, ctypes.c_double, vp, vp]
     lib.tdscha_apply_static_L_device.argtypes = [vp, ctypes.c_int, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp]
     lib.tdscha_lanczos_run_device.argtypes = [ctypes.c_int, ctypes.POINTER(RunSystem), ctypes.c_int, ctypes.c_int, vp]
+    lib.tdscha_set_wait_budget.argtypes = [ctypes.c_double]
+    lib.tdscha_debug_stall_next_contraction.argtypes = []
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
-    for name in ("tdscha_apply_L1_static_device", "tdscha_apply_static_L_device", "tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    for name in ("tdscha_set_wait_budget", "tdscha_debug_stall_next_contraction", "tdscha_apply_L1_static_device", "tdscha_apply_static_L_device", "tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -302,6 +304,17 @@ def tc_contract(precision, A_hi, A_lo, B_hi, B_lo, D, stream=None):
     ptr = lambda t: None if t is None else t.data_ptr()   # noqa: E731
     check(lib.tdscha_tc_contract(PREC[precision], M, N, K, ptr(A_hi), ptr(A_lo), A_hi.stride(0), ptr(B_hi),
                                  ptr(B_lo), B_hi.stride(0), D.data_ptr(), D.stride(0), _stream_ptr(stream)))
+
+
+def set_wait_budget(seconds):
+    """Budget of every bounded wait of the tensor-core kernels launched afterwards (default 4 s)."""
+    check(load().tdscha_set_wait_budget(float(seconds)))
+
+
+def debug_stall_next_contraction():
+    """The next tensor-core contraction launch issues no operand copy: its waits run out and the call
+    returns TDSCHA_ETIMEOUT (a test of the abort path)."""
+    check(load().tdscha_debug_stall_next_contraction())
 
 
 def get_perturb_average_sym(X, Y, w, rho, R1, Y1, T, apply_D4, N_syms, sym_list, n_deg, deg_space_list, blocks_ids,

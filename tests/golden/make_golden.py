@@ -1,6 +1,6 @@
 """Generate the golden fixtures in tests/golden/ (run here, where the reference is mounted).
 
-    python tests/golden/make_golden.py            # needs /root/reference and `make -C oracle ref`
+    python tests/golden/make_golden.py     # needs the reference sources ($TDSCHA_REFERENCE) and `make -C oracle ref`
 
 mode10.npz
     The reference's own test system (tests/test_lanczos_fast/test_c_code_lanczos/mode10.*: the exact
@@ -25,7 +25,7 @@ sys.path.insert(0, os.path.join(REPO, "python-sscha_b200"))
 
 from oracle import lanczos_oracle as LO  # noqa: E402
 
-REF = "/root/reference/tests/test_lanczos_fast"
+REF = os.path.join(os.environ.get("TDSCHA_REFERENCE", "/root/reference"), "tests", "test_lanczos_fast")
 
 
 def load_mode10():

@@ -21,6 +21,7 @@ def test_reference_arm_prints_the_contract_line():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
+    assert line["reference_kind"] == line["cpu_baseline"]["kind"]     # which CPU code ran, at the top level
 
 
 def test_cpu_timing_with_the_port_backend():

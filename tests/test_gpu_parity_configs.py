@@ -1,0 +1,185 @@
+"""Parity at the benchmark workloads against the reference's own averaging kernel.
+
+* rock-salt 4x4x4 (n = 381 modes, the full O_h x 64 = 3072-operation group, degenerate blocks of up
+  to 72 modes): the GPU averages (FP64 and the mixed modes) and one transposed apply_full_L against
+  GetPerturbAverageSym compiled from the reference's sources (oracle/_ref; CModules/odd_corr_module.c
+  :491-634, LanczosFunctions.c:2082-2754), run inside the test on the host cores over slices of
+  (configuration, symmetry) pairs recombined as the reference's MPI_Allreduce does.  The C port
+  oracle/tdscha_oracle.c (pinned to the reference kernel to ~1e-15 by tests/test_oracle.py) stands in
+  where oracle/_ref is not built.
+* rock-salt 2x2x2, N = 2000, 384 operations: the 100-step FP64 bi-conjugate chain against the chain
+  computed with the reference kernel (tests/golden/c1_reference_chain.npz, made by
+  tests/golden/make_c1_reference_chain.py): a_n, b_n, c_n within 1e-10 relative, the GPU apply of
+  the reference chain's own Krylov vectors within 1e-12, and G(w) of the mixed-precision chain.
+"""
+import os
+import types
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, load_golden
+from oracle import lanczos_oracle as LO
+
+pytestmark = pytest.mark.gpu
+
+C1 = os.path.join(GOLDEN, "c1_reference_chain.npz")
+
+
+def _rel(a, b):
+    return float(np.abs(a - b).max() / np.abs(b).max())
+
+
+def _backend():
+    try:
+        LO.reference_module()
+        return "reference"
+    except Exception:
+        return "port"
+
+
+def _procs():
+    return max(2, min(os.cpu_count() or 2, 48))
+
+
+@pytest.fixture(scope="module")
+def l4():
+    from tdscha_b200 import rocksalt as RS
+    s = RS.build_system(4, T=300.0)
+    X, Y, rho = RS.sample_ensemble(s, 3, seed=5)
+    return s, X, Y, rho
+
+
+# max-norm error relative to the max-norm of the reference output (3 configurations x 3072 symmetries)
+TOL_L4 = {"fp64": 1e-12, "bf16x3": 5e-5, "tf32x3": 5e-5}
+
+
+def test_averages_4x4x4_full_group_vs_reference_kernel(cuda, l4):
+    from tdscha_b200 import _native
+    s, X, Y, rho = l4
+    n = s.n_modes
+    n_deg = np.array([len(d) for d in s.deg_space], dtype=np.intc)
+    rng = np.random.default_rng(44)
+    cases = []
+    for d4 in (1, 0):
+        R1 = rng.standard_normal(n)
+        Y1 = rng.standard_normal((n, n))
+        cases.append((R1, Y1 + Y1.T, d4))
+    backend = _backend()
+    with LO.SlicedAverages(X, Y, s.w, rho, s.T, s.symmetries, n_deg, s.deg_space, s.blocks_ids,
+                           backend=backend, procs=_procs()) as ref_avg:
+        refs = [ref_avg(R1, Y1, d4) for R1, Y1, d4 in cases]
+    ens = _native.DeviceEnsemble(X, Y, s.w, rho, s.T, s.symmetries, s.deg_space, s.blocks_ids)
+    worst = {}
+    for prec, tol in TOL_L4.items():
+        for (R1, Y1, d4), (f_ref, d_ref) in zip(cases, refs):
+            f, dv = ens.perturb_average(R1, Y1, d4, prec)
+            ef, ed = _rel(f, f_ref), _rel(dv, d_ref)
+            worst[prec] = max(worst.get(prec, 0.0), ef, ed)
+            print(f"4x4x4 {prec} d4={d4} ({backend} kernel): f {ef:.2e}  d2v {ed:.2e}")
+            assert ef < tol and ed < tol, (prec, d4, ef, ed)
+    ens.close()
+
+
+def test_apply_full_L_4x4x4_vs_reference_kernel(cuda, l4):
+    """One transposed apply (half off-diagonals, cY/cR mixing, doubled output) at 4x4x4."""
+    from tdscha_b200 import DynamicalLanczos as DL
+    from tdscha_b200 import rocksalt as RS
+    s, X, Y, rho = l4
+    n = s.n_modes
+    n_deg = np.array([len(d) for d in s.deg_space], dtype=np.intc)
+    psi = np.random.default_rng(45).standard_normal(n + n * (n + 1)) * 1e-2
+    O = LO.OracleLanczos(X, Y, s.w, rho, s.T, s.symmetries, s.deg_space, s.blocks_ids)
+    with LO.SlicedAverages(X, Y, s.w, rho, s.T, s.symmetries, n_deg, s.deg_space, s.blocks_ids,
+                           backend=_backend(), procs=_procs()) as ref_avg:
+        O.averages = ref_avg
+        ref = O.apply_full_L(psi.copy(), transpose=True)
+    eo = RS.SyntheticEnsemble(T=s.T, nat=s.nat, m=s.masses, w=s.w, pols=s.pols, N=3, rho=rho, X=X, Y=Y,
+                              symmetries=s.symmetries, deg_space=s.deg_space, blocks_ids=s.blocks_ids,
+                              supercell=(4, 4, 4))
+    L = DL.Lanczos(eo, precision="fp64")
+    L.init()
+    got = L.apply_full_L(psi.copy(), transpose=True)
+    err = _rel(got, ref)
+    print(f"4x4x4 apply_full_L(transpose) fp64: {err:.2e}")
+    assert err < 1e-12, err
+
+
+# ------------------------------------------------------------------------------------------------
+def _c1():
+    if not os.path.exists(C1):
+        pytest.skip("tests/golden/c1_reference_chain.npz not generated")
+    return load_golden("c1_reference_chain.npz")
+
+
+def _c1_lanczos(d, precision):
+    from tdscha_b200 import DynamicalLanczos as DL
+    n = d["X"].shape[1]
+    nat = (n + 3) // 3
+    eo = types.SimpleNamespace(T=d["T"], nat=nat, m=np.ones(3 * nat), w=d["w"], pols=np.eye(3 * nat, n),
+                               N=len(d["rho"]), rho=d["rho"], X=d["X"], Y=d["Y"], symmetries=d["syms"],
+                               deg_space=d["blocks"], blocks_ids=d["blocks_ids"], supercell=(2, 2, 2), nat_uc=2)
+    L = DL.Lanczos(eo, precision=precision)
+    L.init()
+    return L
+
+
+def test_c1_apply_of_reference_krylov_vectors(cuda):
+    """Per-step parity: the GPU FP64 apply of the reference chain's q_k (L) and p_k (L^T)."""
+    d = _c1()
+    L = _c1_lanczos(d, "fp64")
+    worst = 0.0
+    for i, k in enumerate(d["probe_steps"]):
+        for vec, out, tr in ((d["probe_q"][i], d["probe_Lq"][i], False), (d["probe_p"][i], d["probe_pL"][i], True)):
+            got = L.apply_full_L(vec.copy(), transpose=tr)
+            e = _rel(got, out)
+            worst = max(worst, e)
+            assert e < 1e-12, (int(k), tr, e)
+    print(f"2x2x2 N=2000: apply of {len(d['probe_steps'])} reference Krylov pairs, worst rel err {worst:.2e}")
+
+
+def _gf(a, b, c, L, ns):
+    from tdscha_b200 import rocksalt as RS
+    w, eta = RS.gf_grid()
+    L.a_coeffs, L.b_coeffs, L.c_coeffs = list(a[:ns]), list(b[:ns - 1]), list(c[:ns - 1])
+    return L.get_green_function_continued_fraction(w, use_terminator=False, smearing=eta)
+
+
+def test_c1_fp64_chain_matches_reference_chain(cuda):
+    """a_n, b_n, c_n of the 100-step FP64 GPU chain within 1e-10 of the reference-kernel chain."""
+    d = _c1()
+    L = _c1_lanczos(d, "fp64")
+    L.psi = d["psi0"].copy()
+    L.run_FT(int(d["steps"]), verbose=False)
+    k = len(d["a"])
+    assert len(L.a_coeffs) == k
+    ea = np.abs(np.array(L.a_coeffs) - d["a"]) / np.abs(d["a"])
+    eb = np.abs(np.array(L.b_coeffs) - d["b"]) / np.abs(d["b"])
+    ec = np.abs(np.array(L.c_coeffs) - d["c"]) / np.abs(d["c"])
+    worst = np.maximum(ea[:-1], np.maximum(eb, ec)) if len(eb) == k - 1 else np.maximum(ea, np.maximum(eb, ec))
+    over = np.nonzero(worst > 1e-10)[0]
+    print(f"2x2x2 N=2000 FP64 chain, {k} steps: max rel err a {ea.max():.2e} b {eb.max():.2e} c {ec.max():.2e}; "
+          f"first step above 1e-10: {int(over[0]) if len(over) else None}")
+    g64 = _gf(np.array(L.a_coeffs), np.array(L.b_coeffs), np.array(L.c_coeffs), L, k)
+    gref = _gf(d["a"], d["b"], d["c"], L, k)
+    eg = _rel(g64, gref)
+    print(f"  G(w) FP64 vs reference chain: {eg:.2e}")
+    assert ea.max() < 1e-10 and eb.max() < 1e-10 and ec.max() < 1e-10
+    assert eg < 1e-10
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
+def test_c1_mixed_chain_green_function(cuda, precision):
+    """G(w) (500 points 0-400 cm^-1, 5 cm^-1 smearing) of the 100-step mixed-precision chain against
+    the reference-kernel chain, at every step count 25..100 (bound 1e-5)."""
+    d = _c1()
+    L = _c1_lanczos(d, precision)
+    L.psi = d["psi0"].copy()
+    L.run_FT(int(d["steps"]), verbose=False)
+    a, b, c = np.array(L.a_coeffs), np.array(L.b_coeffs), np.array(L.c_coeffs)
+    errs = {}
+    for ns in (25, 50, 75, 100):
+        if ns <= min(len(a), len(d["a"])):
+            errs[ns] = _rel(_gf(a, b, c, L, ns), _gf(d["a"], d["b"], d["c"], L, ns))
+    print(f"2x2x2 N=2000 {precision} chain: G rel err by steps {errs}")
+    assert max(errs.values()) < 1e-5, errs

@@ -20,11 +20,11 @@ def _inputs(torch, nc, length, step, seed):
     return Lq, pL, q, p, qp, pp, sc
 
 
-def _run(torch, fn, args):
+def _run(torch, fn, args, mask=None):
     Lq, pL, q, p, qp, pp, sc = args
     qn, pn = torch.empty_like(q), torch.empty_like(p)
     sc_out = torch.empty((q.shape[0], 4), dtype=torch.float64, device="cuda")
-    fn(Lq, pL, q, p, qp, pp, sc, None, qn, pn, sc_out)
+    fn(Lq, pL, q, p, qp, pp, sc, mask, qn, pn, sc_out)
     torch.cuda.synchronize()
     return qn.cpu().numpy(), pn.cpu().numpy(), sc_out.cpu().numpy()
 
@@ -39,6 +39,43 @@ def test_noalloc_step_matches_allocating_step(cuda):
         for r, g in zip(ref, got):
             assert np.all(np.isfinite(g))
             assert np.abs(g - r).max() <= 1e-12 * np.abs(r).max()
+
+
+def test_noalloc_step_with_mask_matches_allocating_step(cuda):
+    """The weighted scalar products of the symmetric Wigner Lanczos (mask_dot_wigner) on both paths."""
+    torch = cuda
+    from tdscha_b200 import _native
+    n = 45
+    length = n + n * (n + 1)
+    mask = np.ones(length)
+    r, c = np.triu_indices(n)
+    m = n * (n + 1) // 2
+    mask[n:n + m][r < c] = 2
+    mask[n + m:][r < c] = 2
+    mask = torch.as_tensor(mask, device="cuda")
+    args = _inputs(torch, 7, length, 2, seed=11)
+    ref = _run(torch, _native.lanczos_step, args, mask)
+    got = _run(torch, _native.lanczos_step_noalloc, args, mask)
+    for rr, g in zip(ref, got):
+        assert np.abs(g - rr).max() <= 1e-12 * np.abs(rr).max()
+
+
+def test_noalloc_step_allocates_no_device_memory(cuda):
+    """After one warm-up call (which may look up the array's address), further calls leave the
+    device's free memory unchanged: nothing is allocated behind the caller's back."""
+    torch = cuda
+    from tdscha_b200 import _native
+    args = _inputs(torch, 8, 100003, 4, seed=21)
+    Lq, pL, q, p, qp, pp, sc = args
+    qn, pn = torch.empty_like(q), torch.empty_like(p)
+    sc_out = torch.empty((q.shape[0], 4), dtype=torch.float64, device="cuda")
+    _native.lanczos_step_noalloc(Lq, pL, q, p, qp, pp, sc, None, qn, pn, sc_out)
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(3):
+        _native.lanczos_step_noalloc(Lq, pL, q, p, qp, pp, sc, None, qn, pn, sc_out)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
 
 
 def test_noalloc_step_rejects_too_many_chains(cuda):
