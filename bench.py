@@ -55,6 +55,10 @@ def parse():
                     help="16 chains (3 IR, 6 Raman, 7 random) on each of three uneven rock-salt systems "
                          "(2x2x2 N=2000, 3x3x3 N=5000, 4x4x4 N=10000) in one graph-captured multi-system run")
     ap.add_argument("--batch-steps", type=int, default=150)
+    ap.add_argument("--grad", action="store_true",
+                    help="gradient of sum_w Im G(w) (64 points 50-350 cm^-1) of one chain w.r.t. the forces, the "
+                         "weights and (k3, k4), with finite-difference checks (use with --L 3 --N 5000)")
+    ap.add_argument("--grad-steps", type=int, default=50)
     ap.add_argument("--shard-configs", action="store_true",
                     help="strong scaling of one batch of chains: every rank holds a contiguous slice of the "
                          "configurations and each apply all-reduces (f_av, d2v_av) over NCCL")
@@ -293,7 +297,14 @@ def precision_check(a, s, X, Y, rho, ens, precision=None):
             res[ns] = float(np.abs(gf(av, bv, cv, ns) - g_ref).max() / np.abs(g_ref).max())
         return res
 
+    def first_divergence(av):   # first step whose a_n differs from the reference chain's by > 1e-6 relative
+        kk_ = min(len(av), len(ref["a"]))
+        e = np.abs(np.asarray(av[:kk_]) - ref["a"][:kk_]) / np.abs(ref["a"][:kk_])
+        idx = np.nonzero(e > 1e-6)[0]
+        return int(idx[0]) if len(idx) else None
+
     out["g_rel_err_max_by_steps"] = by_steps_of(amx, bmx, cmx)
+    out["a_first_step_rel_err_above_1e-6"] = first_divergence(amx)
     # the same for FP64 chains with tiny seeded perturbations (start vector 1e-12; every apply
     # 3e-9 / 3e-10 relative): how much any error of that size moves G(w) of the unconverged chain
     if ref["source"].startswith("stored") and os.path.exists(FP64_PERTURBED):
@@ -301,6 +312,8 @@ def precision_check(a, s, X, Y, rho, ens, precision=None):
         if np.allclose(dp["checksum"], RS.ensemble_checksum(X, Y, rho), rtol=1e-12, atol=0) and int(dp["steps"]) >= k:
             out["fp64_perturbed_g_rel_err_max_by_steps"] = {
                 str(nm): by_steps_of(dp[f"{nm}_a"], dp[f"{nm}_b"], dp[f"{nm}_c"]) for nm in dp["names"]}
+            out["fp64_perturbed_a_first_step_rel_err_above_1e-6"] = {
+                str(nm): first_divergence(dp[f"{nm}_a"]) for nm in dp["names"]}
     return out
 
 
@@ -406,6 +419,101 @@ def run_batch_systems(a):
     print(json.dumps(line))
 
 
+def run_grad(a):
+    """dG/d(Y, rho, k3, k4) of one seeded chain (checkpoint every 10 steps) through the hand-written
+    adjoint: time per gradient with FP64 contractions and with the benchmark's mixed precision
+    (recurrence, continued fraction and the averages' VJP FP64 in both), the mixed gradient against
+    the FP64 one, and central finite differences of the FP64 value along random directions of Y and
+    rho and along k3, k4 (Richardson-extrapolated)."""
+    import torch
+    from tdscha_b200 import adjoint
+    from tdscha_b200 import DynamicalLanczos as DL
+    from tdscha_b200 import rocksalt as RS
+    s = RS.build_system(a.L, T=a.T, k3=a.k3, k4=a.k4)
+    X, Y3, Y4, rho = RS.sample_force_components(s, a.N, seed=0)
+    k3, k4 = s.k3, s.k4
+    Y = k3 * Y3 + k4 * Y4
+    w = np.linspace(50.0, 350.0, 64) / RS.RY_TO_CM
+    eta = 5.0 / RS.RY_TO_CM
+    steps = a.grad_steps
+
+    def lanczos(Yv, rv):
+        ens = RS.SyntheticEnsemble(T=s.T, nat=s.nat, m=s.masses, w=s.w, pols=s.pols, N=len(rv), rho=rv, X=X, Y=Yv,
+                                   symmetries=s.symmetries, deg_space=s.deg_space, blocks_ids=s.blocks_ids,
+                                   supercell=(a.L,) * 3)
+        L = DL.Lanczos(ens)
+        L.init()
+        L.prepare_random(seed=RS.CHAIN_SEED, sector="R")
+        return L
+
+    base = lanczos(Y, rho)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def gradient(prec):
+        Yt = torch.tensor(Y, device="cuda", requires_grad=True)
+        rt = torch.tensor(rho, device="cuda", requires_grad=True)
+        torch.cuda.synchronize()
+        e0.record()
+        G = adjoint.green_function(base, w, eta, steps, Yt, rt, checkpoint_every=10, precision=prec)
+        gY, gr = torch.autograd.grad(G.imag.sum(), (Yt, rt))
+        e1.record()
+        torch.cuda.synchronize()
+        return G.detach().cpu().numpy(), gY.cpu().numpy(), gr.cpu().numpy(), e0.elapsed_time(e1)
+
+    res = {}
+    for prec in ("fp64", a.precision):
+        gradient(prec)                                   # warm-up: tiles, workspaces
+        G, gY, gr, ms = gradient(prec)
+        res[prec] = {"G": G, "gY": gY, "gr": gr, "ms": ms}
+
+    def value(Yv, rv):
+        L = lanczos(Yv, rv)
+        with torch.no_grad():
+            v = adjoint.green_function(L, w, eta, steps, torch.as_tensor(Yv, device="cuda"),
+                                       torch.as_tensor(rv, device="cuda")).imag.sum()
+        out = float(v)
+        L.device_ensemble.close()
+        return out
+
+    def richardson(f, h):
+        c1 = (f(h) - f(-h)) / (2 * h)
+        c2 = (f(h / 2) - f(-h / 2)) / h
+        return (4 * c2 - c1) / 3
+
+    rng = np.random.default_rng(17)
+    dY = rng.standard_normal(Y.shape)
+    dr = rng.standard_normal(rho.shape) * 0.1
+    g64 = res["fp64"]
+    hY = 1e-5 * np.abs(Y).max()
+    checks = {
+        "Y_direction": (float((g64["gY"] * dY).sum()),
+                        richardson(lambda t: value(Y + t * dY, rho), hY)),
+        "rho_direction": (float((g64["gr"] * dr).sum()), richardson(lambda t: value(Y, rho + t * dr), 1e-5)),
+        "k3": (adjoint.force_gradient_to_k(g64["gY"], Y3, Y4)[0],
+               richardson(lambda t: value((k3 + t) * Y3 + k4 * Y4, rho), 1e-3 * abs(k3))),
+        "k4": (adjoint.force_gradient_to_k(g64["gY"], Y3, Y4)[1],
+               richardson(lambda t: value(k3 * Y3 + (k4 + t) * Y4, rho), 1e-3 * abs(k4))),
+    }
+    fd = {k: {"adjoint": v[0], "finite_difference": v[1], "rel_err": abs(v[0] - v[1]) / abs(v[1])}
+          for k, v in checks.items()}
+    gm = res[a.precision]
+    line = {"metric": "gradient of sum_w Im G(w) w.r.t. forces, weights and (k3, k4): ms per gradient",
+            "value": gm["ms"], "unit": "ms", "higher_is_better": False, "n_gpus": 1,
+            "dtype": f"{a.precision} contractions in the applies; f64 recurrence, continued fraction and VJP",
+            "data": "synthetic (seeded rock-salt ensemble)",
+            "config": {"workload": f"rock-salt {a.L}x{a.L}x{a.L} (n={s.n_modes}), N={a.N}, T={a.T:g} K, "
+                                   f"{s.n_syms} symmetries, {steps} Lanczos steps, checkpoint every 10, "
+                                   "64 frequencies 50-350 cm^-1, smearing 5 cm^-1",
+                       "objective": "sum over the 64 frequencies of Im G(w)"},
+            "ms_per_gradient": {p: round(r["ms"], 1) for p, r in res.items()},
+            "mixed_vs_fp64": {"G_rel_err_max": float(np.abs(gm["G"] - g64["G"]).max() / np.abs(g64["G"]).max()),
+                              "dY_rel_err_max": float(np.abs(gm["gY"] - g64["gY"]).max() / np.abs(g64["gY"]).max()),
+                              "drho_rel_err_max": float(np.abs(gm["gr"] - g64["gr"]).max() / np.abs(g64["gr"]).max())},
+            "finite_differences_fp64": fd,
+            "dk": {"dG_dk3": checks["k3"][0], "dG_dk4": checks["k4"][0], "units": "per internal Ry/Bohr^n coupling"}}
+    print(json.dumps(line))
+
+
 def run_sharded(a, rank, world, local_rank):
     """Configuration-sharded apply_full_L (tdscha_b200.parallel.ShardedEnsemble): the `chains` chains'
     2 x chains vectors are replicated on every rank, each rank averages over its slice of the N
@@ -494,6 +602,13 @@ def main():
 
     if a.shard_configs:
         run_sharded(a, rank, world, local_rank)
+        return
+
+    if a.grad:
+        import torch
+        torch.cuda.set_device(local_rank)
+        if rank == 0:
+            run_grad(a)
         return
 
     if a.batch_systems:

@@ -15,7 +15,7 @@ around the C kernel, following these reference lines (Modules/DynamicalLanczos.p
   apply_anharmonic_FT (standard + Wigner)  :2891-3281
   apply_full_L                             :3467-3570
   mask_dot_wigner                          :5790-5839
-  run_FT (bi-conjugate Lanczos, GS off)    :5843-6374
+  run_FT (bi-conjugate Lanczos, with the optional Gram-Schmidt of :6244-6316)    :5843-6374
   get_green_function_continued_fraction    :4951-5047
   prepare_perturbation / prepare_mode      :1963-2031
   apply_L1_static / apply_anharmonic_static :2502-2565, 3287-3354
@@ -557,8 +557,8 @@ class OracleLanczos:
         mask[n + m:][off] = 2
         return mask
 
-    # ---- bi-conjugate Lanczos, n_rep_orth = 0 (DynamicalLanczos.py:5843-6374) ----
-    def run_FT(self, n_iter, run_simm=False, step_callback=None):
+    # ---- bi-conjugate Lanczos (DynamicalLanczos.py:5843-6374) ----
+    def run_FT(self, n_iter, run_simm=False, step_callback=None, n_rep_orth=0, n_ortho=10):
         psi_norm = np.sum(self.psi ** 2)
         if np.isnan(psi_norm) or psi_norm == 0:
             raise ValueError("initialise a perturbation before running")
@@ -574,6 +574,7 @@ class OracleLanczos:
             first = self.psi / np.sqrt(dot(self.psi, self.psi))
             self.basis_Q, self.basis_P, self.s_norm = [first], [first], [1]
         psi_q, psi_p = self.basis_Q[-1], self.basis_P[-1]
+        next_converged = False
         for _ in range(i_step, i_step + n_iter):
             L_q = self.apply_full_L(psi_q, transpose=False)
             if self.use_wigner and run_simm:
@@ -598,10 +599,37 @@ class OracleLanczos:
             b_coeff = np.sqrt(dot(rk, rk))
             c_coeff = dot(sk_tilde, rk / b_coeff) * s_norm
             self.a_coeffs.append(a_coeff)
-            if np.abs(b_coeff) < EPSILON or np.abs(c_coeff) < EPSILON:
+            if np.abs(b_coeff) < EPSILON or np.abs(c_coeff) < EPSILON or next_converged:
                 break
             psi_q = rk / b_coeff
             psi_p = sk_tilde.copy()
+            if n_rep_orth > 0:
+                # Gram-Schmidt against the last n_ortho basis pairs (DynamicalLanczos.py:6244-6316),
+                # with the reference's own conventions: sequential updates, q normalised by its norm,
+                # p by its squared norm, s_norm re-derived from p . q, and the stop test on the q
+                # coefficients only (its p accumulator adds |0| to itself)
+                new_q, new_p = psi_q.copy(), psi_p.copy()
+                for _rep in range(n_rep_orth):
+                    ortho_q = 0.0
+                    start = max(0, len(self.basis_P) - n_ortho) if n_ortho is not None else 0
+                    for j in range(start, len(self.basis_P)):
+                        coeff1 = dot(self.basis_P[j], new_q)
+                        coeff2 = dot(self.basis_Q[j], new_p)
+                        new_q = new_q - coeff1 * self.basis_P[j]
+                        new_p = new_p - coeff2 * self.basis_Q[j]
+                        ortho_q += np.abs(coeff1)
+                    normq = np.sqrt(dot(new_q, new_q))
+                    if normq < EPSILON:
+                        next_converged = True
+                    new_q = new_q / normq
+                    normp = dot(new_p, new_p)
+                    if np.abs(normp) < EPSILON:
+                        next_converged = True
+                    new_p = new_p / normp
+                    s_norm = c_coeff / dot(new_p, new_q)
+                    if ortho_q < EPSILON:
+                        break
+                psi_q, psi_p = new_q, new_p
             self.basis_Q.append(psi_q.copy())
             self.basis_P.append(psi_p.copy())
             self.b_coeffs.append(b_coeff)

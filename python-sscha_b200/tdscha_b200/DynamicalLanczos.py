@@ -328,7 +328,7 @@ class Lanczos(object):
     def run_FT(self, n_iter, save_dir=None, save_each=5, verbose=True, n_rep_orth=0, n_ortho=10, flush_output=True,
                debug=False, prefix="LANCZOS", run_simm=False, optimized=False):
         run_FT_batched([self], n_iter, save_dir=save_dir, save_each=save_each, verbose=verbose, n_rep_orth=n_rep_orth,
-                       run_simm=run_simm, prefix=[prefix])
+                       run_simm=run_simm, prefix=[prefix], n_ortho=n_ortho)
 
     # ---- Green function (DynamicalLanczos.py:4951-5047) --------------------------------------
     def get_green_function_continued_fraction(self, w_array, use_terminator=True, last_average=1, smearing=0):
@@ -1032,14 +1032,44 @@ Error, algorithm type '{algorithm}' in subroutine run_biconjugate_gradient not i
         self.N_eff = float(np.sum(self.rho))
 
 
+def _gram_schmidt(q, p, window, n_rep_orth, c_coeff, mask):
+    """Gram-Schmidt of the new pair (q, p) against the last basis pairs `window` (device vectors),
+    DynamicalLanczos.py:6244-6316 with its conventions: sequential updates, q normalised by its norm
+    and p by its squared norm, s_norm re-derived from p . q, and the stop test on the q coefficients
+    only.  Returns (q, p, s_norm, next_converged)."""
+    def dot(a, b):
+        return float((a * b).sum()) if mask is None else float((a * b * mask).sum())
+
+    next_converged = False
+    s_norm = None
+    for _ in range(n_rep_orth):
+        ortho_q = 0.0
+        for Qj, Pj in window:
+            c1 = dot(Pj, q)
+            c2 = dot(Qj, p)
+            q = q - c1 * Pj
+            p = p - c2 * Qj
+            ortho_q += abs(c1)
+        normq = np.sqrt(dot(q, q))
+        if normq < __EPSILON__:
+            next_converged = True
+        q = q / normq
+        normp = dot(p, p)
+        if abs(normp) < __EPSILON__:
+            next_converged = True
+        p = p / normp
+        s_norm = c_coeff / dot(p, q)
+        if ortho_q < __EPSILON__:
+            break
+    return q, p, s_norm, next_converged
+
+
 def run_FT_batched(lanczos_list, n_iter, save_dir=None, save_each=5, verbose=False, n_rep_orth=0, run_simm=False,
-                   prefix=None, precision=None):
+                   prefix=None, precision=None, n_ortho=10):
     """Advance several bi-conjugate Lanczos chains that share one ensemble in lockstep: each step
     is ONE batched apply over [L q_c, L^T p_c for every active chain] plus one batched recurrence
     launch; all vectors stay in HBM.  Chains stop independently on breakdown (|b| or |c| < 1e-12)."""
     torch = _torch()
-    if n_rep_orth:
-        raise NotImplementedError("Gram-Schmidt re-orthogonalisation (n_rep_orth > 0) is not available in MODE_B200")
     L0 = lanczos_list[0]
     dev_ens = L0.device_ensemble
     for L in lanczos_list:
@@ -1071,7 +1101,13 @@ def run_FT_batched(lanczos_list, n_iter, save_dir=None, save_each=5, verbose=Fal
         p = torch.as_tensor(np.asarray(L.basis_P[-1]), device=dev)
         qp = torch.as_tensor(np.asarray(L.basis_Q[-2]), device=dev) if len(L.basis_Q) > 1 else torch.zeros_like(q)
         pp = torch.as_tensor(np.asarray(L.basis_P[-2]), device=dev) if len(L.basis_P) > 1 else torch.zeros_like(p)
-        state.append({"q": q, "p": p, "qp": qp, "pp": pp, "done": False, "L": L})
+        window = []
+        if n_rep_orth:      # the last n_ortho basis pairs, for the Gram-Schmidt of the next vectors
+            start = max(0, len(L.basis_P) - n_ortho) if n_ortho is not None else 0
+            window = [(torch.as_tensor(np.asarray(L.basis_Q[j]), device=dev),
+                       torch.as_tensor(np.asarray(L.basis_P[j]), device=dev)) for j in range(start, len(L.basis_P))]
+        state.append({"q": q, "p": p, "qp": qp, "pp": pp, "done": False, "L": L, "window": window,
+                      "next_converged": False})
     opts = L0._opts()
     for it in range(n_iter):
         active = [s for s in state if not s["done"]]
@@ -1109,13 +1145,22 @@ def run_FT_batched(lanczos_list, n_iter, save_dir=None, save_each=5, verbose=Fal
             if np.isnan(a):
                 raise ValueError("Invalid value encountered during the Lanczos.")
             L.a_coeffs.append(a)
-            if abs(b) < __EPSILON__ or abs(c) < __EPSILON__:
+            if abs(b) < __EPSILON__ or abs(c) < __EPSILON__ or s["next_converged"]:
                 s["done"] = True
                 continue
+            q_new, p_new = qn[ci], pn[ci]
+            if n_rep_orth:
+                q_new, p_new, s_gs, s["next_converged"] = _gram_schmidt(q_new.clone(), p_new.clone(), s["window"],
+                                                                        n_rep_orth, c, mask)
+                if s_gs is not None:
+                    snew = s_gs
+                s["window"].append((q_new, p_new))
+                if n_ortho is not None and len(s["window"]) > n_ortho:
+                    s["window"].pop(0)
             s["qp"], s["pp"] = s["q"], s["p"]
-            s["q"], s["p"] = qn[ci], pn[ci]
-            L.basis_Q.append(qn[ci].cpu().numpy())
-            L.basis_P.append(pn[ci].cpu().numpy())
+            s["q"], s["p"] = q_new, p_new
+            L.basis_Q.append(q_new.cpu().numpy())
+            L.basis_P.append(p_new.cpu().numpy())
             L.b_coeffs.append(b)
             L.c_coeffs.append(c)
             L.s_norm.append(snew)

@@ -33,8 +33,11 @@ def _torch():
 class _Ctl:
     """What the autograd function needs besides tensors."""
 
-    def __init__(self, lanc):
+    def __init__(self, lanc, precision="fp64"):
         torch = _torch()
+        if precision not in _native.PREC:
+            raise ValueError(f"precision must be one of {list(_native.PREC)}")
+        self.precision = precision
         if lanc.use_wigner:
             raise NotImplementedError("gradients are available in the standard representation (use_wigner = False)")
         lanc._check_init()
@@ -85,7 +88,7 @@ def _make_function():
         @staticmethod
         def forward(ctx, psi, Y, rho, ctl, transpose):
             out = torch.empty_like(psi)
-            ctl.ens.apply_full_L(psi.contiguous(), out, transpose, ctl.opts, "fp64")
+            ctl.ens.apply_full_L(psi.contiguous(), out, transpose, ctl.opts, ctl.precision)
             ctx.save_for_backward(psi)
             ctx.ctl, ctx.transpose = ctl, list(transpose)
             return out
@@ -98,7 +101,7 @@ def _make_function():
             psi_bar = None
             if ctx.needs_input_grad[0]:
                 psi_bar = torch.empty_like(gout)
-                ctl.ens.apply_full_L(gout, psi_bar, [1 - t for t in tr], ctl.opts, "fp64")
+                ctl.ens.apply_full_L(gout, psi_bar, [1 - t for t in tr], ctl.opts, ctl.precision)
             Y_bar = rho_bar = None
             if (ctx.needs_input_grad[1] or ctx.needs_input_grad[2]) and ctl.anharmonic:
                 kb, n = psi.shape[0], ctl.n
@@ -129,12 +132,14 @@ def apply_full_L(psi, Y, rho, lanc, transpose, ctl=None):
     return _FN.apply(psi, Y, rho, ctl or _Ctl(lanc), list(transpose))
 
 
-def green_function(lanc, omega, smearing, n_steps, Y, rho, psi0=None, checkpoint_every=10):
+def green_function(lanc, omega, smearing, n_steps, Y, rho, psi0=None, checkpoint_every=10, precision="fp64"):
     """G(omega) (complex, CUDA) of the bi-conjugate chain of n_steps steps from psi0 (default
-    lanc.psi), differentiable with respect to Y and rho."""
+    lanc.psi), differentiable with respect to Y and rho.  `precision` is the arithmetic of the
+    ensemble contractions inside the forward and transposed applies; the recurrence, the continued
+    fraction and the vector-Jacobian product of the averages are FP64."""
     torch = _torch()
     from torch.utils.checkpoint import checkpoint
-    ctl = _Ctl(lanc)
+    ctl = _Ctl(lanc, precision)
     dev = "cuda"
     v = torch.as_tensor(np.asarray(lanc.psi if psi0 is None else psi0, dtype=np.float64), device=dev)
     q = v / torch.sqrt((v * v).sum())

@@ -168,3 +168,51 @@ def test_green_function_gradient_wrt_couplings(cuda):
     fd4 = richardson(lambda t: value(k3, k4 + t), 1e-3 * abs(k4))
     assert abs(d3 - fd3) <= 1e-6 * abs(fd3), (d3, fd3)
     assert abs(d4 - fd4) <= 1e-6 * abs(fd4), (d4, fd4)
+
+
+def test_gradient_at_the_differentiation_workload_size(cuda):
+    """The adjoint at the size of the differentiation workload (rock-salt 3x3x3, n = 159, N = 5000,
+    1296 symmetries; a shorter chain of 12 steps, checkpoint every 5): directional derivatives of
+    sum_w Im G(w) along random directions of the forces and weights against central differences."""
+    from tdscha_b200 import adjoint, rocksalt as RS
+    from tdscha_b200 import DynamicalLanczos as DL
+    s = RS.build_system(3)
+    X, Y, rho = RS.sample_ensemble(s, 5000, seed=0)
+
+    def lanczos(Yv, rv):
+        ens = RS.SyntheticEnsemble(T=s.T, nat=s.nat, m=s.masses, w=s.w, pols=s.pols, N=len(rv), rho=rv, X=X, Y=Yv,
+                                   symmetries=s.symmetries, deg_space=s.deg_space, blocks_ids=s.blocks_ids,
+                                   supercell=(3, 3, 3))
+        L = DL.Lanczos(ens)
+        L.init()
+        L.prepare_random(seed=RS.CHAIN_SEED, sector="R")
+        return L
+
+    w = np.linspace(50, 350, 64) / RS.RY_TO_CM
+    eta = 20.0 / RS.RY_TO_CM
+    steps = 12
+    Yt = torch.tensor(Y, device="cuda", requires_grad=True)
+    rt = torch.tensor(rho, device="cuda", requires_grad=True)
+    G = adjoint.green_function(lanczos(Y, rho), w, eta, steps, Yt, rt, checkpoint_every=5)
+    gY, gr = torch.autograd.grad(G.imag.sum(), (Yt, rt))
+    rng = np.random.default_rng(23)
+    dY = rng.standard_normal(Y.shape)
+    dr = rng.standard_normal(rho.shape) * 0.1
+
+    def value(Yv, rv):
+        L = lanczos(Yv, rv)
+        with torch.no_grad():
+            v = float(adjoint.green_function(L, w, eta, steps, torch.as_tensor(Yv, device="cuda"),
+                                             torch.as_tensor(rv, device="cuda")).imag.sum())
+        L.device_ensemble.close()
+        return v
+
+    hY = 1e-5 * np.abs(Y).max()
+    fdY = (value(Y + hY * dY, rho) - value(Y - hY * dY, rho)) / (2 * hY)
+    adY = float((gY.cpu().numpy() * dY).sum())
+    hr = 1e-5
+    fdr = (value(Y, rho + hr * dr) - value(Y, rho - hr * dr)) / (2 * hr)
+    adr = float((gr.cpu().numpy() * dr).sum())
+    print(f"3x3x3 N=5000 gradient: Y {adY:.8e} vs FD {fdY:.8e}; rho {adr:.8e} vs FD {fdr:.8e}")
+    assert abs(adY - fdY) <= 1e-6 * abs(fdY)
+    assert abs(adr - fdr) <= 1e-6 * abs(fdr)

@@ -121,3 +121,35 @@ def test_continued_fraction_matches_oracle(cuda, mode10, opts):
     g = L.get_green_function_continued_fraction(w, **kw)
     go = O.get_green_function_continued_fraction(w, **kw)
     assert np.abs(g - go).max() <= 1e-10 * np.abs(go).max()
+
+
+@pytest.mark.parametrize("n_rep_orth", [1, 2])
+def test_chain_with_gram_schmidt_matches_oracle(cuda, rocksalt_l2, n_rep_orth):
+    """run_FT with Gram-Schmidt re-orthogonalisation (DynamicalLanczos.py:6244-6316) against the
+    oracle's restatement, with a window shorter than the chain (n_ortho = 4).  On this short chain the
+    re-orthogonalisation moves the coefficients by ~1e-11 relative, so the check is on that shift
+    itself: (with GS) / (without GS) - 1 of s_norm, c and a, GPU against oracle."""
+    d = rocksalt_l2
+    steps = 10
+
+    def chains(**kw):
+        L = _lanczos(d)
+        O = _oracle(d)
+        L.prepare_mode(3)
+        O.prepare_mode(3)
+        L.run_FT(steps, verbose=False, **kw)
+        O.run_FT(steps, **kw)
+        return L, O
+
+    L0, O0 = chains()
+    L1, O1 = chains(n_rep_orth=n_rep_orth, n_ortho=4)
+    assert len(L1.a_coeffs) == len(O1.a_coeffs) == len(O0.a_coeffs)
+    for attr in ("s_norm", "c_coeffs", "a_coeffs"):
+        shift_gpu = np.array(getattr(L1, attr)) / np.array(getattr(L0, attr)) - 1
+        shift_ref = np.array(getattr(O1, attr)) / np.array(getattr(O0, attr)) - 1
+        scale = np.abs(shift_ref).max()
+        print(f"GS x{n_rep_orth} {attr}: shift {scale:.2e}, GPU - oracle {np.abs(shift_gpu - shift_ref).max():.2e}")
+        assert scale > 1e-13
+        assert np.abs(shift_gpu - shift_ref).max() <= 0.05 * scale, attr
+        ref = np.array(getattr(O1, attr))
+        assert np.abs(np.array(getattr(L1, attr)) - ref).max() <= 1e-10 * np.abs(ref).max()
