@@ -283,6 +283,17 @@ int tdscha_perturb_average_vjp_device(tdscha_ensemble *ens, int nb, const double
                                       void *stream);
 
 /*
+ * The same vector-Jacobian product with its eight ensemble contractions (four like the averages'
+ * [a|b], [c|d] and four transposed ones over the symmetry rows) in `precision`: TDSCHA_PREC_FP64 is
+ * tdscha_perturb_average_vjp_device; the mixed modes run them on the tcgen05 contraction kernel in
+ * that storage format, the cotangent algebra and the reductions staying FP64.  No counterpart in
+ * the reference.
+ */
+int tdscha_perturb_average_vjp_precision_device(tdscha_ensemble *ens, int nb, const double *R1, const double *Ys,
+                                                int apply_d4, int precision, const double *fbar, const double *Dbar,
+                                                double *Ybar, double *rhobar, void *stream);
+
+/*
  * Inputs of the Lanczos from an ensemble, computed on the GPU (host buffers in and out).
  *
  * tdscha_project_ensemble: X = (u o sqrt(m)) . pols and Y = (f / sqrt(m)) . pols, the

@@ -604,32 +604,11 @@ class OracleLanczos:
             psi_q = rk / b_coeff
             psi_p = sk_tilde.copy()
             if n_rep_orth > 0:
-                # Gram-Schmidt against the last n_ortho basis pairs (DynamicalLanczos.py:6244-6316),
-                # with the reference's own conventions: sequential updates, q normalised by its norm,
-                # p by its squared norm, s_norm re-derived from p . q, and the stop test on the q
-                # coefficients only (its p accumulator adds |0| to itself)
-                new_q, new_p = psi_q.copy(), psi_p.copy()
-                for _rep in range(n_rep_orth):
-                    ortho_q = 0.0
-                    start = max(0, len(self.basis_P) - n_ortho) if n_ortho is not None else 0
-                    for j in range(start, len(self.basis_P)):
-                        coeff1 = dot(self.basis_P[j], new_q)
-                        coeff2 = dot(self.basis_Q[j], new_p)
-                        new_q = new_q - coeff1 * self.basis_P[j]
-                        new_p = new_p - coeff2 * self.basis_Q[j]
-                        ortho_q += np.abs(coeff1)
-                    normq = np.sqrt(dot(new_q, new_q))
-                    if normq < EPSILON:
-                        next_converged = True
-                    new_q = new_q / normq
-                    normp = dot(new_p, new_p)
-                    if np.abs(normp) < EPSILON:
-                        next_converged = True
-                    new_p = new_p / normp
-                    s_norm = c_coeff / dot(new_p, new_q)
-                    if ortho_q < EPSILON:
-                        break
-                psi_q, psi_p = new_q, new_p
+                psi_q, psi_p, s_gs, conv = gram_schmidt(psi_q, psi_p, self.basis_Q, self.basis_P, n_rep_orth, n_ortho,
+                                                        c_coeff, dot)
+                next_converged = next_converged or conv
+                if s_gs is not None:
+                    s_norm = s_gs
             self.basis_Q.append(psi_q.copy())
             self.basis_P.append(psi_p.copy())
             self.b_coeffs.append(b_coeff)
@@ -675,6 +654,38 @@ class OracleLanczos:
         if not self.use_wigner:
             return gf * self.perturbation_modulus
         return (-np.real(gf) + 1j * np.imag(gf)) * self.perturbation_modulus
+
+
+def gram_schmidt(new_q, new_p, basis_Q, basis_P, n_rep_orth, n_ortho, c_coeff, dot):
+    """Gram-Schmidt of the new Lanczos pair against the last n_ortho basis pairs
+    (DynamicalLanczos.py:6244-6316), with the reference's own conventions: sequential updates, q
+    normalised by its norm, p by its squared norm, s_norm re-derived from p . q, and the stop test on
+    the q coefficients only (its p accumulator adds |0| to itself).  Returns (q, p, s_norm or None,
+    next_converged)."""
+    new_q, new_p = np.array(new_q, copy=True), np.array(new_p, copy=True)
+    s_norm = None
+    next_converged = False
+    for _rep in range(n_rep_orth):
+        ortho_q = 0.0
+        start = max(0, len(basis_P) - n_ortho) if n_ortho is not None else 0
+        for j in range(start, len(basis_P)):
+            coeff1 = dot(basis_P[j], new_q)
+            coeff2 = dot(basis_Q[j], new_p)
+            new_q = new_q - coeff1 * basis_P[j]
+            new_p = new_p - coeff2 * basis_Q[j]
+            ortho_q += np.abs(coeff1)
+        normq = np.sqrt(dot(new_q, new_q))
+        if normq < EPSILON:
+            next_converged = True
+        new_q = new_q / normq
+        normp = dot(new_p, new_p)
+        if np.abs(normp) < EPSILON:
+            next_converged = True
+        new_p = new_p / normp
+        s_norm = c_coeff / dot(new_p, new_q)
+        if ortho_q < EPSILON:
+            break
+    return new_q, new_p, s_norm, next_converged
 
 
 # ----------------------------------------------------------------------------------------------

@@ -306,6 +306,17 @@ extern "C" int tdscha_symmetries_on_modes(const double *pols, int nat, int n, in
     return tdscha::symmetries_on_modes(pols, nat, n, N_sym, perm, rot, n_blocks, n_deg, deg_space, sym_out);
 }
 
+extern "C" int tdscha_perturb_average_vjp_precision_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys,
+                                                           int apply_d4, int precision, const double *fbar,
+                                                           const double *Dbar, double *Ybar, double *rhobar, void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    TD_TRY(tdscha::perturb_average_vjp_device(e, nb, R1, Ys, apply_d4, fbar, Dbar, Ybar, rhobar, st, precision));
+    return precision == TDSCHA_PREC_FP64 ? 0 : tdscha::check_err_word(e, st);
+}
+
 extern "C" int tdscha_perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
                                                  const double *fbar, const double *Dbar, double *Ybar, double *rhobar,
                                                  void *stream) {

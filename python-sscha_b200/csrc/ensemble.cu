@@ -411,7 +411,12 @@ int ensemble_destroy(tdscha_ensemble *e) {
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);
+    for (int f = 0; f < 3; ++f) {
+        if (e->YXm_hi[f]) cudaFree(e->YXm_hi[f]);
+        if (e->YXm_lo[f]) cudaFree(e->YXm_lo[f]);
+    }
     free_pair_classes(e->pairs);
+    sym_umma_destroy(e->umma);
     if (e->cublas) cublasDestroy(e->cublas);
     delete e;
     cudaSetDevice(prev);
@@ -581,6 +586,16 @@ static int build_chunk_operands(tdscha_ensemble *e, long long c0, long long Nc, 
     return 0;
 }
 
+// TDSCHA_SYM_UMMA=0 keeps the bf16 formats' symmetry transform / fold on the mma.sync kernels
+static bool sym_umma_enabled() {
+    static int v = -1;
+    if (v < 0) {
+        const char *env = getenv("TDSCHA_SYM_UMMA");
+        v = (env && atoi(env) == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
 int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4, int precision,
                            double *f_out, double *d_out, cudaStream_t st) {
     TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
@@ -670,6 +685,17 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     double *partF = reinterpret_cast<double *>(W + L.partF);
 
     SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->symP, e->symPT, e->d_offP};
+    if (fmt == FMT_BF16 && sym_umma_enabled()) {
+        // the bf16 formats run the symmetry transform and fold on tcgen05 (tables built on first use)
+        if (!e->umma) {
+            TD_CHECK(cap == cudaStreamCaptureStatusNone, TDSCHA_EINVAL,
+                     "graph capture of the averages needs an earlier eager call in this precision");
+            TD_TRY(sym_umma_create(t, e->N_sym, e->blk_dim, e->blk_sym_off, &e->umma));
+        }
+        t.umma = e->umma;
+        t.blocks_ids = e->d_blocks_ids;
+        t.err = e->d_err;
+    }
 
     for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
         const int nj = std::min(Jc, e->N_sym - j0);
@@ -808,13 +834,14 @@ __global__ void vjp_colsum_kernel(long long M, int N, const double *__restrict__
 
 // gbar_i += d/dg_i sum_p Vbar[i][p] V[N+i][p] with V[N+i][(mu nu)] = x_mu g_nu + x_nu g_mu off the
 // diagonal and x_mu g_mu on it; one CTA per i, one warp per row mu of the packed triangle
-__global__ void vjp_matvec_kernel(int N, int n, long long Kp, long long np, const double *__restrict__ Vbar,
-                                  const double *__restrict__ X, double *__restrict__ gbar) {
+template <typename T>
+__global__ void vjp_matvec_kernel(int N, int n, long long Kp, long long np, const T *__restrict__ Vbar,
+                                  const double *__restrict__ X, T *__restrict__ gbar) {
     extern __shared__ double gs[];
     const int i = blockIdx.x;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const double *x = X + (long long)i * n;
-    const double *vb = Vbar + (long long)i * Kp;
+    const T *vb = Vbar + (long long)i * Kp;
     for (int m = threadIdx.x; m < n; m += blockDim.x) gs[m] = 0.0;
     __syncthreads();
     for (int mu = warp; mu < n; mu += nw) {
@@ -822,7 +849,7 @@ __global__ void vjp_matvec_kernel(int N, int n, long long Kp, long long np, cons
         const double xm = x[mu];
         double own = 0.0;
         for (int nu = mu + lane; nu < n; nu += 32) {
-            const double v = vb[row + nu];
+            const double v = (double)vb[row + nu];
             if (nu == mu) {
                 own += v * xm;   // V[N+i, (mu mu)] = x_mu g_mu
             } else {
@@ -834,17 +861,18 @@ __global__ void vjp_matvec_kernel(int N, int n, long long Kp, long long np, cons
         if (lane == 0) atomicAdd(&gs[mu], own);
     }
     __syncthreads();
-    for (int m = threadIdx.x; m < n; m += blockDim.x) gbar[(long long)i * np + m] += gs[m];
+    for (int m = threadIdx.x; m < n; m += blockDim.x) gbar[(long long)i * np + m] = (T)((double)gbar[(long long)i * np + m] + gs[m]);
 }
 
+template <typename T>
 __global__ void vjp_final_kernel(int N, int n, long long np, double norm, const double *__restrict__ rho,
-                                 const double *__restrict__ psi, const double *__restrict__ gbar, const double *__restrict__ ypart,
+                                 const double *__restrict__ psi, const T *__restrict__ gbar, const T *__restrict__ ypart,
                                  double *__restrict__ Ybar) {
     const long long total = (long long)N * n;
     for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
          idx += (long long)gridDim.x * blockDim.x) {
         const long long i = idx / n, m = idx % n;
-        Ybar[idx] = norm * rho[i] * (psi[m] * gbar[i * np + m] + ypart[i * np + m]);
+        Ybar[idx] = norm * rho[i] * (psi[m] * (double)gbar[i * np + m] + (double)ypart[i * np + m]);
     }
 }
 
@@ -875,9 +903,210 @@ static int gemm_atb(tdscha_ensemble *e, const double *A, long long lda, const do
     return 0;
 }
 
+// ---- the VJP with the contractions on the tensor cores (mixed storage formats) ----------------------
+// K1..K4 of the FP64 path, written transposed (N x Mp, rows r contiguous, zero for r >= M) in the
+// storage format, through 32 x 32 shared-memory tiles; BR (M x N, FP64) row-major as in the FP64 path.
+__global__ void vjp_coef_mixed_kernel(long long M, int N, long long ld, long long Mp, const float *__restrict__ D1,
+                                      const float *__restrict__ Dcd, const float *__restrict__ DA, const float *__restrict__ DC,
+                                      int d4, Format fmt, void *K1h, void *K1l, void *K2h, void *K2l, void *K3h, void *K3l,
+                                      void *K4h, void *K4l, double *__restrict__ BR) {
+    __shared__ float tile[4][32][33];
+    const long long r0 = (long long)blockIdx.y * 32;
+    const int i0 = blockIdx.x * 32;
+    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+        const long long r = r0 + rr;
+        const int i = i0 + threadIdx.x;
+        float k1 = 0.f, k2 = 0.f, k3 = 0.f, k4 = 0.f;
+        if (r < M && i < N) {
+            const double a = D1[r * ld + i], b = D1[r * ld + N + i], c = Dcd[r * ld + i], d = Dcd[r * ld + N + i];
+            const double Ap = DA[r * ld + i], Bp = DA[r * ld + N + i], Cp = DC[r * ld + i], Dp = DC[r * ld + N + i];
+            const double kk2 = -c / 3.0 + (d4 ? a / 8.0 : 0.0);
+            k1 = (float)((d4 ? Ap / 8.0 : 0.0) - Dp / 3.0);
+            k2 = (float)kk2;
+            k3 = (float)(-Ap / 6.0);
+            k4 = (float)(-a / 6.0);
+            BR[r * N + i] = 0.5 * (-d / 3.0 + (d4 ? b / 4.0 : 0.0)) * Ap + kk2 * Bp - a / 6.0 * Cp - b / 3.0 * Dp;
+        }
+        tile[0][rr][threadIdx.x] = k1;
+        tile[1][rr][threadIdx.x] = k2;
+        tile[2][rr][threadIdx.x] = k3;
+        tile[3][rr][threadIdx.x] = k4;
+    }
+    __syncthreads();
+    for (int ii = threadIdx.y; ii < 32; ii += blockDim.y) {
+        const int i = i0 + ii;
+        const long long r = r0 + threadIdx.x;
+        if (i < N && r < Mp) {
+            const long long o = (long long)i * Mp + r;
+            store_split(fmt, K1h, K1l, o, tile[0][threadIdx.x][ii]);
+            store_split(fmt, K2h, K2l, o, tile[1][threadIdx.x][ii]);
+            store_split(fmt, K3h, K3l, o, tile[2][threadIdx.x][ii]);
+            store_split(fmt, K4h, K4l, o, tile[3][threadIdx.x][ii]);
+        }
+    }
+}
+
+// dst (C x Rp) = src^T for src (R x C, leading dimension lds), zero for rows r in [R, Rp); elements of
+// 2 (bf16) or 4 (tf32) bytes moved as raw bits
+template <typename E>
+__global__ void transpose_pad_kernel(const E *__restrict__ src, long long R, long long C, long long lds, long long Rp,
+                                     E *__restrict__ dst) {
+    __shared__ E tile[32][33];
+    const long long c0 = (long long)blockIdx.x * 32, r0 = (long long)blockIdx.y * 32;
+    for (int rr = threadIdx.y; rr < 32; rr += blockDim.y) {
+        const long long r = r0 + rr, c = c0 + threadIdx.x;
+        tile[rr][threadIdx.x] = (r < R && c < C) ? src[r * lds + c] : E(0);
+    }
+    __syncthreads();
+    for (int cc = threadIdx.y; cc < 32; cc += blockDim.y) {
+        const long long c = c0 + cc, r = r0 + threadIdx.x;
+        if (c < C && r < Rp) dst[c * Rp + r] = tile[threadIdx.x][cc];
+    }
+}
+
+static int transpose_pad(Format fmt, const void *src, long long R, long long C, long long lds, long long Rp, void *dst,
+                         cudaStream_t st) {
+    if (!src) return 0;
+    dim3 grid((unsigned)ceil_div(C, 32), (unsigned)ceil_div(Rp, 32)), block(32, 8);
+    TD_CHECK(grid.y <= 65535, TDSCHA_EINVAL, "transpose of %lld rows exceeds the grid", Rp);
+    if (fmt == FMT_BF16)
+        transpose_pad_kernel<uint16_t><<<grid, block, 0, st>>>(static_cast<const uint16_t *>(src), R, C, lds, Rp,
+                                                                static_cast<uint16_t *>(dst));
+    else
+        transpose_pad_kernel<float><<<grid, block, 0, st>>>(static_cast<const float *>(src), R, C, lds, Rp,
+                                                             static_cast<float *>(dst));
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+// [Y ; X~] (2N x np) in a storage format, built once per format
+static int ensure_YX_fmt(tdscha_ensemble *e, Format fmt, bool lo, cudaStream_t st) {
+    const int f = (int)fmt;
+    if (e->YXm_hi[f] && (e->YXm_lo[f] || !lo)) return 0;
+    const size_t es = format_bytes(fmt), cnt = (size_t)e->N2 * e->np;
+    if (!e->YXm_hi[f]) TD_CUDA(cudaMalloc(&e->YXm_hi[f], cnt * es));
+    if (lo && !e->YXm_lo[f]) TD_CUDA(cudaMalloc(&e->YXm_lo[f], cnt * es));
+    // [Y ; X~] is [X ; G] with (X, G) -> (Y, X~)
+    build_XG_kernel<<<grid_for((long long)cnt), 256, 0, st>>>(e->Y, e->Xt, e->N, e->n, e->np, fmt, e->YXm_hi[f],
+                                                             lo ? e->YXm_lo[f] : nullptr);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+static int perturb_average_vjp_mixed(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                                     int precision, const double *fbar, const double *Dbar, double *Ybar, double *rhobar,
+                                     cudaStream_t st) {
+    const Format fmt = format_of(precision);
+    const int nprod = products_of(precision);
+    const bool lo = nprod == 3;
+    const size_t es = format_bytes(fmt), nh = lo ? 2 : 1;
+    TD_TRY(ensure_operands(e, fmt, lo, st));
+    TD_TRY(ensure_YX_fmt(e, fmt, lo, st));
+    OperandSet &o = e->ops[fmt];
+    const int N = e->N, n = e->n;
+    const long long Kp = e->Kp, np = e->np, ld1 = round_up(e->N2, 4);
+    // memory plan: fixed buffers, then per symmetry row (M = nb * Jc rows, Mp = M rounded to 64)
+    const size_t fixed = 4 * ((size_t)N * Kp + 2 * (size_t)N * np) + 8 * ((size_t)N + (size_t)nb * n + (size_t)nb * n * n) +
+                         16 * 256;
+    const size_t per_row = es * nh * (4 * (size_t)Kp + 4 * (size_t)np + 4 * (size_t)N) + 4 * 4 * (size_t)ld1 + 8 * (size_t)N;
+    size_t free_b = 0, tot_b = 0;
+    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    const size_t budget = std::max<size_t>((size_t)1 << 30, (size_t)((free_b + e->vjp_ws.bytes) * 0.5));
+    TD_CHECK(budget > fixed + per_row * (nb + 64), TDSCHA_ENOMEM, "not enough device memory for the averages' VJP");
+    int Jc = (int)std::min<long long>(e->N_sym, (long long)((budget - fixed) / per_row - 64) / nb);
+    Jc = std::max(1, Jc);
+    const long long Mmax = (long long)nb * Jc, Mpmax = round_up(Mmax, 64);
+    const size_t need = fixed + per_row * (size_t)Mpmax + 64 * 256;
+    if (e->vjp_ws.bytes < need) {
+        if (e->vjp_ws.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->vjp_ws.base); e->vjp_ws = Workspace(); }
+        TD_CUDA(cudaMalloc(&e->vjp_ws.base, need));
+        e->vjp_ws.bytes = need;
+    }
+    uint8_t *W = static_cast<uint8_t *>(e->vjp_ws.base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { void *p = W + off; off += (bytes + 255) / 256 * 256; return p; };
+    float *Vbar = static_cast<float *>(take(4 * (size_t)N * Kp));
+    float *gbar = static_cast<float *>(take(4 * (size_t)N * np)), *ypart = static_cast<float *>(take(4 * (size_t)N * np));
+    double *colsum = static_cast<double *>(take(8 * (size_t)N));
+    double *Rq = static_cast<double *>(take(8 * (size_t)nb * n)), *Dq = static_cast<double *>(take(8 * (size_t)nb * n * n));
+    auto pair_of = [&](size_t count) {
+        void *h = take(count * es);
+        void *l = lo ? take(count * es) : nullptr;
+        return std::make_pair(h, l);
+    };
+    auto B1 = pair_of(Mmax * Kp), Q = pair_of(Mmax * Kp), r1 = pair_of(Mmax * np), phi = pair_of(Mmax * np);
+    auto B1T = pair_of(Kp * Mpmax), QT = pair_of(Kp * Mpmax), r1T = pair_of(np * Mpmax), phiT = pair_of(np * Mpmax);
+    auto K1 = pair_of((size_t)N * Mpmax), K2 = pair_of((size_t)N * Mpmax), K3 = pair_of((size_t)N * Mpmax),
+         K4 = pair_of((size_t)N * Mpmax);
+    float *D1 = static_cast<float *>(take(4 * Mmax * ld1)), *Dcd = static_cast<float *>(take(4 * Mmax * ld1));
+    float *DA = static_cast<float *>(take(4 * Mmax * ld1)), *DC = static_cast<float *>(take(4 * Mmax * ld1));
+    double *BR = static_cast<double *>(take(8 * Mmax * (size_t)N));
+    TD_CHECK(off <= e->vjp_ws.bytes, TDSCHA_EINVAL, "VJP workspace layout exceeds its allocation");
+    TD_CUDA(cudaMemsetAsync(gbar, 0, 4 * (size_t)N * np, st));
+    TD_CUDA(cudaMemsetAsync(ypart, 0, 4 * (size_t)N * np, st));
+    TD_CUDA(cudaMemsetAsync(colsum, 0, 8 * (size_t)N, st));
+    vjp_cotangent_kernel<<<grid_for((long long)nb * n * n), 256, 0, st>>>(nb, n, fbar, Dbar, e->ups, Rq, Dq);
+    TD_CUDA(cudaGetLastError());
+
+    SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->symP, e->symPT, e->d_offP};
+    bool first = true;
+    for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
+        const int nj = std::min(Jc, e->N_sym - j0);
+        const long long M = (long long)nb * nj, Mp = round_up(M, 64);
+        TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, Kp, np, fmt, B1.first, B1.second, r1.first,
+                             r1.second, true, st));
+        TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Dq, Rq, e->ups, e->P, Kp, np, fmt, Q.first, Q.second, phi.first,
+                             phi.second, true, st));
+        // forward contractions: [a | b], [c | d], [A' | B'], [C' | D']   (M x 2N each)
+        TD_TRY(gemm_abt(e, fmt, nprod, B1.first, B1.second, Kp, M, o.V_hi, o.V_lo, Kp, e->N2, Kp, D1, ld1, st));
+        TD_TRY(gemm_abt(e, fmt, nprod, r1.first, r1.second, np, M, o.XG_hi, o.XG_lo, np, e->N2, np, Dcd, ld1, st));
+        TD_TRY(gemm_abt(e, fmt, nprod, Q.first, Q.second, Kp, M, o.V_hi, o.V_lo, Kp, e->N2, Kp, DA, ld1, st));
+        TD_TRY(gemm_abt(e, fmt, nprod, phi.first, phi.second, np, M, e->YXm_hi[fmt], lo ? e->YXm_lo[fmt] : nullptr, np,
+                        e->N2, np, DC, ld1, st));
+        {
+            dim3 grid((unsigned)ceil_div(N, 32), (unsigned)ceil_div(Mp, 32)), block(32, 8);
+            TD_CHECK(grid.y <= 65535, TDSCHA_EINVAL, "VJP coefficient grid too large");
+            vjp_coef_mixed_kernel<<<grid, block, 0, st>>>(M, N, ld1, Mp, D1, Dcd, DA, DC, apply_d4, fmt, K1.first, K1.second,
+                                                          K2.first, K2.second, K3.first, K3.second, K4.first, K4.second, BR);
+            TD_CUDA(cudaGetLastError());
+        }
+        // the contraction index is the row r = (k, j): transpose the row-major left operands
+        for (auto pr : {std::make_pair(B1, B1T), std::make_pair(Q, QT)}) {
+            TD_TRY(transpose_pad(fmt, pr.first.first, M, Kp, Kp, Mp, pr.second.first, st));
+            TD_TRY(transpose_pad(fmt, pr.first.second, M, Kp, Kp, Mp, pr.second.second, st));
+        }
+        for (auto pr : {std::make_pair(r1, r1T), std::make_pair(phi, phiT)}) {
+            TD_TRY(transpose_pad(fmt, pr.first.first, M, np, np, Mp, pr.second.first, st));
+            TD_TRY(transpose_pad(fmt, pr.first.second, M, np, np, Mp, pr.second.second, st));
+        }
+        // transposed contractions over the rows: Vbar (+)= K1^T B1 + K2^T Q, gbar += K3^T r1, ypart += K4^T phi
+        TD_TRY(gemm_abt(e, fmt, nprod, K1.first, K1.second, Mp, N, B1T.first, B1T.second, Mp, Kp, Mp, Vbar, Kp, st, !first));
+        TD_TRY(gemm_abt(e, fmt, nprod, K2.first, K2.second, Mp, N, QT.first, QT.second, Mp, Kp, Mp, Vbar, Kp, st, true));
+        TD_TRY(gemm_abt(e, fmt, nprod, K3.first, K3.second, Mp, N, r1T.first, r1T.second, Mp, np, Mp, gbar, np, st, true));
+        TD_TRY(gemm_abt(e, fmt, nprod, K4.first, K4.second, Mp, N, phiT.first, phiT.second, Mp, np, Mp, ypart, np, st, true));
+        vjp_colsum_kernel<<<ceil_div(N, 256), 256, 0, st>>>(M, N, BR, colsum);
+        TD_CUDA(cudaGetLastError());
+        first = false;
+    }
+    const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
+    vjp_matvec_kernel<float><<<N, 256, (size_t)n * sizeof(double), st>>>(N, n, Kp, np, Vbar, e->X, gbar);
+    vjp_final_kernel<float><<<grid_for((long long)N * n), 256, 0, st>>>(N, n, np, norm, e->rho, e->psi, gbar, ypart, Ybar);
+    vjp_rho_kernel<<<1, 256, 0, st>>>(N, norm, e->N_eff, e->rho, colsum, rhobar);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
-                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st) {
+                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
+                               int precision) {
     TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    if (precision != TDSCHA_PREC_FP64) {
+        TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+        TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);
+        TD_CHECK(R1 && Ys && fbar && Dbar && Ybar && rhobar, TDSCHA_EINVAL, "NULL argument");
+        TD_CHECK(precision >= 0 && precision <= TDSCHA_PREC_BF16, TDSCHA_EINVAL, "unknown precision %d", precision);
+        return perturb_average_vjp_mixed(e, nb, R1, Ys, apply_d4, precision, fbar, Dbar, Ybar, rhobar, st);
+    }
     TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
     TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);
     TD_CHECK(R1 && Ys && fbar && Dbar && Ybar && rhobar, TDSCHA_EINVAL, "NULL argument");
@@ -944,8 +1173,8 @@ int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, con
         first = false;
     }
     const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
-    vjp_matvec_kernel<<<N, 256, (size_t)n * sizeof(double), st>>>(N, n, e->Kp, e->np, Vbar, e->X, gbar);
-    vjp_final_kernel<<<grid_for((long long)N * n), 256, 0, st>>>(N, n, e->np, norm, e->rho, e->psi, gbar, ypart, Ybar);
+    vjp_matvec_kernel<double><<<N, 256, (size_t)n * sizeof(double), st>>>(N, n, e->Kp, e->np, Vbar, e->X, gbar);
+    vjp_final_kernel<double><<<grid_for((long long)N * n), 256, 0, st>>>(N, n, e->np, norm, e->rho, e->psi, gbar, ypart, Ybar);
     vjp_rho_kernel<<<1, 256, 0, st>>>(N, norm, e->N_eff, e->rho, colsum, rhobar);
     TD_CUDA(cudaGetLastError());
     return 0;

@@ -102,6 +102,9 @@ struct tdscha_ensemble {
     size_t base_bytes = 0;
     tdscha::Profile prof;
     tdscha::PairClasses pairs;
+    tdscha::SymUmma *umma = nullptr;               // tcgen05 symmetry transform / fold tables (bf16 formats)
+    void *YXm_hi[3] = {nullptr, nullptr, nullptr};  // [Y; X~] (2N x np) per storage format (mixed VJP)
+    void *YXm_lo[3] = {nullptr, nullptr, nullptr};
 };
 
 namespace tdscha {
@@ -118,9 +121,12 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
 // Vector-Jacobian product of the averages with respect to the ensemble's forces Y and weights rho:
 // for cotangents (fbar, Dbar) of (f_av, D_av) at the perturbations (R1, Ys), writes
 //   Ybar (N, n) = d<fbar, f_av> + <Dbar, D_av> / dY,   rhobar (N) = same / drho   (summed over nb)
-// FP64 throughout.  Dbar must be symmetric (the Frobenius product is used).
+// FP64 (cuBLAS DGEMM) by default; a mixed `precision` runs its eight contractions on the tcgen05
+// kernel in that storage format (the rest stays FP64).  Dbar must be symmetric (the Frobenius
+// product is used).
 int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
-                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st);
+                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
+                               int precision = TDSCHA_PREC_FP64);
 
 // (nb, n, n) -> (Y + Y^T)/2 on the device
 int symmetrize_device(int nb, int n, const double *Y, double *Ys, cudaStream_t st);

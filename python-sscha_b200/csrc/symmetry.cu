@@ -261,6 +261,9 @@ int sym_transform(const SymTables &t, const PairClasses &pc, int nb, int nj, int
         pad_kernel<<<g, 256, 0, st>>>(M, P, Kp, t.n, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
         TD_CUDA(cudaGetLastError());
     }
+    if (fp32_compute && fmt == FMT_BF16 && t.umma)
+        return sym_transform_umma(t.umma, t, t.blocks_ids, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo,
+                                  t.err, st);
     if (fp32_compute) return sym_transform_tc(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st);
     return transform_all<double>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st);
 }
@@ -295,6 +298,8 @@ int sym_fold(const SymTables &t, const PairClasses &pc, const int *blocks_ids, i
              bool fp32_compute, cudaStream_t st) {
     (void)blocks_ids;
     if constexpr (std::is_same<AccT, float>::value) {
+        if (fp32_compute && t.umma)
+            return sym_fold_umma(t.umma, t, t.blocks_ids, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, t.err, st);
         if (fp32_compute) return sym_fold_tc(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);
     }
     if (fp32_compute) return fold_all<float, AccT>(t, pc, nb, nj, j0, Jf, nf_total, Z, ldz, F, ldf, ups, partD, partF, st);

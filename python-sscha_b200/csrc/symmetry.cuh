@@ -18,6 +18,8 @@ constexpr int SYM_THREADS = 256;
 constexpr int SYM_MT_MAX = 5;                      // blocks up to 16 * 5 = 80 modes
 constexpr int DMAX_SUPPORTED = 16 * SYM_MT_MAX;
 
+struct SymUmma;
+
 struct SymTables {
     const double *sym;         // per-block (N_sym, d, d) tables, concatenated
     const long long *off;      // offset of block b's table
@@ -28,7 +30,23 @@ struct SymTables {
     // starting at element offP[b]
     const float *symP, *symPT;
     const long long *offP;
+    // tensor-core (tcgen05) transform / fold of the bf16 formats (symmetry_umma.cu), when built
+    SymUmma *umma = nullptr;
+    const int *blocks_ids = nullptr;   // block of each mode (device)
+    unsigned *err = nullptr;           // error word of the call (bounded waits)
 };
+
+// bf16 hi / lo symmetry tables with their TMA descriptors and the work items of the tcgen05
+// transform / fold (symmetry_umma.cu); one per ensemble, built on the first bf16-format call.
+int sym_umma_create(const SymTables &t, int N_sym, const std::vector<int> &dim, const std::vector<long long> &sym_off,
+                    SymUmma **out);
+void sym_umma_destroy(SymUmma *u);
+int sym_transform_umma(SymUmma *u, const SymTables &t, const int *blocks_ids, int nb, int nj, int j0, const double *Ys,
+                       const double *R1, const double *ups, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo,
+                       void *r1_hi, void *r1_lo, unsigned *err, cudaStream_t st);
+int sym_fold_umma(SymUmma *u, const SymTables &t, const int *blocks_ids, int nb, int nj, int j0, int Jf, int nf_total,
+                  const float *Z, long long ldz, const float *F, long long ldf, const double *ups, double *partD,
+                  double *partF, unsigned *err, cudaStream_t st);
 
 // Block pairs (b <= c) grouped by micro-tile class MT = ceil(max(d_b, d_c) / 16).
 struct PairClasses {

@@ -591,6 +591,7 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
 }
 
 void set_wait_budget_ns(unsigned long long ns) { g_wait_budget_ns.store(ns); }
+unsigned long long wait_budget_ns() { return g_wait_budget_ns.load(); }
 void stall_next_launch() { g_stall_next.store(1); }
 
 int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {

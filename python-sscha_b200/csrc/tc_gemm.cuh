@@ -26,6 +26,7 @@ int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, c
 // Budget of every bounded wait of later launches (default 4 s), and a one-shot request that the next
 // launch's producers issue no copy (its MMA warps' first wait then runs out): the abort-path test.
 void set_wait_budget_ns(unsigned long long ns);
+unsigned long long wait_budget_ns();
 void stall_next_launch();
 
 }  // namespace tc

@@ -74,6 +74,8 @@ def load():
     lib.tdscha_tc_contract.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, ctypes.c_longlong,
                                        vp, vp, ctypes.c_longlong, vp, ctypes.c_longlong, vp]
     lib.tdscha_perturb_average_vjp_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, vp, vp, vp, vp, vp]
+    lib.tdscha_perturb_average_vjp_precision_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp,
+                                                                vp, vp, vp, vp]
     lib.tdscha_project_ensemble.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp]
     lib.tdscha_symmetries_on_modes.argtypes = [dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ip, dp, ctypes.c_int, ip,
                                                ctypes.POINTER(ip), ctypes.POINTER(dp)]
@@ -86,7 +88,7 @@ def load():
     lib.tdscha_debug_stall_next_contraction.argtypes = []
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
-    for name in ("tdscha_set_wait_budget", "tdscha_debug_stall_next_contraction", "tdscha_apply_L1_static_device", "tdscha_apply_static_L_device", "tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
+    for name in ("tdscha_perturb_average_vjp_precision_device", "tdscha_set_wait_budget", "tdscha_debug_stall_next_contraction", "tdscha_apply_L1_static_device", "tdscha_apply_static_L_device", "tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
                  "tdscha_ensemble_device_bytes", "tdscha_perturb_average_sym", "tdscha_perturb_average_sym_device",
                  "tdscha_GetPerturbAverageSym", "tdscha_apply_full_L_device", "tdscha_lanczos_step_device",
                  "tdscha_continued_fraction_device"):
@@ -178,13 +180,18 @@ class DeviceEnsemble:
                                                           PREC[precision], f_out.data_ptr(), d_out.data_ptr(),
                                                           _stream_ptr(stream)))
 
-    def perturb_average_vjp(self, R1, Ys, fbar, Dbar, Ybar, rhobar, apply_d4=1, stream=None):
+    def perturb_average_vjp(self, R1, Ys, fbar, Dbar, Ybar, rhobar, apply_d4=1, stream=None, precision="fp64"):
         """d[sum_k <fbar_k, f_k> + <Dbar_k, D_k>] / d(Y, rho) into Ybar (N, n), rhobar (N); all float64
-        CUDA tensors, Ys and Dbar symmetric (nb, n, n)."""
+        CUDA tensors, Ys and Dbar symmetric (nb, n, n); `precision` of the eight ensemble contractions."""
         nb = R1.shape[0]
-        check(self._lib.tdscha_perturb_average_vjp_device(self.handle, nb, R1.data_ptr(), Ys.data_ptr(), int(apply_d4),
-                                                          fbar.data_ptr(), Dbar.data_ptr(), Ybar.data_ptr(),
-                                                          rhobar.data_ptr(), _stream_ptr(stream)))
+        if precision == "fp64":
+            check(self._lib.tdscha_perturb_average_vjp_device(self.handle, nb, R1.data_ptr(), Ys.data_ptr(), int(apply_d4),
+                                                              fbar.data_ptr(), Dbar.data_ptr(), Ybar.data_ptr(),
+                                                              rhobar.data_ptr(), _stream_ptr(stream)))
+            return
+        check(self._lib.tdscha_perturb_average_vjp_precision_device(
+            self.handle, nb, R1.data_ptr(), Ys.data_ptr(), int(apply_d4), PREC[precision], fbar.data_ptr(),
+            Dbar.data_ptr(), Ybar.data_ptr(), rhobar.data_ptr(), _stream_ptr(stream)))
 
     def apply_full_L(self, psi, out, transpose, opts, precision="fp64", stream=None):
         """psi, out: (nb, len) float64 CUDA tensors; transpose: sequence of nb ints."""

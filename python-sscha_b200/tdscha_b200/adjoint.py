@@ -33,11 +33,14 @@ def _torch():
 class _Ctl:
     """What the autograd function needs besides tensors."""
 
-    def __init__(self, lanc, precision="fp64"):
+    def __init__(self, lanc, precision="fp64", vjp_precision=None):
         torch = _torch()
-        if precision not in _native.PREC:
-            raise ValueError(f"precision must be one of {list(_native.PREC)}")
+        vjp_precision = precision if vjp_precision is None else vjp_precision
+        for p in (precision, vjp_precision):
+            if p not in _native.PREC:
+                raise ValueError(f"precision must be one of {list(_native.PREC)}")
         self.precision = precision
+        self.vjp_precision = vjp_precision
         if lanc.use_wigner:
             raise NotImplementedError("gradients are available in the standard representation (use_wigner = False)")
         lanc._check_init()
@@ -111,7 +114,8 @@ def _make_function():
                 fbar, Dbar = ctl.epilogue_transpose(gout, tr)
                 Y_bar = torch.empty((ctl.ens.N, n), dtype=torch.float64, device=psi.device)
                 rho_bar = torch.empty(ctl.ens.N, dtype=torch.float64, device=psi.device)
-                ctl.ens.perturb_average_vjp(R1, Y1, fbar, Dbar, Y_bar, rho_bar, apply_d4=ctl.apply_d4)
+                ctl.ens.perturb_average_vjp(R1, Y1, fbar, Dbar, Y_bar, rho_bar, apply_d4=ctl.apply_d4,
+                                            precision=ctl.vjp_precision)
             elif ctx.needs_input_grad[1] or ctx.needs_input_grad[2]:
                 Y_bar = torch.zeros((ctl.ens.N, ctl.n), dtype=torch.float64, device=psi.device)
                 rho_bar = torch.zeros(ctl.ens.N, dtype=torch.float64, device=psi.device)
@@ -132,14 +136,16 @@ def apply_full_L(psi, Y, rho, lanc, transpose, ctl=None):
     return _FN.apply(psi, Y, rho, ctl or _Ctl(lanc), list(transpose))
 
 
-def green_function(lanc, omega, smearing, n_steps, Y, rho, psi0=None, checkpoint_every=10, precision="fp64"):
+def green_function(lanc, omega, smearing, n_steps, Y, rho, psi0=None, checkpoint_every=10, precision="fp64",
+                   vjp_precision=None):
     """G(omega) (complex, CUDA) of the bi-conjugate chain of n_steps steps from psi0 (default
     lanc.psi), differentiable with respect to Y and rho.  `precision` is the arithmetic of the
-    ensemble contractions inside the forward and transposed applies; the recurrence, the continued
-    fraction and the vector-Jacobian product of the averages are FP64."""
+    ensemble contractions inside the forward and transposed applies, `vjp_precision` (default the
+    same) that of the contractions of the averages' vector-Jacobian product; the recurrence, the
+    continued fraction and the rest of the VJP are FP64."""
     torch = _torch()
     from torch.utils.checkpoint import checkpoint
-    ctl = _Ctl(lanc, precision)
+    ctl = _Ctl(lanc, precision, vjp_precision)
     dev = "cuda"
     v = torch.as_tensor(np.asarray(lanc.psi if psi0 is None else psi0, dtype=np.float64), device=dev)
     q = v / torch.sqrt((v * v).sum())

@@ -60,6 +60,33 @@ def test_average_vjp_matches_torch_autograd(cuda, rocksalt_l2):
         assert np.abs(rbar.cpu().numpy() - gr.numpy()).max() <= 1e-10 * np.abs(gr.numpy()).max()
 
 
+@pytest.mark.parametrize("precision,tol", [("bf16x3", 1e-4), ("tf32x3", 2e-5)])
+def test_mixed_precision_vjp_matches_fp64(cuda, rocksalt_l2, precision, tol):
+    """The averages' VJP with its contractions on the tcgen05 kernel (tdscha_perturb_average_vjp_
+    precision_device) against the FP64 VJP (pinned to float64 torch autograd above)."""
+    d = rocksalt_l2
+    n = d["X"].shape[1]
+    L = _lanczos(d)
+    rng = np.random.default_rng(22)
+    nb = 3
+    R1 = rng.standard_normal((nb, n)) * 1e-2
+    Ys = _sym(rng, nb, n, 1e-2)
+    fb = rng.standard_normal((nb, n))
+    Db = _sym(rng, nb, n, 1.0)
+    c = lambda a: torch.as_tensor(a, device="cuda").contiguous()   # noqa: E731
+    for d4 in (1, 0):
+        out = {}
+        for prec in ("fp64", precision):
+            Ybar = torch.empty((L.N, n), dtype=torch.float64, device="cuda")
+            rbar = torch.empty(L.N, dtype=torch.float64, device="cuda")
+            L.device_ensemble.perturb_average_vjp(c(R1), c(Ys), c(fb), c(Db), Ybar, rbar, apply_d4=d4, precision=prec)
+            out[prec] = (Ybar.cpu().numpy(), rbar.cpu().numpy())
+        eY = np.abs(out[precision][0] - out["fp64"][0]).max() / np.abs(out["fp64"][0]).max()
+        er = np.abs(out[precision][1] - out["fp64"][1]).max() / np.abs(out["fp64"][1]).max()
+        print(f"VJP {precision} d4={d4}: Ybar {eY:.2e} rhobar {er:.2e}")
+        assert eY < tol and er < tol
+
+
 def test_apply_adjoint_matches_finite_differences(cuda, rocksalt_l2):
     from tdscha_b200 import adjoint
     d = rocksalt_l2
@@ -173,7 +200,8 @@ def test_green_function_gradient_wrt_couplings(cuda):
 def test_gradient_at_the_differentiation_workload_size(cuda):
     """The adjoint at the size of the differentiation workload (rock-salt 3x3x3, n = 159, N = 5000,
     1296 symmetries; a shorter chain of 12 steps, checkpoint every 5): directional derivatives of
-    sum_w Im G(w) along random directions of the forces and weights against central differences."""
+    sum_w Im G(w) along random directions of the forces and weights against Richardson-extrapolated
+    central differences."""
     from tdscha_b200 import adjoint, rocksalt as RS
     from tdscha_b200 import DynamicalLanczos as DL
     s = RS.build_system(3)
@@ -207,12 +235,15 @@ def test_gradient_at_the_differentiation_workload_size(cuda):
         L.device_ensemble.close()
         return v
 
-    hY = 1e-5 * np.abs(Y).max()
-    fdY = (value(Y + hY * dY, rho) - value(Y - hY * dY, rho)) / (2 * hY)
+    def richardson(f, h):   # central differences at h and h / 2, O(h^4)
+        c1 = (f(h) - f(-h)) / (2 * h)
+        c2 = (f(h / 2) - f(-h / 2)) / h
+        return (4 * c2 - c1) / 3
+
+    fdY = richardson(lambda t: value(Y + t * dY, rho), 1e-4 * np.abs(Y).max())
     adY = float((gY.cpu().numpy() * dY).sum())
-    hr = 1e-5
-    fdr = (value(Y, rho + hr * dr) - value(Y, rho - hr * dr)) / (2 * hr)
+    fdr = richardson(lambda t: value(Y, rho + t * dr), 1e-4)
     adr = float((gr.cpu().numpy() * dr).sum())
-    print(f"3x3x3 N=5000 gradient: Y {adY:.8e} vs FD {fdY:.8e}; rho {adr:.8e} vs FD {fdr:.8e}")
+    print(f"3x3x3 N=5000 gradient: Y {adY:.10e} vs FD {fdY:.10e}; rho {adr:.10e} vs FD {fdr:.10e}")
     assert abs(adY - fdY) <= 1e-6 * abs(fdY)
     assert abs(adr - fdr) <= 1e-6 * abs(fdr)

@@ -124,32 +124,46 @@ def test_continued_fraction_matches_oracle(cuda, mode10, opts):
 
 
 @pytest.mark.parametrize("n_rep_orth", [1, 2])
+def test_gram_schmidt_step_matches_oracle(cuda, n_rep_orth):
+    """The device Gram-Schmidt of one new Lanczos pair (DynamicalLanczos.py:6244-6316) against the
+    oracle's restatement on the same inputs: a window of 4 basis pairs, with and without the
+    symmetric Wigner mask."""
+    torch = cuda
+    from tdscha_b200 import DynamicalLanczos as DL
+    rng = np.random.default_rng(3 + n_rep_orth)
+    n = 12
+    ln = n + n * (n + 1)
+    basis_Q = [rng.standard_normal(ln) for _ in range(6)]
+    basis_P = [rng.standard_normal(ln) for _ in range(6)]
+    q, p = rng.standard_normal(ln), rng.standard_normal(ln)
+    c = 0.37
+    o = LO.OracleLanczos.__new__(LO.OracleLanczos)
+    o.n_modes = n
+    for mask in (None, o.mask_dot_wigner()):
+        dot = (lambda a, b: a.dot(b)) if mask is None else (lambda a, b: a.dot(b * mask))   # noqa: E731
+        rq, rp, rs, _ = LO.gram_schmidt(q, p, basis_Q, basis_P, n_rep_orth, 4, c, dot)
+        window = [(torch.as_tensor(Q, device="cuda"), torch.as_tensor(P, device="cuda")) for Q, P in zip(basis_Q[-4:], basis_P[-4:])]
+        tm = None if mask is None else torch.as_tensor(mask, device="cuda")
+        gq, gp, gs, _ = DL._gram_schmidt(torch.as_tensor(q, device="cuda"), torch.as_tensor(p, device="cuda"), window,
+                                         n_rep_orth, c, tm)
+        assert np.abs(gq.cpu().numpy() - rq).max() <= 1e-12 * np.abs(rq).max()
+        assert np.abs(gp.cpu().numpy() - rp).max() <= 1e-12 * np.abs(rp).max()
+        assert abs(gs - rs) <= 1e-12 * abs(rs)
+
+
+@pytest.mark.parametrize("n_rep_orth", [1, 2])
 def test_chain_with_gram_schmidt_matches_oracle(cuda, rocksalt_l2, n_rep_orth):
-    """run_FT with Gram-Schmidt re-orthogonalisation (DynamicalLanczos.py:6244-6316) against the
-    oracle's restatement, with a window shorter than the chain (n_ortho = 4).  On this short chain the
-    re-orthogonalisation moves the coefficients by ~1e-11 relative, so the check is on that shift
-    itself: (with GS) / (without GS) - 1 of s_norm, c and a, GPU against oracle."""
+    """run_FT with Gram-Schmidt re-orthogonalisation against the oracle's chain (n_ortho = 4, shorter
+    than the chain); on this 6-configuration ensemble both chains agree to ~1e-11 over 10 steps, the
+    size of the re-orthogonalisation's own effect, which the test above checks exactly."""
     d = rocksalt_l2
-    steps = 10
-
-    def chains(**kw):
-        L = _lanczos(d)
-        O = _oracle(d)
-        L.prepare_mode(3)
-        O.prepare_mode(3)
-        L.run_FT(steps, verbose=False, **kw)
-        O.run_FT(steps, **kw)
-        return L, O
-
-    L0, O0 = chains()
-    L1, O1 = chains(n_rep_orth=n_rep_orth, n_ortho=4)
-    assert len(L1.a_coeffs) == len(O1.a_coeffs) == len(O0.a_coeffs)
-    for attr in ("s_norm", "c_coeffs", "a_coeffs"):
-        shift_gpu = np.array(getattr(L1, attr)) / np.array(getattr(L0, attr)) - 1
-        shift_ref = np.array(getattr(O1, attr)) / np.array(getattr(O0, attr)) - 1
-        scale = np.abs(shift_ref).max()
-        print(f"GS x{n_rep_orth} {attr}: shift {scale:.2e}, GPU - oracle {np.abs(shift_gpu - shift_ref).max():.2e}")
-        assert scale > 1e-13
-        assert np.abs(shift_gpu - shift_ref).max() <= 0.05 * scale, attr
-        ref = np.array(getattr(O1, attr))
-        assert np.abs(np.array(getattr(L1, attr)) - ref).max() <= 1e-10 * np.abs(ref).max()
+    L = _lanczos(d)
+    O = _oracle(d)
+    L.prepare_mode(3)
+    O.prepare_mode(3)
+    L.run_FT(10, verbose=False, n_rep_orth=n_rep_orth, n_ortho=4)
+    O.run_FT(10, n_rep_orth=n_rep_orth, n_ortho=4)
+    assert len(L.a_coeffs) == len(O.a_coeffs)
+    for attr in ("a_coeffs", "b_coeffs", "c_coeffs", "s_norm"):
+        ref = np.array(getattr(O, attr))
+        assert np.abs(np.array(getattr(L, attr)) - ref).max() <= 1e-9 * np.abs(ref).max(), attr
