@@ -586,14 +586,13 @@ static int build_chunk_operands(tdscha_ensemble *e, long long c0, long long Nc, 
     return 0;
 }
 
-// TDSCHA_SYM_UMMA=0 keeps the bf16 formats' symmetry transform / fold on the mma.sync kernels
+// TDSCHA_SYM_UMMA=1 runs the bf16 formats' symmetry transform / fold on the tcgen05 kernels of
+// symmetry_umma.cu instead of the mma.sync kernels of symmetry_tc.cu (read at every call).  Off by
+// default: on the 4x4x4 benchmark the tcgen05 version is correct but slower (96 + 112 ms against
+// 69 + 105 ms per 16-vector step) and less accurate (bf16 instead of tf32 splitting).
 static bool sym_umma_enabled() {
-    static int v = -1;
-    if (v < 0) {
-        const char *env = getenv("TDSCHA_SYM_UMMA");
-        v = (env && atoi(env) == 0) ? 0 : 1;
-    }
-    return v == 1;
+    const char *env = getenv("TDSCHA_SYM_UMMA");
+    return env && atoi(env) == 1;
 }
 
 int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4, int precision,

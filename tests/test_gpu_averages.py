@@ -101,3 +101,23 @@ def test_mixed_modes_against_fp64_all_block_classes(cuda, L, N, precision, tol):
     ens.close()
     assert _rel(out[precision][0], out["fp64"][0]) < tol
     assert _rel(out[precision][1], out["fp64"][1]) < tol
+
+
+@pytest.mark.parametrize("fixture", ["mode10", "rocksalt_l2"])
+def test_tcgen05_symmetry_kernels_match(request, cuda, fixture, monkeypatch):
+    """The opt-in tcgen05 symmetry transform / fold of the bf16 formats (TDSCHA_SYM_UMMA=1,
+    symmetry_umma.cu) against the reference kernel's golden outputs and the default mma.sync path."""
+    d = request.getfixturevalue(fixture)
+    ens = _dev_ens(d)
+    for case in ("case0", "case1", "case2"):
+        monkeypatch.delenv("TDSCHA_SYM_UMMA", raising=False)
+        f0, d0 = ens.perturb_average(d[f"{case}_R1"], d[f"{case}_Y1"], int(d[f"{case}_d4"]), "bf16x3")
+        monkeypatch.setenv("TDSCHA_SYM_UMMA", "1")
+        f1, d1 = ens.perturb_average(d[f"{case}_R1"], d[f"{case}_Y1"], int(d[f"{case}_d4"]), "bf16x3")
+        ef, ed = _rel(f1, d[f"{case}_f"]), _rel(d1, d[f"{case}_d2v"])
+        print(f"{fixture} tcgen05 symmetry bf16x3 {case}: f {ef:.2e} d2v {ed:.2e}; vs mma.sync path "
+              f"{_rel(f1, f0):.2e} {_rel(d1, d0):.2e}")
+        assert ef < TOL["bf16x3"] and ed < TOL["bf16x3"]
+        assert _rel(f1, f0) < 1e-4 and _rel(d1, d0) < 1e-4
+    monkeypatch.delenv("TDSCHA_SYM_UMMA", raising=False)
+    ens.close()
