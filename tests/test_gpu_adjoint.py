@@ -242,7 +242,7 @@ def test_gradient_at_the_differentiation_workload_size(cuda):
 
     fdY = richardson(lambda t: value(Y + t * dY, rho), 1e-4 * np.abs(Y).max())
     adY = float((gY.cpu().numpy() * dY).sum())
-    fdr = richardson(lambda t: value(Y, rho + t * dr), 1e-4)
+    fdr = richardson(lambda t: value(Y, rho + t * dr), 1e-3)
     adr = float((gr.cpu().numpy() * dr).sum())
     print(f"3x3x3 N=5000 gradient: Y {adY:.10e} vs FD {fdY:.10e}; rho {adr:.10e} vs FD {fdr:.10e}")
     assert abs(adY - fdY) <= 1e-6 * abs(fdY)
