@@ -49,6 +49,9 @@ def parse():
     ap.add_argument("--sym-on-gpu", action="store_true",
                     help="project the symmetry operations onto the modes on the GPU (large supercells)")
     ap.add_argument("--accuracy-steps", type=int, default=200)
+    ap.add_argument("--perturbed-fp64", action="store_true",
+                    help="when no stored FP64 chain matches: run the live FP64 reference chain together with a "
+                         "copy whose applies are perturbed by 3e-10 (the sensitivity of G(w) at each step count)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--batch-systems", action="store_true",
@@ -241,6 +244,47 @@ FP64_CHAIN = os.path.join(REPO, "tests", "golden", "c2_fp64_chain.npz")
 FP64_PERTURBED = os.path.join(REPO, "tests", "golden", "c2_fp64_perturbed_chains.npz")
 
 
+def fp64_device_chains(ens, psi0, steps, apply_noise, seed=5):
+    """Bi-conjugate FP64 chains (run_FT semantics, DynamicalLanczos.py:6059-6153) from the rows of
+    psi0, advanced together; the apply outputs of chain c are moved by a seeded Gaussian vector of
+    relative 2-norm apply_noise[c].  Returns (steps, chains, 4): a, b, c, s_norm."""
+    import torch
+    from tdscha_b200 import _native
+    dev = "cuda"
+    nc, ln = psi0.shape
+    q = torch.as_tensor(psi0, device=dev)
+    q = q / q.norm(dim=1, keepdim=True)
+    p = q.clone()
+    qp, pp = torch.zeros_like(q), torch.zeros_like(q)
+    sc = torch.tensor([[0.0, 0.0, 1.0, 0.0, 1.0, 0.0]] * nc, dtype=torch.float64, device=dev)
+    opts = _native.ApplyOpts(0, 0, 0, 0, 0, 0.0)
+    tr = [0] * nc + [1] * nc
+    vec = torch.empty((2 * nc, ln), dtype=torch.float64, device=dev)
+    out = torch.empty_like(vec)
+    qn, pn = torch.empty_like(q), torch.empty_like(q)
+    sc_out = torch.empty((nc, 4), dtype=torch.float64, device=dev)
+    eps = torch.as_tensor(np.concatenate([apply_noise, apply_noise]), device=dev)[:, None]
+    gen = torch.Generator(device=dev).manual_seed(seed)
+    coef = []
+    for k in range(steps):
+        vec[:nc].copy_(q)
+        vec[nc:].copy_(p)
+        ens.apply_full_L(vec, out, tr, opts, "fp64")
+        g = torch.randn(out.shape, generator=gen, dtype=torch.float64, device=dev)
+        out += eps * out.norm(dim=1, keepdim=True) * g / g.norm(dim=1, keepdim=True)
+        _native.lanczos_step(out[:nc], out[nc:], q, p, qp, pp, sc, None, qn, pn, sc_out)
+        new = torch.empty_like(sc)
+        new[:, 0] = sc_out[:, 2]
+        new[:, 1] = sc_out[:, 1]
+        new[:, 2] = sc_out[:, 3]
+        new[:, 3] = sc[:, 2]
+        new[:, 4] = sc[:, 0] if k >= 1 else 1.0
+        new[:, 5] = k + 1
+        qp, pp, q, p, sc = q, p, qn.clone(), pn.clone(), new
+        coef.append(sc_out.cpu().numpy().copy())
+    return np.array(coef)
+
+
 def precision_check(a, s, X, Y, rho, ens, precision=None):
     """G(w) of the seeded chain after `accuracy_steps` steps in `precision` (default the benchmark's)
     against the same chain in FP64: the stored FP64 chain when it was made from these inputs, else
@@ -259,10 +303,21 @@ def precision_check(a, s, X, Y, rho, ens, precision=None):
     t0 = time.perf_counter()
     mixed = RS.seeded_chain(s, X, Y, rho, ens, precision, steps)
     t_mixed = time.perf_counter() - t0
+    live_perturbed = None
     if ref is None:
-        c64 = RS.seeded_chain(s, X, Y, rho, ens, "fp64", steps)
-        ref = {"a": np.array(c64.a_coeffs), "b": np.array(c64.b_coeffs), "c": np.array(c64.c_coeffs),
-               "source": "live FP64 chain"}
+        if a.perturbed_fp64:
+            # the FP64 chain and, beside it, the same chain with every apply moved by a seeded 3e-10
+            # (relative 2-norm), advanced together
+            n = s.n_modes
+            psi0 = np.zeros(n + n * (n + 1))
+            psi0[:n] = np.random.default_rng(RS.CHAIN_SEED).standard_normal(n)
+            coef = fp64_device_chains(ens, np.tile(psi0, (2, 1)), steps, np.array([0.0, 3e-10]))
+            ref = {"a": coef[:, 0, 0], "b": coef[:, 0, 1], "c": coef[:, 0, 2], "source": "live FP64 chain"}
+            live_perturbed = {"apply_3e-10": (coef[:, 1, 0], coef[:, 1, 1], coef[:, 1, 2])}
+        else:
+            c64 = RS.seeded_chain(s, X, Y, rho, ens, "fp64", steps)
+            ref = {"a": np.array(c64.a_coeffs), "b": np.array(c64.b_coeffs), "c": np.array(c64.c_coeffs),
+                   "source": "live FP64 chain"}
     w, eta = RS.gf_grid()
     k = min(len(ref["a"]), len(mixed.a_coeffs))
     amx, bmx, cmx = (np.array(x) for x in (mixed.a_coeffs, mixed.b_coeffs, mixed.c_coeffs))
@@ -307,6 +362,10 @@ def precision_check(a, s, X, Y, rho, ens, precision=None):
     out["a_first_step_rel_err_above_1e-6"] = first_divergence(amx)
     # the same for FP64 chains with tiny seeded perturbations (start vector 1e-12; every apply
     # 3e-9 / 3e-10 relative): how much any error of that size moves G(w) of the unconverged chain
+    if live_perturbed is not None:
+        out["fp64_perturbed_g_rel_err_max_by_steps"] = {nm: by_steps_of(*v) for nm, v in live_perturbed.items()}
+        out["fp64_perturbed_a_first_step_rel_err_above_1e-6"] = {nm: first_divergence(v[0])
+                                                                  for nm, v in live_perturbed.items()}
     if ref["source"].startswith("stored") and os.path.exists(FP64_PERTURBED):
         dp = np.load(FP64_PERTURBED)
         if np.allclose(dp["checksum"], RS.ensemble_checksum(X, Y, rho), rtol=1e-12, atol=0) and int(dp["steps"]) >= k:

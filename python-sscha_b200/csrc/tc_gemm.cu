@@ -21,6 +21,7 @@
 #include <atomic>
 #include <cstdint>
 #include <cstdlib>
+#include <functional>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -448,11 +449,7 @@ static int default_drain(int nprod) {
     return nprod == 3 ? 1 : 16;
 }
 
-// ---- tile-order autotuner -------------------------------------------------------------------------
-// The best tile-group size depends on the problem shape (the two L2 halves of the part make it hard
-// to predict), so on the first call for a (format, products, M, N, K) the launcher times a few
-// candidates on the caller's stream (fastest of two runs each; every run writes the same D) and
-// remembers the winner.  Small problems, or TDSCHA_AUTOTUNE=0, use the m-fastest order.
+// Autotuner key: one choice per (format, products, M, N, K, device).
 struct TuneKey {
     int tf32, nprod, M, N, K, dev;
     bool operator<(const TuneKey &o) const {
@@ -460,54 +457,6 @@ struct TuneKey {
     }
 };
 static std::mutex g_tune_mutex;
-static std::map<TuneKey, int> g_tune;
-
-template <typename Launch>
-static int tuned_group(int tf32, int nprod, int M, int N, int K, int num_m, long long tiles, int sms, cudaStream_t st,
-                       Launch &launch, bool allow_trials, int *gm_out) {
-    int dev = 0;
-    TD_CUDA(cudaGetDevice(&dev));
-    const TuneKey key{tf32, nprod, M, N, K, dev};
-    {
-        std::lock_guard<std::mutex> lock(g_tune_mutex);
-        auto it = g_tune.find(key);
-        if (it != g_tune.end()) { *gm_out = it->second; return 0; }
-    }
-    const char *env = getenv("TDSCHA_AUTOTUNE");
-    const bool enabled = allow_trials && !(env && atoi(env) == 0);
-    int best = num_m;
-    if (enabled && tiles >= 8LL * sms) {
-        const int cand_all[] = {num_m, 48, 24, 12, 6};
-        cudaEvent_t e0, e1;
-        TD_CUDA(cudaEventCreate(&e0));
-        TD_CUDA(cudaEventCreate(&e1));
-        float best_ms = 1e30f;
-        for (int ci = 0; ci < 5; ++ci) {
-            const int cand = cand_all[ci];
-            bool dup = cand > num_m;
-            for (int cj = 0; cj < ci; ++cj) dup = dup || cand_all[cj] == cand;
-            if (dup) continue;
-            float t_min = 1e30f;
-            for (int rep = 0; rep < 2; ++rep) {
-                TD_CUDA(cudaEventRecord(e0, st));
-                launch(cand);
-                TD_CUDA(cudaGetLastError());
-                TD_CUDA(cudaEventRecord(e1, st));
-                TD_CUDA(cudaEventSynchronize(e1));
-                float ms = 0.f;
-                TD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                t_min = std::min(t_min, ms);
-            }
-            if (t_min < best_ms) { best_ms = t_min; best = cand; }
-        }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-    }
-    std::lock_guard<std::mutex> lock(g_tune_mutex);
-    if (allow_trials) g_tune[key] = best;
-    *gm_out = best;
-    return 0;
-}
 
 // One tile-start counter per (device, stream), zeroed on the stream before every launch, so that
 // contractions running concurrently on different streams never share one.  A counter (256 bytes)
@@ -538,8 +487,16 @@ static unsigned tile_sync_budget_ns() {
     return (unsigned)v;
 }
 
+// One tile configuration of a contraction, ready to launch with a tile-group size.
+struct Prepared {
+    std::function<void(int)> launch;
+    int num_m = 0;
+    long long tiles = 0;
+};
+
 template <int BN, int STAGES, bool TF32, int NPROD>
-static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+static int prepare_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err,
+                       unsigned *counter, int stall, Prepared *out) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     CUtensorMap a_hi, a_lo, b_hi, b_lo;
     TD_TRY(make_map(&a_hi, op.A_hi, TF32, M, K, op.lda, BM));
@@ -559,33 +516,112 @@ static int launch_cfg(const GemmOperands &op, int M, int N, int K, float *D, lon
     const long long tiles = (long long)ceil_div(M, BM) * ceil_div(N, BN);
     const int num_kb = K / C::K_ELEMS;
     const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(NPROD), num_kb);
-    dim3 grid((unsigned)std::min<long long>(tiles, sms));
-    const int num_m = ceil_div(M, BM);
+    const dim3 grid((unsigned)std::min<long long>(tiles, sms));
     const unsigned sync_ns = tile_sync_budget_ns();
     const int accumulate = op.accumulate ? 1 : 0;
+    const unsigned long long wait_ns = g_wait_budget_ns.load();
+    unsigned *cnt = (sync_ns > 0 && tiles > grid.x) ? counter : nullptr;
+    out->num_m = ceil_div(M, BM);
+    out->tiles = tiles;
+    out->launch = [=](int gm) {
+        if (cnt) cudaMemsetAsync(cnt, 0, sizeof(unsigned), st);
+        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err, cnt, sync_ns,
+                                                        accumulate, wait_ns, stall);
+    };
+    return 0;
+}
+
+// ---- tile-shape and tile-order autotuner -----------------------------------------------------------
+// On the first call for a (format, products, M, N, K) the launcher times every candidate (tile
+// configuration, tile-group size) on the caller's stream (fastest of two runs each; every run writes
+// the same D) and remembers the winner.  Tile configurations: 128 x 256 with the stage count that
+// fits (2 for the split modes, 4 otherwise) and 128 x 128 with more stages (3 / 6): the wide tile
+// reads each A panel half as often, the narrow one keeps a deeper copy pipeline.  Small problems,
+// launches that accumulate or are being captured, and TDSCHA_AUTOTUNE=0 use the wide tile in the
+// m-fastest order; TDSCHA_TILE_N (256 | 128) and TDSCHA_GROUP_M fix the choice.
+static std::map<TuneKey, std::pair<int, int>> g_tune_cfg;
+
+static int choose(int tf32, int nprod, int M, int N, int K, const Prepared *cfgs, int ncfg, cudaStream_t st, bool allow_trials,
+                  int *cfg_out, int *gm_out) {
+    int dev = 0, sms = 148;
+    TD_CUDA(cudaGetDevice(&dev));
+    TD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int forced_cfg = -1;
+    if (const char *env = getenv("TDSCHA_TILE_N")) forced_cfg = atoi(env) == 128 ? 1 : 0;
+    const char *env_gm = getenv("TDSCHA_GROUP_M");
+    if (forced_cfg >= 0 || env_gm) {
+        const int c = forced_cfg >= 0 ? std::min(forced_cfg, ncfg - 1) : 0;
+        *cfg_out = c;
+        *gm_out = env_gm ? std::max(1, std::min(cfgs[c].num_m, atoi(env_gm))) : cfgs[c].num_m;
+        return 0;
+    }
+    const TuneKey key{tf32, nprod, M, N, K, dev};
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        auto it = g_tune_cfg.find(key);
+        if (it != g_tune_cfg.end()) { *cfg_out = it->second.first; *gm_out = it->second.second; return 0; }
+    }
+    const char *env = getenv("TDSCHA_AUTOTUNE");
+    const bool enabled = allow_trials && !(env && atoi(env) == 0);
+    int best_c = 0, best_gm = cfgs[0].num_m;
+    if (enabled && cfgs[0].tiles >= 8LL * sms) {
+        cudaEvent_t e0, e1;
+        TD_CUDA(cudaEventCreate(&e0));
+        TD_CUDA(cudaEventCreate(&e1));
+        float best_ms = 1e30f;
+        for (int c = 0; c < ncfg; ++c) {
+            const int num_m = cfgs[c].num_m;
+            const int cand_all[] = {num_m, 48, 24, 12, 6};
+            for (int ci = 0; ci < 5; ++ci) {
+                const int cand = cand_all[ci];
+                bool dup = cand > num_m;
+                for (int cj = 0; cj < ci; ++cj) dup = dup || cand_all[cj] == cand;
+                if (dup) continue;
+                float t_min = 1e30f;
+                for (int rep = 0; rep < 2; ++rep) {
+                    TD_CUDA(cudaEventRecord(e0, st));
+                    cfgs[c].launch(cand);
+                    TD_CUDA(cudaGetLastError());
+                    TD_CUDA(cudaEventRecord(e1, st));
+                    TD_CUDA(cudaEventSynchronize(e1));
+                    float ms = 0.f;
+                    TD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                    t_min = std::min(t_min, ms);
+                }
+                if (t_min < best_ms) { best_ms = t_min; best_c = c; best_gm = cand; }
+            }
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+    }
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    if (allow_trials) g_tune_cfg[key] = {best_c, best_gm};
+    *cfg_out = best_c;
+    *gm_out = best_gm;
+    return 0;
+}
+
+template <bool TF32, int NPROD>
+static int launch_tuned(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+    constexpr int S_WIDE = NPROD == 3 ? 2 : 4, S_NARROW = NPROD == 3 ? 3 : 6;
+    int dev = 0;
+    TD_CUDA(cudaGetDevice(&dev));
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     TD_CUDA(cudaStreamIsCapturing(st, &cap));
     const bool capturing = cap != cudaStreamCaptureStatusNone;
     unsigned *counter = nullptr;
-    if (sync_ns > 0 && tiles > grid.x) TD_TRY(tile_sync_counter(dev, st, capturing, &counter));
-    const unsigned long long wait_ns = g_wait_budget_ns.load();
+    if (tile_sync_budget_ns() > 0) TD_TRY(tile_sync_counter(dev, st, capturing, &counter));
     const int stall = g_stall_next.exchange(0);
-    auto launch = [&](int gm) {
-        if (counter) cudaMemsetAsync(counter, 0, sizeof(unsigned), st);
-        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err,
-                                                        counter, sync_ns, accumulate, wait_ns, stall);
-    };
-    if (stall) {                                        // abort-path test: one launch, no tuning trials
-        launch(num_m);
-    } else if (const char *env = getenv("TDSCHA_GROUP_M")) {   // tuning knob: fixed tile-group size
-        launch(std::max(1, std::min(num_m, atoi(env))));
-    } else {
-        int gm = 0;
-        // trial runs write D, so an accumulating launch only reuses a group size tuned earlier
-        // (and a launch being captured into a CUDA graph runs nothing, so it cannot time trials)
-        TD_TRY(tuned_group(TF32 ? 1 : 0, NPROD, M, N, K, num_m, tiles, sms, st, launch, !accumulate && !capturing, &gm));
-        launch(gm);
+    Prepared cfgs[2];
+    TD_TRY((prepare_cfg<256, S_WIDE, TF32, NPROD>(op, M, N, K, D, ldd, st, err, counter, stall, &cfgs[0])));
+    TD_TRY((prepare_cfg<128, S_NARROW, TF32, NPROD>(op, M, N, K, D, ldd, st, err, counter, stall, &cfgs[1])));
+    int c = 0, gm = cfgs[0].num_m;
+    if (!stall) {   // abort-path test: one launch of the wide tile, no tuning trials
+        // trial runs write D, so an accumulating launch only reuses a choice tuned earlier (and a
+        // launch being captured into a CUDA graph runs nothing, so it cannot time trials)
+        TD_TRY(choose(TF32 ? 1 : 0, NPROD, M, N, K, cfgs, 2, st, !op.accumulate && !capturing, &c, &gm));
     }
+    cfgs[c].launch(gm);
     TD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -605,11 +641,11 @@ int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, c
              "tc::gemm: leading dimensions lda=%lld ldb=%lld ldd=%lld inconsistent with K=%d N=%d", op.lda, op.ldb, ldd, K, N);
     TD_CHECK(op.A_hi && op.B_hi && D && (op.nprod == 1 || (op.A_lo && op.B_lo)), TDSCHA_EINVAL, "tc::gemm: NULL operand");
     if (tf32) {
-        if (op.nprod == 3) return launch_cfg<256, 2, true, 3>(op, M, N, K, D, ldd, st, err);
-        return launch_cfg<256, 4, true, 1>(op, M, N, K, D, ldd, st, err);
+        if (op.nprod == 3) return launch_tuned<true, 3>(op, M, N, K, D, ldd, st, err);
+        return launch_tuned<true, 1>(op, M, N, K, D, ldd, st, err);
     }
-    if (op.nprod == 3) return launch_cfg<256, 2, false, 3>(op, M, N, K, D, ldd, st, err);
-    return launch_cfg<256, 4, false, 1>(op, M, N, K, D, ldd, st, err);
+    if (op.nprod == 3) return launch_tuned<false, 3>(op, M, N, K, D, ldd, st, err);
+    return launch_tuned<false, 1>(op, M, N, K, D, ldd, st, err);
 }
 
 }  // namespace tc

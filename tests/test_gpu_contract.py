@@ -29,10 +29,14 @@ def split(torch, A, mode):
 SHAPES = [(128, 256, 64), (256, 512, 256), (200, 300, 192), (384, 72, 128), (128, 256, 2048), (333, 129, 4096)]
 
 
+@pytest.mark.parametrize("tile_n", ["256", "128"])
 @pytest.mark.parametrize("mode", ["bf16", "bf16x3", "tf32", "tf32x3"])
 @pytest.mark.parametrize("shape", SHAPES)
-def test_tc_contract_matches_fp64(cuda, mode, shape):
+def test_tc_contract_matches_fp64(cuda, mode, shape, tile_n, monkeypatch):
+    """Both tile configurations the autotuner chooses from (128 x 256 and 128 x 128 output tiles),
+    forced through TDSCHA_TILE_N."""
     torch = cuda
+    monkeypatch.setenv("TDSCHA_TILE_N", tile_n)
     from tdscha_b200 import _native
     M, N, K = shape
     if mode.startswith("tf32") and K % 32:
