@@ -27,9 +27,12 @@ for _p in (REPO, os.path.join(REPO, "python-sscha_b200")):
     if _p not in sys.path:
         sys.path.insert(0, _p)
 
-# DRAM bytes (read + write) of one [a|b] contraction launch, from a 1-pass ncu capture of the same
-# workload (profiles/tc_gemm_c2.md); keyed by (L, N, chains, precision).
-MEASURED_TRAFFIC = {(4, 10000, 8, "bf16x3"): 3.062e11}
+# DRAM bytes (read + write) of one [a|b] contraction launch, keyed by (L, N, chains, precision).
+# Captured by ncu on a reduced launch of the same kernel (N = 2500 configurations, symmetry chunk
+# of 768, 16 vectors: M = 12288, N = 5000, K = 72832; 4.92e10 B read + written against 5.29e9 B of
+# algorithmic operand and output bytes, 9.3x) and scaled to the full launch by its algorithmic bytes
+# (2.406e10 B x 9.3).
+MEASURED_TRAFFIC = {(4, 10000, 8, "bf16x3"): 2.24e11}
 METRIC = "apply_L/s at 128 atoms N=1e4: mixed+batched vs FP64 GPU at G(w) rel err <=1e-5"
 
 
@@ -833,8 +836,9 @@ def main():
                 "achieved": achieved, "peak": bf16_peak / rate_div, "unit": "TFLOP/s",
                 "frac": achieved / (bf16_peak / rate_div),
                 "traffic": MEASURED_TRAFFIC.get((a.L, a.N, a.chains, a.precision)),
-                "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one [a|b] launch; algorithmic "
-                                f"bytes {(nb * s.n_syms + 2 * a.N) * P * 4 + nb * s.n_syms * 2 * a.N * 4:.3e}",
+                "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a reduced [a|b] launch (M 12288, "
+                                "N 5000, K 72832: 9.3x its algorithmic bytes), scaled to this launch by algorithmic bytes "
+                                f"{(nb * s.n_syms + 2 * a.N) * P * 4 + nb * s.n_syms * 2 * a.N * 4:.3e}",
                 "peak_basis": f"{peak_src} bf16 dense sustained {bf16_peak} TFLOP/s / {rate_div:g} "
                               f"({nprod} product(s){', tf32 at half the bf16 rate' if a.precision.startswith('tf32') else ''})",
                 "algorithmic_flops_per_launch": flops_per_launch, "avg_launch_ms": t_launch * 1e3}

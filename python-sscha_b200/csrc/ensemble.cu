@@ -589,7 +589,9 @@ static int build_chunk_operands(tdscha_ensemble *e, long long c0, long long Nc, 
 // TDSCHA_SYM_UMMA=1 runs the bf16 formats' symmetry transform / fold on the tcgen05 kernels of
 // symmetry_umma.cu instead of the mma.sync kernels of symmetry_tc.cu (read at every call).  Off by
 // default: on the 4x4x4 benchmark the tcgen05 version is correct but slower (96 + 112 ms against
-// 69 + 105 ms per 16-vector step) and less accurate (bf16 instead of tf32 splitting).
+// 69 + 105 ms per 16-vector step) and less accurate (bf16 instead of tf32 splitting); its profile
+// shows one 14-warp CTA per SM waiting on the per-symmetry chain copy -> MMA -> TMEM read-back ->
+// MMA -> store (tensor pipe active 2 %, issue active 13 %).
 static bool sym_umma_enabled() {
     const char *env = getenv("TDSCHA_SYM_UMMA");
     return env && atoi(env) == 1;

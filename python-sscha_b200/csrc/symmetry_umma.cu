@@ -58,7 +58,7 @@ struct Item {
 // shared-memory layout of one work item (bytes from the 1024-aligned base)
 struct Lay {
     int nkb_b, nkb_c, Db, Dc, N1, N2;
-    int A1h, A1l, A2h, A2l, slot, Vh, Vl, B2h, B2l, stg, bars, total;
+    int A1h, A1l, A2h, A2l, slot, Vh, Vl, B2h, B2l, bars, total;
 };
 __host__ __device__ inline Lay layout_of(int db, int dc, int g) {
     Lay L;
@@ -82,9 +82,6 @@ __host__ __device__ inline Lay layout_of(int db, int dc, int g) {
     L.B2h = off; off += L.nkb_b * L.N2 * 32;
     L.B2l = off; off += L.nkb_b * L.N2 * 32;
     off += 128 * 32;              // an A operand's 128 rows read past its last region
-    // drained rows of one vector's T staged as bf16 (row stride kpad(dc) + 2), written back to the
-    // packed rows of B1 by whole warps along nu (coalesced)
-    L.stg = off; off += (L.Db * (kpad(dc) + 2) * 2 + 255) / 256 * 256;
     L.bars = off; off += 256;
     L.total = off + 1024;         // alignment slack
     return L;
@@ -455,49 +452,34 @@ __global__ void __launch_bounds__(THREADS, 1) sym_umma_kernel(const Params p) {
                 for (int s = 0; s < MAXKB; ++s)
                     if (s < L.nkb_c) tmem_ld16_nw(D2 + ((uint32_t)(q * 32) << 16) + (uint32_t)(k * Kc + 16 * s), rr[s]);
                 tmem_wait_ld();
-                if (FOLD) {
 #pragma unroll
-                    for (int s = 0; s < MAXKB; ++s) {
-                        if (s >= L.nkb_c) break;
-                        if (mup >= db) continue;
+                for (int s = 0; s < MAXKB; ++s) {
+                    if (s >= L.nkb_c) break;
+                    float v[16];
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) v[e] = __uint_as_float(rr[s][e]);
+                    if (mup >= db) continue;
+                    const int gm = sb + mup;
+                    if (FOLD) {
                         double *out = p.partD + ((long long)(k0 + k) * p.nf_total + it.fg) * (long long)p.n * p.n +
-                                      (long long)(sb + mup) * p.n + sc;
+                                      (long long)gm * p.n + sc;
 #pragma unroll
                         for (int e = 0; e < 16; ++e)
-                            if (16 * s + e < dc) out[16 * s + e] = (double)__uint_as_float(rr[s][e]);
-                    }
-                } else {
-                    // bf16 hi, then lo: each thread stages its row, then the warp writes its 32 rows
-                    // along nu (consecutive lanes -> consecutive packed pairs)
-                    const long long r = (long long)(k0 + k) * p.nj + (j - p.j0);
-                    const int ldst = Kc + 2;
-                    __nv_bfloat16 *stg = reinterpret_cast<__nv_bfloat16 *>(sm + L.stg);
-                    for (int pass = 0; pass < (p.B1_lo ? 2 : 1); ++pass) {
-                        if (mup < db) {
+                            if (16 * s + e < dc) out[16 * s + e] = (double)v[e];
+                    } else {
+                        const long long r = (long long)(k0 + k) * p.nj + (j - p.j0);
+                        const long long row = r * p.Kp + pair_index(gm, gm, p.n) - gm;   // + gn = pair(gm, gn)
+                        __nv_bfloat16 *hi = static_cast<__nv_bfloat16 *>(p.B1_hi);
+                        __nv_bfloat16 *lo = static_cast<__nv_bfloat16 *>(p.B1_lo);
 #pragma unroll
-                            for (int s = 0; s < MAXKB; ++s) {
-                                if (s >= L.nkb_c) break;
-#pragma unroll
-                                for (int e = 0; e < 16; ++e) {
-                                    const int nu = 16 * s + e;
-                                    if (nu < dc) {
-                                        const float v = __uint_as_float(rr[s][e]);
-                                        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-                                        stg[mup * ldst + nu] = pass == 0 ? h : __float2bfloat16_rn(v - __bfloat162float(h));
-                                    }
-                                }
+                        for (int e = 0; e < 16; ++e) {
+                            const int nu = 16 * s + e, gn = sc + nu;
+                            if (nu < dc && gm <= gn) {
+                                const __nv_bfloat16 h = __float2bfloat16_rn(v[e]);
+                                hi[row + gn] = h;
+                                if (lo) lo[row + gn] = __float2bfloat16_rn(v[e] - __bfloat162float(h));
                             }
                         }
-                        __syncwarp();
-                        __nv_bfloat16 *dst = static_cast<__nv_bfloat16 *>(pass == 0 ? p.B1_hi : p.B1_lo);
-                        for (int m = 0; m < 32; ++m) {
-                            const int mu = q * 32 + m;
-                            if (mu >= db) break;
-                            const int gm = sb + mu;
-                            const long long row = r * p.Kp + pair_index(gm, gm, p.n) - gm + sc;   // + nu: pair(gm, sc + nu)
-                            for (int nu = (b == c ? mu : 0) + lane; nu < dc; nu += 32) dst[row + nu] = stg[mu * ldst + nu];
-                        }
-                        __syncwarp();
                     }
                 }
             }
