@@ -406,7 +406,7 @@ def batch_chains(base):
 
 def run_batch_systems(a):
     """Throughput of 48 chains (16 per system) over three uneven systems advanced together by
-    tdscha_lanczos_run_device (one CUDA graph launch per step after two eager steps), against the
+    tdscha_lanczos_run_device (two eager steps, then one CUDA graph holding all remaining steps), against the
     host-driven per-system loop; G(w) error of the mixed chains against FP64 on the two small
     systems."""
     import torch
@@ -475,7 +475,7 @@ def run_batch_systems(a):
             "higher_is_better": True, "dtype": f"{prec} contractions (f32 accumulate) + f64 recurrence",
             "data": "synthetic (seeded rock-salt ensembles, T = 300 K)",
             "config": {"workload": "16 chains (3 IR, 6 Raman, 7 random R1) on each of " + "; ".join(names),
-                       "graph": "2 eager steps, then one CUDA graph launch per step for all systems",
+                       "graph": "2 eager steps, then one CUDA graph launch holding every remaining step of all systems",
                        "streams": "one per system, forked from and joined into the run's stream"},
             "chain_lengths": lengths, "comparison_20_steps": cmp, "accuracy_vs_fp64": acc, "clocks": clocks}
     print(json.dumps(line))

@@ -203,8 +203,8 @@ int tdscha_apply_static_L_device(tdscha_ensemble *ens, int nb, const double *psi
  *   coef  device (n_steps, nc, 4): [a_k, b_k, c_k, s_norm_{k+1}] of every step (out)
  * Each step is one batched apply of the 2 nc vectors [q; p] (transpose 0 for q, 1 for p), one
  * batched recurrence and the history update.  Systems run on their own streams forked from and
- * joined into `stream`.  With use_graph != 0 the first two steps run eagerly and one step of all
- * systems is captured into a CUDA graph launched once per remaining step.  A chain whose |b| or
+ * joined into `stream`.  With use_graph != 0 the first two steps run eagerly and every remaining
+ * step of all systems is captured into one CUDA graph, launched once.  A chain whose |b| or
  * |c| falls below 1e-12 ends there as in run_FT (:6129-6141): its last coef row is that step's,
  * later rows are left untouched, its qp and sc stay at that step (its vectors still go through
  * the batched apply, whose other chains are unaffected).  Returns after the last step completed.

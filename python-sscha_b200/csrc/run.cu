@@ -9,11 +9,12 @@
 // Systems run on their own streams, forked from and joined back into the caller's stream, so the
 // small systems' kernels fill the SMs the large system's contraction leaves idle.  With use_graph
 // the first two steps run eagerly (they tune the contraction tiles, allocate the workspaces and fix
-// the chunking plans) and one step of all systems is captured into a CUDA graph that is launched
-// once per remaining step: per step the host issues one graph launch, nothing else.
+// the chunking plans) and all remaining steps of all systems are captured into one CUDA graph that
+// is launched once: the rest of the run is a single launch from the host.
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <mutex>
 #include <vector>
 
@@ -240,23 +241,45 @@ int lanczos_run_device(int ns, const tdscha_run_system *sys, int n_steps, int us
     for (int k = 0; k < eager; ++k) TD_TRY(enqueue_step(ns, sys, rs, n_steps, st));
     if (eager < n_steps) {
         TD_TRY(check_err_words(ns, sys, st));   // also completes the eager steps
-        cudaGraph_t graph = nullptr;
-        cudaGraphExec_t exec = nullptr;
-        TD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
-        const int rc = enqueue_step(ns, sys, rs, n_steps, st);
-        const cudaError_t ec = cudaStreamEndCapture(st, &graph);
-        if (rc != 0) {
-            if (graph) cudaGraphDestroy(graph);
-            return rc;
+        // the remaining steps go into as few graphs as possible: `per` consecutive steps of all
+        // systems are captured into one graph (TDSCHA_RUN_GRAPH_STEPS caps it; by default all
+        // remaining steps, i.e. a single graph launch for the rest of the run), and a shorter graph
+        // takes the remainder
+        const int rem = n_steps - eager;
+        const char *env = getenv("TDSCHA_RUN_GRAPH_STEPS");
+        const int cap_steps = env && atoi(env) > 0 ? atoi(env) : rem;
+        const int per = std::min(rem, cap_steps);
+        auto build = [&](int steps, cudaGraphExec_t *exec) -> int {
+            cudaGraph_t graph = nullptr;
+            TD_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+            int rc = 0;
+            for (int k = 0; k < steps && rc == 0; ++k) rc = enqueue_step(ns, sys, rs, n_steps, st);
+            const cudaError_t ec = cudaStreamEndCapture(st, &graph);
+            if (rc != 0) {
+                if (graph) cudaGraphDestroy(graph);
+                return rc;
+            }
+            TD_CHECK(ec == cudaSuccess && graph, TDSCHA_ECUDA, "graph capture of run steps failed: %s", cudaGetErrorString(ec));
+            const cudaError_t ei = cudaGraphInstantiate(exec, graph, 0);
+            cudaGraphDestroy(graph);
+            TD_CHECK(ei == cudaSuccess, TDSCHA_ECUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ei));
+            return 0;
+        };
+        cudaGraphExec_t full = nullptr, tail = nullptr;
+        TD_TRY(build(per, &full));
+        if (rem % per) {
+            const int rc = build(rem % per, &tail);
+            if (rc != 0) {
+                cudaGraphExecDestroy(full);
+                return rc;
+            }
         }
-        TD_CHECK(ec == cudaSuccess && graph, TDSCHA_ECUDA, "graph capture of a run step failed: %s", cudaGetErrorString(ec));
-        const cudaError_t ei = cudaGraphInstantiate(&exec, graph, 0);
-        cudaGraphDestroy(graph);
-        TD_CHECK(ei == cudaSuccess, TDSCHA_ECUDA, "cudaGraphInstantiate failed: %s", cudaGetErrorString(ei));
         cudaError_t el = cudaSuccess;
-        for (int k = eager; k < n_steps && el == cudaSuccess; ++k) el = cudaGraphLaunch(exec, st);
+        for (int k = 0; k + per <= rem && el == cudaSuccess; k += per) el = cudaGraphLaunch(full, st);
+        if (tail && el == cudaSuccess) el = cudaGraphLaunch(tail, st);
         const cudaError_t es = cudaStreamSynchronize(st);
-        cudaGraphExecDestroy(exec);
+        cudaGraphExecDestroy(full);
+        if (tail) cudaGraphExecDestroy(tail);
         TD_CHECK(el == cudaSuccess && es == cudaSuccess, TDSCHA_ECUDA, "graph launch failed: %s",
                  cudaGetErrorString(el != cudaSuccess ? el : es));
     }

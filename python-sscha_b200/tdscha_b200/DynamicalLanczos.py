@@ -1180,8 +1180,8 @@ def run_FT_multi(groups, n_iter, precision=None, use_graph=True):
     to the host (tdscha_lanczos_run_device): ``groups`` has one entry per system, a list of at most
     32 Lanczos objects sharing that system's initialised device ensemble.  Every step is one batched
     apply per system (all its chains' L q and L^T p), one batched recurrence and the history update;
-    systems run on their own streams and, with use_graph, one step of all systems is a single CUDA
-    graph launch after two eager steps.
+    systems run on their own streams and, with use_graph, all steps after the first two are one CUDA
+    graph launch.
 
     Afterwards every chain holds its coefficients up to its first breakdown (|b| or |c| < 1e-12, where
     run_FT stops, DynamicalLanczos.py:6129-6141) and psi = its last q.  Unlike run_FT the basis is not
