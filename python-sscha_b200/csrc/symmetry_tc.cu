@@ -21,6 +21,7 @@
 //     shared array has leading dimension ld = 4 (mod 8) floats, which makes the ldmatrix row
 //     addresses and the transposed fragment stores free of bank conflicts.
 #include <algorithm>
+#include <cstdlib>
 #include <cstdint>
 #include <cuda_bf16.h>
 
@@ -258,6 +259,80 @@ transform_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restr
     }
 }
 
+// The same transform with a quarter of the shared memory (four arrays instead of eight), so that two
+// CTAs share an SM and hide each other's per-symmetry latency: the Ys block and the intermediate
+// product are kept as fp32 and split into tf32 hi / lo as they are loaded into fragments (the same
+// values as the pre-split arrays, so the results are bit-identical), and the two symmetry tables
+// have one buffer (the copy of symmetry j + 1 is issued after symmetry j is stored).
+template <int MT>
+__global__ void __launch_bounds__(threads_for(MT), 2)
+transform_tc_lean_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__ pc, int nj, int j0, int JT,
+                         const double *__restrict__ Ys, const double *__restrict__ R1, const double *__restrict__ ups,
+                         long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo, void *r1_hi, void *r1_lo) {
+    using S = TcShape<MT>;
+    constexpr int LD = S::LD, ARR = S::ARR, NW = S::NW;
+    extern __shared__ __align__(16) float smf[];
+    float *Yr = smf;                       // Ys_k[b, c] (mu, nu), fp32
+    float *MTr = smf + ARR;                // M1^T (nu', mu'), fp32
+    float *STb = smf + 2 * ARR, *STc = smf + 3 * ARR;   // S_b^T (mu, p), S_c^T (nu', nu) of the symmetry
+    const int b = pb[blockIdx.x], c = pc[blockIdx.x];
+    const int k = blockIdx.z;
+    const int ja = j0 + blockIdx.y * JT, jb = min(ja + JT, j0 + nj);
+    const int n = tb.n;
+    const int sb = tb.start[b], db = tb.dim[b], sc = tb.start[c], dc = tb.dim[c];
+    const int DB = (db + 15) & ~15, DB8 = (db + 7) & ~7, DC = (dc + 7) & ~7;
+    const int dpb = (db + 3) & ~3, dpc = (dc + 3) & ~3;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float *Tb_base = tb.symPT + tb.offP[b], *Tc_base = tb.symPT + tb.offP[c];
+    const double *Yg = Ys + (long long)k * n * n;
+    for (int mu = warp; mu < DB; mu += NW)
+        for (int nu = lane; nu < DC; nu += 32)
+            Yr[mu * LD + nu] = (mu < db && nu < dc) ? (float)Yg[(long long)(sb + mu) * n + sc + nu] : 0.f;
+    const int mt = DB / 16, nt = DC / 8, tiles = mt * nt;
+    for (int j = ja; j < jb; ++j) {
+        const long long r = (long long)k * nj + (j - j0);
+        copy_table<LD, S::THREADS>(STb, Tb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
+        copy_table<LD, S::THREADS>(STc, Tc_base + (long long)j * dpc * dpc, dpc, DC, DC);
+        cp_async_commit();
+        cp_async_wait<0>();
+        __syncthreads();
+        for (int ti = warp; ti < tiles; ti += NW) {
+            const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            warp_tile<LD, false, false>(acc, Yr, nullptr, STc, nullptr, m0, n0, DC / 8);
+            const int g = lane >> 2, t = lane & 3;
+#pragma unroll
+            for (int e = 0; e < 4; ++e) MTr[(n0 + 2 * t + (e & 1)) * LD + m0 + g + 8 * (e >> 1)] = acc[e];
+        }
+        if (b == c && (int)threadIdx.x < db) {   // r1 for the modes of block b: ups o (S_b^T R)
+            const double *Rk = R1 + (long long)k * n + sb;
+            double s = 0.0;
+            for (int p = 0; p < db; ++p) s += (double)STb[threadIdx.x * LD + p] * Rk[p];
+            store_split(fmt, r1_hi, r1_lo, r * np + sb + threadIdx.x, ups[sb + threadIdx.x] * s);
+        }
+        __syncthreads();             // M1 complete; S_c of this symmetry no longer needed
+        float *T = STc;              // step-2 result staged where S_c^T was
+        for (int ti = warp; ti < tiles; ti += NW) {
+            const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            warp_tile<LD, false, false>(acc, STb, nullptr, MTr, nullptr, m0, n0, DB8 / 8);
+            const int g = lane >> 2, t = lane & 3;
+            *reinterpret_cast<float2 *>(&T[(m0 + g) * LD + n0 + 2 * t]) = make_float2(acc[0], acc[1]);
+            *reinterpret_cast<float2 *>(&T[(m0 + g + 8) * LD + n0 + 2 * t]) = make_float2(acc[2], acc[3]);
+        }
+        __syncthreads();
+        for (int mu = warp; mu < db; mu += NW) {
+            const int gm = sb + mu;
+            const long long row = r * Kp + pair_index(gm, gm, n) - gm;   // + gn gives pair(gm, gn)
+            for (int nu = lane; nu < dc; nu += 32) {
+                const int gn = sc + nu;
+                if (gm <= gn) store_split_f(fmt, B1_hi, B1_lo, row + gn, T[mu * LD + nu]);
+            }
+        }
+        __syncthreads();             // the tables' buffers are free for the next symmetry's copy
+    }
+}
+
 // ---- fold ---------------------------------------------------------------------------------------------
 // grid (pairs of the class, fold chunks of Jf symmetries, nb).  Per symmetry:
 //   W  (d_b x d_c) = ups_mu ups_nu (2 on the diagonal) Z[r, pair(mu, nu)]
@@ -368,6 +443,103 @@ fold_tc_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__
     if (b == c && (int)threadIdx.x < db) partF[((long long)k * nf_total + fg) * n + sb + threadIdx.x] = facc;
 }
 
+// The fold with four shared arrays (U^T as fp32 split into tf32 hi / lo on load, one buffer of the
+// symmetry's S_b, S_c and W) and at most 256 threads, so that two CTAs share an SM: bit-identical to
+// fold_tc_kernel (same split values, same product order, same fp64 sums).
+__host__ __device__ constexpr int lean_fold_threads(int MT) { return threads_for(MT) < 256 ? threads_for(MT) : 256; }
+
+template <int MT>
+__global__ void __launch_bounds__(lean_fold_threads(MT), 2)
+fold_tc_lean_kernel(SymTables tb, const int *__restrict__ pb, const int *__restrict__ pc, const float *__restrict__ Z,
+                    long long ldz, const float *__restrict__ F, long long ldf, const double *__restrict__ ups, int nj, int j0,
+                    int Jf, int nf_total, double *__restrict__ partD, double *__restrict__ partF) {
+    using S = TcShape<MT>;
+    constexpr int LD = S::LD, ARR = S::ARR;
+    constexpr int THREADS = lean_fold_threads(MT), NW = THREADS / 32;
+    constexpr int TPW = ((S::DM / 16) * (S::DM / 8) + NW - 1) / NW;
+    extern __shared__ __align__(16) float smf[];
+    float *UTr = smf;                                       // U^T (nu', mu'), fp32
+    float *SNb = smf + ARR, *SNc = smf + 2 * ARR, *W = smf + 3 * ARR;
+    const int b = pb[blockIdx.x], c = pc[blockIdx.x];
+    const int fc = blockIdx.y, k = blockIdx.z;
+    const int n = tb.n;
+    const int sb = tb.start[b], db = tb.dim[b], sc = tb.start[c], dc = tb.dim[c];
+    const int DB = (db + 15) & ~15, DB8 = (db + 7) & ~7, DC = (dc + 7) & ~7;
+    const int dpb = (db + 3) & ~3, dpc = (dc + 3) & ~3;
+    const int fg = j0 / Jf + fc;
+    const int ja = j0 + fc * Jf, jb = min(j0 + (fc + 1) * Jf, j0 + nj);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+    const int mt = DB / 16, nt = DC / 8, tiles = mt * nt;
+    const float *Pb_base = tb.symP + tb.offP[b], *Pc_base = tb.symP + tb.offP[c];
+    double accD[TPW][4];
+#pragma unroll
+    for (int i = 0; i < TPW; ++i)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) accD[i][e] = 0.0;
+    double facc = 0.0;
+    for (int j = ja; j < jb; ++j) {
+        const long long r = (long long)k * nj + (j - j0);
+        copy_table<LD, THREADS>(SNb, Pb_base + (long long)j * dpb * dpb, dpb, DB, DB8);
+        copy_table<LD, THREADS>(SNc, Pc_base + (long long)j * dpc * dpc, dpc, DC, DC);
+        const float *Zr = Z + r * ldz;
+        for (int mu = warp; mu < DB; mu += NW)
+            for (int nu = lane; nu < DC; nu += 32) {
+                const bool v = mu < db && nu < dc;
+                int gm = sb + mu, gn = sc + nu;
+                if (gm > gn) { const int s2 = gm; gm = gn; gn = s2; }
+                cp_async4(&W[mu * LD + nu], v ? Zr + pair_index(gm, gn, n) : Zr, v);
+            }
+        cp_async_commit();
+        cp_async_wait<0>();
+        // W = ups_mu ups_nu (2 on the diagonal) Z: each thread scales the elements it copied itself
+        for (int mu = warp; mu < db; mu += NW)
+            for (int nu = lane; nu < dc; nu += 32) {
+                const int gm = sb + mu, gn = sc + nu;
+                W[mu * LD + nu] *= (float)((gm == gn ? 2.0 : 1.0) * ups[gm] * ups[gn]);
+            }
+        __syncthreads();
+        for (int ti = warp; ti < tiles; ti += NW) {
+            const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
+            float acc[4] = {0.f, 0.f, 0.f, 0.f};
+            warp_tile<LD, false, false>(acc, W, nullptr, SNc, nullptr, m0, n0, DC / 8);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) UTr[(n0 + 2 * t + (e & 1)) * LD + m0 + g + 8 * (e >> 1)] = acc[e];
+        }
+        if (b == c && (int)threadIdx.x < db) {
+            const float *Fr = F + r * ldf + sb;
+            double sum = 0.0;
+            for (int p = 0; p < db; ++p) sum += (double)SNb[threadIdx.x * LD + p] * (double)Fr[p];
+            facc += sum;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < TPW; ++i) {
+            const int ti = warp + i * NW;
+            if (ti < tiles) {
+                const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
+                float acc[4] = {0.f, 0.f, 0.f, 0.f};
+                warp_tile<LD, false, false>(acc, SNb, nullptr, UTr, nullptr, m0, n0, DB8 / 8);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) accD[i][e] += (double)acc[e];
+            }
+        }
+        __syncthreads();   // U^T and this symmetry's buffers free
+    }
+    double *out = partD + ((long long)k * nf_total + fg) * (long long)n * n;
+#pragma unroll
+    for (int i = 0; i < TPW; ++i) {
+        const int ti = warp + i * NW;
+        if (ti >= tiles) continue;
+        const int m0 = (ti / nt) * 16, n0 = (ti % nt) * 8;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int mu = m0 + g + 8 * (e >> 1), nu = n0 + 2 * t + (e & 1);
+            if (mu < db && nu < dc) out[(long long)(sb + mu) * n + sc + nu] = accD[i][e];
+        }
+    }
+    if (b == c && (int)threadIdx.x < db) partF[((long long)k * nf_total + fg) * n + sb + threadIdx.x] = facc;
+}
+
 template <int MT>
 int launch_transform_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, const double *Ys, const double *R1,
                         const double *ups, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo, void *r1_hi,
@@ -376,10 +548,14 @@ int launch_transform_tc(const SymTables &t, const PairClasses &pc, int nb, int n
     using S = TcShape<MT>;
     static_assert(S::SMEM <= 227 * 1024, "shared memory");
     constexpr int JT = 16;
-    auto kern = transform_tc_kernel<MT>;
-    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
+    // the lean kernel (half the shared memory: two CTAs per SM) unless TDSCHA_SYM_LEAN=0
+    const char *env = getenv("TDSCHA_SYM_LEAN");
+    const bool lean = !(env && atoi(env) == 0);
+    auto kern = lean ? transform_tc_lean_kernel<MT> : transform_tc_kernel<MT>;
+    const size_t smem = lean ? S::SMEM / 2 : S::SMEM;
+    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, JT), (unsigned)nb);
-    kern<<<grid, S::THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], nj, j0, JT, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
+    kern<<<grid, S::THREADS, smem, st>>>(t, pc.b[MT], pc.c[MT], nj, j0, JT, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo);
     TD_CUDA(cudaGetLastError());
     return 0;
 }
@@ -390,10 +566,15 @@ int launch_fold_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, in
     if (!pc.count[MT]) return 0;
     using S = TcShape<MT>;
     static_assert(S::SMEM <= 227 * 1024, "shared memory");
-    auto kern = fold_tc_kernel<MT>;
-    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SMEM));
+    // the lean kernel (half the shared memory, two CTAs per SM) unless TDSCHA_SYM_LEAN=0
+    const char *env = getenv("TDSCHA_SYM_LEAN");
+    const bool lean = !(env && atoi(env) == 0);
+    auto kern = lean ? fold_tc_lean_kernel<MT> : fold_tc_kernel<MT>;
+    const size_t smem = lean ? S::SMEM / 2 : S::SMEM;
+    const int threads = lean ? lean_fold_threads(MT) : S::THREADS;
+    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     dim3 grid((unsigned)pc.count[MT], (unsigned)ceil_div(nj, Jf), (unsigned)nb);
-    kern<<<grid, S::THREADS, S::SMEM, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
+    kern<<<grid, threads, smem, st>>>(t, pc.b[MT], pc.c[MT], Z, ldz, F, ldf, ups, nj, j0, Jf, nf_total, partD, partF);
     TD_CUDA(cudaGetLastError());
     return 0;
 }

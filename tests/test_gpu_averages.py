@@ -121,3 +121,18 @@ def test_tcgen05_symmetry_kernels_match(request, cuda, fixture, monkeypatch):
         assert _rel(f1, f0) < 1e-4 and _rel(d1, d0) < 1e-4
     monkeypatch.delenv("TDSCHA_SYM_UMMA", raising=False)
     ens.close()
+
+
+@pytest.mark.parametrize("precision", ["bf16x3", "tf32x3"])
+def test_lean_symmetry_kernels_are_bit_identical(cuda, rocksalt_l2, precision, monkeypatch):
+    """The half-shared-memory symmetry transform and fold (default) and the double-buffered ones
+    (TDSCHA_SYM_LEAN=0) form the same tf32 hi / lo values and the same products: identical averages."""
+    d = rocksalt_l2
+    ens = _dev_ens(d)
+    for case in ("case0", "case2"):
+        monkeypatch.setenv("TDSCHA_SYM_LEAN", "0")
+        f0, d0 = ens.perturb_average(d[f"{case}_R1"], d[f"{case}_Y1"], int(d[f"{case}_d4"]), precision)
+        monkeypatch.delenv("TDSCHA_SYM_LEAN")
+        f1, d1 = ens.perturb_average(d[f"{case}_R1"], d[f"{case}_Y1"], int(d[f"{case}_d4"]), precision)
+        assert np.array_equal(f0, f1) and np.array_equal(d0, d1)
+    ens.close()
