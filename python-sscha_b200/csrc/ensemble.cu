@@ -698,12 +698,17 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         t.err = e->d_err;
     }
 
+    // kernels per transform / fold stage: one per non-empty block-pair class (+ the padding kernel of
+    // the transform), or the tcgen05 kernel and its vector-part kernel
+    int n_classes = 0;
+    for (int m = 1; m <= SYM_MT_MAX; ++m) n_classes += e->pairs.count[m] > 0 ? 1 : 0;
+    const int transform_launches = t.umma ? 3 : n_classes + 1, fold_launches = t.umma ? 2 : n_classes;
     for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
         const int nj = std::min(Jc, e->N_sym - j0);
         const long long M = (long long)nb * nj;
         // rows r = k * nj + jj
         {
-            StageScope sc(e, ST_TRANSFORM, st);
+            StageScope sc(e, ST_TRANSFORM, st, transform_launches);
             TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo,
                                  fmt != FMT_F64, st));
         }
@@ -752,7 +757,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         }
         // fold this chunk into the partials
         {
-            StageScope sc(e, ST_FOLD, st);
+            StageScope sc(e, ST_FOLD, st, fold_launches);
             if (fmt == FMT_F64)
                 TD_TRY(sym_fold<double>(t, e->pairs, e->d_blocks_ids, nb, nj, j0, Jf, nf_total, (const double *)Z, L.ldz,
                                         (const double *)F, L.ldf, e->ups, partD, partF, false, st));
