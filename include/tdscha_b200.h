@@ -80,6 +80,33 @@ int tdscha_ensemble_destroy(tdscha_ensemble *ens);
 int tdscha_ensemble_info(const tdscha_ensemble *ens, int *n, int *N, int *N_sym, int *n_blocks,
                          double *T, double *N_eff);
 
+/*
+ * Factorised symmetry path of a resident ensemble.  When the symmetry group has a subgroup K (the
+ * kernel of its representation on one degenerate block: the lattice translations of a supercell)
+ * whose matrices an orthogonal change of basis inside every degenerate block brings to 1 x 1 / 2 x 2
+ * blocks, the ensemble is stored in that basis (inputs and outputs of the averages and of their VJP
+ * stay in the given basis) and the mixed-precision averages run their dense symmetry transform /
+ * fold over the cosets of K only.  rotated: 1 when the basis is rotated; n_cosets, coset_size: the
+ * factorisation (0 when the general path is used); offpattern: the largest matrix entry outside the
+ * 2 x 2 pattern over the whole group (at most 1e-7 for the factorised path).
+ * TDSCHA_SYM_COSETS=0 in the environment at creation keeps the given basis and the general path.
+ * Any pointer may be NULL.
+ */
+int tdscha_ensemble_cosets(const tdscha_ensemble *ens, int *rotated, int *n_cosets, int *coset_size,
+                           double *offpattern);
+
+/*
+ * The analysis behind it, on host arrays (no device): sym_blocks as for tdscha_ensemble_create.
+ * Outputs n_cosets, coset_size (0 when the group has no such structure; tdscha_last_error says
+ * why) and, when non-NULL: order (N_sym) the symmetries coset by coset, partner (n) the partner of
+ * each rotated mode (itself for a real character), R (sum of n_deg[b]^2) the rotation of every block,
+ * R_b[q'][q] = component q' of rotated mode q, row-major; offpattern the largest entry of
+ * R^T S_t R outside the pattern over the subgroup's matrices.
+ */
+int tdscha_symmetry_cosets(int N_sym, int n_blocks, const int *n_deg, const double *const *sym_blocks,
+                           int *n_cosets, int *coset_size, int *order, int *partner, double *R,
+                           double *offpattern);
+
 /* Device bytes the ensemble holds now (operands of every precision built so far included). */
 int tdscha_ensemble_device_bytes(const tdscha_ensemble *ens, long long *bytes);
 

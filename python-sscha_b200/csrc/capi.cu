@@ -92,6 +92,36 @@ int tdscha_ensemble_info(const tdscha_ensemble *e, int *n, int *N, int *N_sym, i
     return 0;
 }
 
+int tdscha_ensemble_cosets(const tdscha_ensemble *e, int *rotated, int *n_cosets, int *coset_size, double *offpattern) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    if (rotated) *rotated = e->Rrow != nullptr;
+    if (n_cosets) *n_cosets = e->cosets ? e->cosets->n_cos : 0;
+    if (coset_size) *coset_size = e->cosets ? e->cosets->sub : 0;
+    if (offpattern) *offpattern = e->cosets ? e->cosets->offpattern : 0.0;
+    return 0;
+}
+
+int tdscha_symmetry_cosets(int N_sym, int n_blocks, const int *n_deg, const double *const *sym_blocks, int *n_cosets,
+                           int *coset_size, int *order, int *partner, double *R, double *offpattern) {
+    clear_error();
+    TD_CHECK(N_sym > 0 && n_blocks > 0 && n_deg && sym_blocks && n_cosets && coset_size, TDSCHA_EINVAL, "bad arguments");
+    std::vector<int> dim(n_deg, n_deg + n_blocks);
+    for (int b = 0; b < n_blocks; ++b) TD_CHECK(dim[b] > 0 && sym_blocks[b], TDSCHA_EINVAL, "block %d empty", b);
+    CosetAnalysis ca;
+    TD_TRY(analyse_cosets(N_sym, dim, sym_blocks, ca));
+    *n_cosets = ca.ok ? ca.n_cos : 0;
+    *coset_size = ca.ok ? ca.sub : 0;
+    if (!ca.ok) {
+        set_error("%s", ca.why.c_str());
+        return 0;
+    }
+    if (order) std::memcpy(order, ca.order.data(), ca.order.size() * sizeof(int));
+    if (partner) std::memcpy(partner, ca.partner.data(), ca.partner.size() * sizeof(int));
+    if (R) std::memcpy(R, ca.R.data(), ca.R.size() * sizeof(double));
+    if (offpattern) *offpattern = ca.offpattern;
+    return 0;
+}
+
 int tdscha_ensemble_device_bytes(const tdscha_ensemble *e, long long *bytes) {
     TD_CHECK(e != nullptr && bytes != nullptr, TDSCHA_EINVAL, "NULL argument");
     size_t b = e->base_bytes + e->ws.bytes;

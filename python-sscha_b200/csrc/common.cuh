@@ -42,8 +42,9 @@ constexpr double RY_TO_K = 157887.32400374097;  // CModules/LanczosFunctions.h:9
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 inline long long round_up(long long a, long long b) { return (a + b - 1) / b * b; }
 
-// Operand storage formats of the tensor-core contractions.
-enum Format : int { FMT_F64 = 0, FMT_BF16 = 1, FMT_TF32 = 2 };
+// Operand storage formats of the tensor-core contractions (FMT_F32: plain fp32, for intermediate
+// products that are not contraction operands).
+enum Format : int { FMT_F64 = 0, FMT_BF16 = 1, FMT_TF32 = 2, FMT_F32 = 3 };
 
 inline Format format_of(int precision) {
     switch (precision) {
@@ -78,6 +79,8 @@ __device__ __forceinline__ float tf32_round(float f) {
 __device__ __forceinline__ void store_split(Format fmt, void *hi, void *lo, long long idx, double x) {
     if (fmt == FMT_F64) {
         static_cast<double *>(hi)[idx] = x;
+    } else if (fmt == FMT_F32) {
+        static_cast<float *>(hi)[idx] = (float)x;
     } else if (fmt == FMT_BF16) {
         uint16_t h = bf16_bits_rn((float)x);
         static_cast<uint16_t *>(hi)[idx] = h;
@@ -89,6 +92,6 @@ __device__ __forceinline__ void store_split(Format fmt, void *hi, void *lo, long
     }
 }
 
-inline size_t format_bytes(Format f) { return f == FMT_F64 ? 8 : (f == FMT_BF16 ? 2 : 4); }
+inline size_t format_bytes(Format f) { return f == FMT_F64 ? 8 : (f == FMT_BF16 ? 2 : 4); }   // FMT_F32: 4
 
 }  // namespace tdscha

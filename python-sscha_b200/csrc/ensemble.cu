@@ -250,6 +250,108 @@ int symmetrize_device(int nb, int n, const double *Y, double *Ys, cudaStream_t s
     return 0;
 }
 
+static void free_cosets(SymCosets *c) {
+    if (!c) return;
+    void *ps[] = {c->order, c->partner, c->c0, c->c1, c->repP, c->repPT, c->d_offRep};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    delete c;
+}
+
+// TDSCHA_SYM_COSETS=0 keeps the ensemble in the given basis and the averages on the general
+// symmetry kernels (read when an ensemble is created, and again by every averages call).
+static bool cosets_enabled() {
+    const char *env = getenv("TDSCHA_SYM_COSETS");
+    return !(env && atoi(env) == 0);
+}
+
+// Rotated basis and factorised symmetry path (cosets.cuh) when the symmetry group has the structure;
+// on the legacy stream, before the fp32 tables, G and X~ are derived from X, Y and the tables.
+static int setup_cosets(tdscha_ensemble *e, const std::vector<int> &dim, const double *const *sym_blocks) {
+    CosetAnalysis ca;
+    TD_TRY(analyse_cosets(e->N_sym, dim, sym_blocks, ca));
+    if (!ca.ok) return 0;
+    const int n = e->n, dmax = e->dmax, nblk = e->n_blocks;
+    std::vector<double> Rrow((size_t)n * dmax, 0.0);
+    for (int b = 0; b < nblk; ++b)
+        for (int q = 0; q < dim[b]; ++q)
+            for (int r = 0; r < dim[b]; ++r)
+                Rrow[(size_t)(e->blk_start[b] + q) * dmax + r] = ca.R[ca.R_off[b] + (size_t)q * dim[b] + r];
+    double *Rblk = nullptr;
+    TD_CUDA(cudaMalloc(&e->Rrow, Rrow.size() * sizeof(double)));
+    TD_CUDA(cudaMemcpy(e->Rrow, Rrow.data(), Rrow.size() * sizeof(double), cudaMemcpyHostToDevice));
+    TD_CUDA(cudaMalloc(&Rblk, ca.R.size() * sizeof(double)));
+    TD_CUDA(cudaMemcpy(Rblk, ca.R.data(), ca.R.size() * sizeof(double), cudaMemcpyHostToDevice));
+    // X, Y into the rotated basis (G is free scratch until it is derived from Y)
+    TD_TRY(rotate_rows_of(e->N, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, e->X, e->G, true, 0));
+    std::swap(e->X, e->G);
+    TD_TRY(rotate_rows_of(e->N, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, e->Y, e->G, true, 0));
+    std::swap(e->Y, e->G);
+    for (int b = 0; b < nblk; ++b)
+        TD_TRY(rotate_sym_tables(e->sym + e->blk_sym_off[b], e->N_sym, dim[b], Rblk + ca.R_off[b], 0));
+    TD_CUDA(cudaDeviceSynchronize());
+    cudaFree(Rblk);
+    // coefficients of every symmetry, checked against the 2 x 2 pattern over the whole group
+    auto *c = new SymCosets();
+    c->n_cos = ca.n_cos;
+    c->sub = ca.sub;
+    auto fail = [&](int rc) { free_cosets(c); return rc; };
+    unsigned long long *offmax = nullptr;
+    const size_t cb = (size_t)e->N_sym * n * sizeof(float);
+    if (cudaMalloc(&c->order, e->N_sym * sizeof(int)) != cudaSuccess || cudaMalloc(&c->partner, n * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->c0, cb) != cudaSuccess || cudaMalloc(&c->c1, cb) != cudaSuccess ||
+        cudaMalloc(&offmax, sizeof(unsigned long long)) != cudaSuccess) {
+        if (offmax) cudaFree(offmax);
+        set_error("allocation of the symmetry cosets failed");
+        return fail(TDSCHA_ENOMEM);
+    }
+    cudaMemcpy(c->order, ca.order.data(), e->N_sym * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->partner, ca.partner.data(), n * sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemset(offmax, 0, sizeof(unsigned long long));
+    int rc = coset_coefficients(e->N_sym, n, ca.sub, c->order, c->partner, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, e->sym,
+                                e->d_blk_sym_off, c->c0, c->c1, offmax, 0);
+    unsigned long long bits = 0;
+    if (!rc && cudaMemcpy(&bits, offmax, sizeof(bits), cudaMemcpyDeviceToHost) != cudaSuccess) rc = TDSCHA_ECUDA;
+    cudaFree(offmax);
+    if (rc) return fail(rc);
+    std::memcpy(&c->offpattern, &bits, sizeof(double));
+    if (!(c->offpattern <= 1e-7)) { free_cosets(c); return 0; }   // not a factorisation to working accuracy
+    // the representatives' tables in the padded fp32 layouts of the tensor-core kernels
+    std::vector<long long> offR(nblk);
+    long long tot = 0, totd = 0;
+    for (int b = 0; b < nblk; ++b) {
+        const long long dp = (dim[b] + 3) & ~3;
+        offR[b] = tot;
+        tot += (long long)ca.n_cos * dp * dp;
+        totd = std::max<long long>(totd, (long long)ca.n_cos * dim[b] * dim[b]);
+    }
+    double *reps = nullptr;
+    if (cudaMalloc(&c->repP, tot * sizeof(float)) != cudaSuccess || cudaMalloc(&c->repPT, tot * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&c->d_offRep, nblk * sizeof(long long)) != cudaSuccess || cudaMalloc(&reps, totd * sizeof(double)) != cudaSuccess) {
+        if (reps) cudaFree(reps);
+        set_error("allocation of the coset tables failed");
+        return fail(TDSCHA_ENOMEM);
+    }
+    cudaMemcpy(c->d_offRep, offR.data(), nblk * sizeof(long long), cudaMemcpyHostToDevice);
+    for (int b = 0; b < nblk; ++b) {
+        const size_t blk = (size_t)dim[b] * dim[b];
+        for (int p = 0; p < ca.n_cos; ++p)
+            cudaMemcpy(reps + p * blk, e->sym + e->blk_sym_off[b] + (size_t)ca.order[(size_t)p * ca.sub] * blk, blk * sizeof(double),
+                       cudaMemcpyDeviceToDevice);
+        const long long dp = (dim[b] + 3) & ~3;
+        pad_sym_kernel<<<grid_for((long long)ca.n_cos * dp * dp), 256>>>(reps, ca.n_cos, dim[b], (int)dp, c->repP + offR[b],
+                                                                         c->repPT + offR[b]);
+        if (cudaDeviceSynchronize() != cudaSuccess) {
+            cudaFree(reps);
+            set_error("coset tables: %s", cudaGetErrorString(cudaGetLastError()));
+            return fail(TDSCHA_ECUDA);
+        }
+    }
+    cudaFree(reps);
+    e->cosets = c;
+    return 0;
+}
+
 int ensemble_create(const double *X, const double *Y, const double *w, const double *rho, int N, int n, double T,
                     int N_sym, int n_blocks, const int *n_deg, const int *const *deg_space,
                     const double *const *sym_blocks, const int *blocks_ids, tdscha_ensemble **out) {
@@ -366,6 +468,10 @@ int ensemble_create(const double *X, const double *Y, const double *w, const dou
     TD_UP(e->d_pair_nu, pnu.data(), e->P * sizeof(int));
 #undef TD_UP
     if (cudaMemset(e->d_err, 0, sizeof(unsigned)) != cudaSuccess) return fail(TDSCHA_ECUDA);
+    if (cosets_enabled()) {
+        const int crc = setup_cosets(e, dim, sym_blocks);
+        if (crc) return fail(crc);
+    }
     thermal_kernel<<<ceil_div(n, 128), 128>>>(e->w, n, T, e->ups, e->psi);
     for (int b = 0; b < n_blocks; ++b) {
         const long long dp = (dim[b] + 3) & ~3;
@@ -407,7 +513,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
     cudaDeviceSynchronize();
     void *ps[] = {e->X, e->Y, e->G, e->Xt, e->rho, e->w, e->ups, e->psi, e->sym, e->symP, e->symPT, e->d_offP, e->d_blk_start, e->d_blk_dim,
                   e->d_blk_sym_off, e->d_blocks_ids, e->d_bp_b, e->d_bp_c, e->d_pair_mu, e->d_pair_nu, e->d_err, e->ws.base,
-                  e->vjp_ws.base, e->YX, e->chunk_ops.base, e->XGT, e->d_static_lam};
+                  e->vjp_ws.base, e->YX, e->chunk_ops.base, e->XGT, e->d_static_lam, e->Rrow, e->rot_ws.base};
     for (void *p : ps)
         if (p) cudaFree(p);
     for (auto &o : e->ops) free_ops(o);
@@ -416,6 +522,7 @@ int ensemble_destroy(tdscha_ensemble *e) {
         if (e->YXm_lo[f]) cudaFree(e->YXm_lo[f]);
     }
     free_pair_classes(e->pairs);
+    free_cosets(e->cosets);
     sym_umma_destroy(e->umma);
     if (e->cublas) cublasDestroy(e->cublas);
     delete e;
@@ -468,11 +575,14 @@ static int ensure_operands(tdscha_ensemble *e, Format fmt, bool with_lo, cudaStr
 
 // Layout of one call's workspace for M = nb * Jc rows.
 struct WsLayout {
-    size_t B1_hi, B1_lo, r1_hi, r1_lo, D1, Dcd, Cw_hi, Cw_lo, AB_hi, AB_lo, Z, F, partD, partF, total;
+    size_t B1_hi, B1_lo, r1_hi, r1_lo, D1, Dcd, Cw_hi, Cw_lo, AB_hi, AB_lo, Z, F, partD, partF;
+    size_t Ucos, r1cos, Ysr, R1r, rtmp;   // coset path and rotated basis (0 when unused)
+    size_t total;
     long long ld1, ldz, ldf;
 };
 
-static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, Format fmt, bool lo, long long Nc) {
+// ncj > 0: the coset path with ncj cosets per symmetry chunk (U / Zs and r1p / Fs share buffers)
+static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, Format fmt, bool lo, long long Nc, int ncj = 0) {
     WsLayout L{};
     const size_t es = format_bytes(fmt);
     const size_t as = (fmt == FMT_F64) ? 8 : 4;
@@ -497,6 +607,16 @@ static WsLayout layout(const tdscha_ensemble *e, int nb, int Jc, int nf_total, F
     L.F = take(M * L.ldf * as);
     L.partD = take((size_t)nb * nf_total * e->n * e->n * 8);
     L.partF = take((size_t)nb * nf_total * e->n * 8);
+    if (ncj > 0) {
+        const long long Mc = (long long)nb * ncj;
+        L.Ucos = take(Mc * std::max<long long>(e->Kp, L.ldz) * 4);
+        L.r1cos = take(Mc * std::max<long long>(e->np, L.ldf) * 4);
+    }
+    if (e->Rrow) {
+        L.Ysr = take((size_t)nb * e->n * e->n * 8);
+        L.R1r = take((size_t)nb * e->n * 8);
+        L.rtmp = take((size_t)nb * e->n * e->n * 8);
+    }
     L.total = off;
     return L;
 }
@@ -606,9 +726,16 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     const Format fmt = format_of(precision);
     const int nprod = products_of(precision);
     const bool lo = needs_lo(precision);
-    // fold chunking over symmetries: Jf symmetries per partial, at most 64 partials
-    const int Jf = std::max(16, ceil_div(e->N_sym, 64));
-    const int nf_total = ceil_div(e->N_sym, Jf);
+    // factorised symmetry path (cosets.cuh) for the mixed formats, unless the tcgen05 symmetry
+    // kernels are selected
+    const bool use_cos = e->cosets && fmt != FMT_F64 && !(fmt == FMT_BF16 && sym_umma_enabled()) && cosets_enabled();
+    const int sub = use_cos ? e->cosets->sub : 1;
+    // fold chunking: Jf symmetries (cosets on the coset path) per partial, at most 64 partials;
+    // symmetry chunks are multiples of `unit` rows
+    const int n_units = use_cos ? e->cosets->n_cos : e->N_sym;
+    const int Jf = use_cos ? ceil_div(n_units, 64) : std::max(16, ceil_div(e->N_sym, 64));
+    const int nf_total = ceil_div(n_units, Jf);
+    const int unit = use_cos ? sub * Jf : Jf;
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
     TD_CUDA(cudaStreamIsCapturing(st, &cap));
     long long Nc = e->N;
@@ -617,7 +744,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     if (cap != cudaStreamCaptureStatusNone) {
         // inside a CUDA graph capture: the plan and buffers of the previous (eager) call, unchanged
         const AvgPlan &pl = e->plan;
-        TD_CHECK(pl.valid && pl.nb == nb && pl.fmt == (int)fmt && pl.lo == lo, TDSCHA_EINVAL,
+        TD_CHECK(pl.valid && pl.nb == nb && pl.fmt == (int)fmt && pl.lo == lo && pl.cosets == use_cos, TDSCHA_EINVAL,
                  "graph capture of the averages needs an earlier call with the same batch (%d) and precision", nb);
         Nc = pl.Nc;
         Jc = pl.Jc;
@@ -659,19 +786,20 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         // GEMM chunk over symmetries: the largest multiple of Jf whose workspace fits in the budget
         // (fewer symmetry chunks = fewer rebuilds of chunked operands and fewer small launches)
         const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
-        Jc = (int)round_up(e->N_sym, Jf);
-        while (Jc > Jf && layout(e, nb, Jc, nf_total, fmt, lo, Nc).total > budget) Jc -= Jf;
+        Jc = (int)round_up(e->N_sym, unit);
+        while (Jc > unit && layout(e, nb, Jc, nf_total, fmt, lo, Nc, use_cos ? Jc / sub : 0).total > budget) Jc -= unit;
         const char *env_sym = getenv("TDSCHA_SYM_CHUNK");   // forces a smaller chunk (tuning and tests)
-        if (env_sym && atoi(env_sym) > 0) Jc = std::min(Jc, std::max(Jf, atoi(env_sym) / Jf * Jf));
+        if (env_sym && atoi(env_sym) > 0) Jc = std::min(Jc, std::max(unit, atoi(env_sym) / unit * unit));
         e->plan.valid = true;
         e->plan.nb = nb;
         e->plan.fmt = (int)fmt;
         e->plan.lo = lo;
+        e->plan.cosets = use_cos;
         e->plan.Nc = Nc;
         e->plan.Jc = Jc;
     }
     const bool chunked = Nc < e->N;
-    const WsLayout L = layout(e, nb, Jc, nf_total, fmt, lo, Nc);
+    const WsLayout L = layout(e, nb, Jc, nf_total, fmt, lo, Nc, use_cos ? Jc / sub : 0);
     if (cap != cudaStreamCaptureStatusNone)
         TD_CHECK(e->ws.bytes >= L.total, TDSCHA_EINVAL, "workspace changed since the plan");
     else
@@ -684,8 +812,27 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     void *AB_hi = W + L.AB_hi, *AB_lo = lo ? W + L.AB_lo : nullptr;
     double *partD = reinterpret_cast<double *>(W + L.partD);
     double *partF = reinterpret_cast<double *>(W + L.partF);
+    float *Ucos = use_cos ? reinterpret_cast<float *>(W + L.Ucos) : nullptr;
+    float *r1cos = use_cos ? reinterpret_cast<float *>(W + L.r1cos) : nullptr;
+    // inputs into the ensemble's rotated basis
+    double *Ysr = e->Rrow ? reinterpret_cast<double *>(W + L.Ysr) : nullptr;
+    double *R1r = e->Rrow ? reinterpret_cast<double *>(W + L.R1r) : nullptr;
+    double *rtmp = e->Rrow ? reinterpret_cast<double *>(W + L.rtmp) : nullptr;
+    if (e->Rrow) {
+        StageScope sc(e, ST_OTHER, st, 3);
+        TD_TRY(rotate_mats(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Ys, rtmp, Ysr, true, st));
+        TD_TRY(rotate_rows_of(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, R1, R1r, true, st));
+        Ys = Ysr;
+        R1 = R1r;
+    }
 
     SymTables t{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, e->symP, e->symPT, e->d_offP};
+    SymTables tr = t;   // the coset representatives' tables
+    if (use_cos) {
+        tr.symP = e->cosets->repP;
+        tr.symPT = e->cosets->repPT;
+        tr.offP = e->cosets->d_offRep;
+    }
     if (fmt == FMT_BF16 && sym_umma_enabled()) {
         // the bf16 formats run the symmetry transform and fold on tcgen05 (tables built on first use)
         if (!e->umma) {
@@ -702,15 +849,27 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     // the transform), or the tcgen05 kernel and its vector-part kernel
     int n_classes = 0;
     for (int m = 1; m <= SYM_MT_MAX; ++m) n_classes += e->pairs.count[m] > 0 ? 1 : 0;
-    const int transform_launches = t.umma ? 3 : n_classes + 1, fold_launches = t.umma ? 2 : n_classes;
+    const int transform_launches = use_cos ? n_classes + 2 : (t.umma ? 3 : n_classes + 1);
+    const int fold_launches = use_cos ? n_classes + 2 : (t.umma ? 2 : n_classes);
+    const SymCosets *cs = e->cosets;
     for (int j0 = 0; j0 < e->N_sym; j0 += Jc) {
         const int nj = std::min(Jc, e->N_sym - j0);
         const long long M = (long long)nb * nj;
-        // rows r = k * nj + jj
+        const int ncj = nj / sub, p0 = j0 / sub;   // cosets of this chunk (coset path)
+        // rows r = k * nj + jj (internal coset-major order of the symmetries on the coset path)
         {
             StageScope sc(e, ST_TRANSFORM, st, transform_launches);
-            TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi, r1_lo,
-                                 fmt != FMT_F64, st));
+            if (use_cos) {
+                // U_p = S_p^T Ys S_p and r1 of the representatives (fp32), then the expansion D_j^T U_p D_j
+                TD_TRY(sym_transform_tc(tr, e->pairs, nb, ncj, p0, Ys, R1, e->ups, e->Kp, e->np, FMT_F32, Ucos, nullptr, r1cos,
+                                        nullptr, st));
+                TD_TRY(coset_expand(nb, ncj, sub, j0, e->P, e->Kp, e->n, Ucos, e->d_pair_mu, e->d_pair_nu, cs->partner, cs->c0,
+                                    cs->c1, fmt, B1_hi, B1_lo, st));
+                TD_TRY(coset_expand_r1(nb, ncj, sub, j0, e->n, e->np, r1cos, cs->partner, cs->c0, cs->c1, fmt, r1_hi, r1_lo, st));
+            } else {
+                TD_TRY(sym_transform(t, e->pairs, nb, nj, j0, Ys, R1, e->ups, e->P, e->Kp, e->np, fmt, B1_hi, B1_lo, r1_hi,
+                                     r1_lo, fmt != FMT_F64, st));
+            }
         }
         for (long long c0 = 0; c0 < e->N; c0 += Nc) {
             const long long Ncur = std::min(Nc, e->N - c0);
@@ -758,7 +917,12 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         // fold this chunk into the partials
         {
             StageScope sc(e, ST_FOLD, st, fold_launches);
-            if (fmt == FMT_F64)
+            if (use_cos) {
+                // sum over each coset of D_j W_j D_j^T, D_j F_j, then the representatives' dense fold
+                TD_TRY(coset_fold_inner(nb, ncj, sub, j0, e->P, L.ldz, L.ldf, e->n, (const float *)Z, (const float *)F,
+                                        e->d_pair_mu, e->d_pair_nu, cs->partner, cs->c0, cs->c1, Ucos, r1cos, st));
+                TD_TRY(sym_fold_tc(tr, e->pairs, nb, ncj, p0, Jf, nf_total, Ucos, L.ldz, r1cos, L.ldf, e->ups, partD, partF, st));
+            } else if (fmt == FMT_F64)
                 TD_TRY(sym_fold<double>(t, e->pairs, e->d_blocks_ids, nb, nj, j0, Jf, nf_total, (const double *)Z, L.ldz,
                                         (const double *)F, L.ldf, e->ups, partD, partF, false, st));
             else
@@ -767,10 +931,16 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         }
     }
     const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
-    StageScope sc(e, ST_OTHER, st);
+    StageScope sc(e, ST_OTHER, st, e->Rrow ? 4 : 1);
+    // in the rotated basis: reduce into the input buffers (free now), then rotate into the outputs
+    double *Dr = e->Rrow ? Ysr : d_out, *fr = e->Rrow ? R1r : f_out;
     fold_reduce_kernel<<<grid_for((long long)nb * e->n * e->n), 256, 0, st>>>(partD, partF, nf_total, e->n, nb, e->d_blocks_ids,
-                                                                               norm, d_out, f_out);
+                                                                               norm, Dr, fr);
     TD_CUDA(cudaGetLastError());
+    if (e->Rrow) {
+        TD_TRY(rotate_mats(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Dr, rtmp, d_out, false, st));
+        TD_TRY(rotate_rows_of(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, fr, f_out, false, st));
+    }
     return 0;
 }
 
@@ -1102,10 +1272,9 @@ static int perturb_average_vjp_mixed(tdscha_ensemble *e, int nb, const double *R
     return 0;
 }
 
-int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
-                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
-                               int precision) {
-    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+static int vjp_in_ensemble_basis(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                                 const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
+                                 int precision) {
     if (precision != TDSCHA_PREC_FP64) {
         TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
         TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);
@@ -1184,6 +1353,37 @@ int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, con
     vjp_rho_kernel<<<1, 256, 0, st>>>(N, norm, e->N_eff, e->rho, colsum, rhobar);
     TD_CUDA(cudaGetLastError());
     return 0;
+}
+
+// The ensemble's rotated basis (X' = X R, tables R^T S R): (R1, Ys, fbar, Dbar) are rotated in,
+// d/dY = d/dY' . R^T rotated back; rho is unchanged.
+int perturb_average_vjp_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                               const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
+                               int precision) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    if (!e->Rrow) return vjp_in_ensemble_basis(e, nb, R1, Ys, apply_d4, fbar, Dbar, Ybar, rhobar, st, precision);
+    TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+    TD_CHECK(R1 && Ys && fbar && Dbar && Ybar && rhobar, TDSCHA_EINVAL, "NULL argument");
+    const int n = e->n;
+    const size_t vec = ((size_t)nb * n * 8 + 255) / 256 * 256, mat = ((size_t)nb * n * n * 8 + 255) / 256 * 256;
+    const size_t yb = ((size_t)e->N * n * 8 + 255) / 256 * 256;
+    const size_t need = 2 * vec + 3 * mat + yb;
+    if (e->rot_ws.bytes < need) {
+        if (e->rot_ws.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->rot_ws.base); e->rot_ws = Workspace(); }
+        TD_CUDA(cudaMalloc(&e->rot_ws.base, need));
+        e->rot_ws.bytes = need;
+    }
+    uint8_t *W = static_cast<uint8_t *>(e->rot_ws.base);
+    double *R1r = reinterpret_cast<double *>(W), *fr = reinterpret_cast<double *>(W + vec);
+    double *Ysr = reinterpret_cast<double *>(W + 2 * vec), *Dr = reinterpret_cast<double *>(W + 2 * vec + mat);
+    double *tmp = reinterpret_cast<double *>(W + 2 * vec + 2 * mat), *Yr = reinterpret_cast<double *>(W + 2 * vec + 3 * mat);
+    const int dmax = e->dmax;
+    TD_TRY(rotate_rows_of(nb, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, R1, R1r, true, st));
+    TD_TRY(rotate_rows_of(nb, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, fbar, fr, true, st));
+    TD_TRY(rotate_mats(nb, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Ys, tmp, Ysr, true, st));
+    TD_TRY(rotate_mats(nb, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Dbar, tmp, Dr, true, st));
+    TD_TRY(vjp_in_ensemble_basis(e, nb, R1r, Ysr, apply_d4, fr, Dr, Yr, rhobar, st, precision));
+    return rotate_rows_of(e->N, n, dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Yr, Ybar, false, st);
 }
 
 }  // namespace tdscha

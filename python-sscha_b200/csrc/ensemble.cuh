@@ -24,6 +24,7 @@
 #include <vector>
 #include "common.cuh"
 #include "symmetry.cuh"
+#include "cosets.cuh"
 
 struct tdscha_ensemble;
 
@@ -50,6 +51,7 @@ struct AvgPlan {
     bool valid = false;
     int nb = 0, fmt = -1;
     bool lo = false;
+    bool cosets = false;
     long long Nc = 0;
     int Jc = 0;
 };
@@ -105,6 +107,12 @@ struct tdscha_ensemble {
     tdscha::SymUmma *umma = nullptr;               // tcgen05 symmetry transform / fold tables (bf16 formats)
     void *YXm_hi[3] = {nullptr, nullptr, nullptr};  // [Y; X~] (2N x np) per storage format (mixed VJP)
     void *YXm_lo[3] = {nullptr, nullptr, nullptr};
+    // Rotated mode basis (inside degenerate blocks) in which a subgroup of the symmetries is 2 x 2
+    // sparse: X, Y, G, X~ and the symmetry tables are stored in it, and the averages and their VJP
+    // rotate their inputs in and their outputs back.  nullptr: the basis as given.
+    double *Rrow = nullptr;                        // n x dmax, Rrow[mu][q] = R_b[mu - s_b][q]
+    tdscha::SymCosets *cosets = nullptr;           // factorised symmetry transform / fold (mixed formats)
+    tdscha::Workspace rot_ws;                      // rotated inputs / outputs of the VJP
 };
 
 namespace tdscha {

@@ -145,9 +145,11 @@ __device__ __forceinline__ void store_tile_t(float *Xhi, float *Xlo, int m0, int
     }
 }
 
-// bf16 / tf32 hi + lo of an fp32 value into the GEMM operand arrays
+// bf16 / tf32 hi + lo of an fp32 value into the GEMM operand arrays (FMT_F32: the value itself)
 __device__ __forceinline__ void store_split_f(Format fmt, void *hi, void *lo, long long idx, float x) {
-    if (fmt == FMT_BF16) {
+    if (fmt == FMT_F32) {
+        static_cast<float *>(hi)[idx] = x;
+    } else if (fmt == FMT_BF16) {
         const __nv_bfloat16 h = __float2bfloat16_rn(x);
         static_cast<__nv_bfloat16 *>(hi)[idx] = h;
         if (lo) static_cast<__nv_bfloat16 *>(lo)[idx] = __float2bfloat16_rn(x - __bfloat162float(h));
@@ -584,7 +586,8 @@ int launch_fold_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, in
 int sym_transform_tc(const SymTables &t, const PairClasses &pc, int nb, int nj, int j0, const double *Ys, const double *R1,
                      const double *ups, long long Kp, long long np, Format fmt, void *B1_hi, void *B1_lo, void *r1_hi,
                      void *r1_lo, cudaStream_t st) {
-    TD_CHECK(fmt == FMT_BF16 || fmt == FMT_TF32, TDSCHA_EINVAL, "tensor-core symmetry transform needs a split storage format");
+    TD_CHECK(fmt == FMT_BF16 || fmt == FMT_TF32 || fmt == FMT_F32, TDSCHA_EINVAL,
+             "tensor-core symmetry transform needs a split storage format or fp32");
     TD_TRY((launch_transform_tc<1>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st)));
     TD_TRY((launch_transform_tc<2>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st)));
     TD_TRY((launch_transform_tc<3>(t, pc, nb, nj, j0, Ys, R1, ups, Kp, np, fmt, B1_hi, B1_lo, r1_hi, r1_lo, st)));

@@ -59,6 +59,8 @@ def load():
     lib.tdscha_ensemble_destroy.argtypes = [vp]
     lib.tdscha_ensemble_info.argtypes = [vp, ip, ip, ip, ip, dp, dp]
     lib.tdscha_ensemble_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
+    lib.tdscha_ensemble_cosets.argtypes = [vp, ip, ip, ip, dp]
+    lib.tdscha_symmetry_cosets.argtypes = [ctypes.c_int, ctypes.c_int, ip, ctypes.POINTER(dp), ip, ip, ip, ip, dp, dp]
     lib.tdscha_perturb_average_sym.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, dp, dp]
     lib.tdscha_perturb_average_sym_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp]
     lib.tdscha_GetPerturbAverageSym.argtypes = [dp, dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
@@ -151,6 +153,14 @@ class DeviceEnsemble:
         b = ctypes.c_longlong()
         check(self._lib.tdscha_ensemble_device_bytes(self.handle, ctypes.byref(b)))
         return b.value
+
+    def cosets(self):
+        """The factorised symmetry path: dict(rotated, n_cosets, coset_size, offpattern)
+        (tdscha_ensemble_cosets; n_cosets = 0 when the general symmetry kernels run)."""
+        r, nc, cs, off = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+        check(self._lib.tdscha_ensemble_cosets(self.handle, ctypes.byref(r), ctypes.byref(nc), ctypes.byref(cs),
+                                               ctypes.byref(off)))
+        return dict(rotated=bool(r.value), n_cosets=nc.value, coset_size=cs.value, offpattern=off.value)
 
     STAGES = ("transform", "gemm_ab", "gemm_cd", "weights", "gemm_z", "gemm_f", "fold", "other")
 
@@ -368,6 +378,33 @@ def project_ensemble(u, f, masses, pols):
     Y = np.empty((N, n))
     check(lib.tdscha_project_ensemble(_d(u), _d(f), _d(m), _d(P), N, nat3, n, _d(X), _d(Y)))
     return X, Y
+
+
+def symmetry_cosets(symmetries):
+    """Host analysis of per-block symmetry tables (list of (N_sym, d, d)) behind the factorised
+    symmetry path (tdscha_symmetry_cosets; no device needed).  Returns None when the group has no
+    such structure, else dict(n_cosets, coset_size, order (N_sym), partner (n), R (list of d x d
+    rotations, R_b[q', q] = component q' of rotated mode q), offpattern)."""
+    lib = load()
+    tabs = [np.ascontiguousarray(t, dtype=np.float64) for t in symmetries]
+    N_sym = tabs[0].shape[0]
+    dims = [t.shape[1] for t in tabs]
+    n = sum(dims)
+    n_deg = np.array(dims, dtype=np.intc)
+    ptrs = (dp * len(tabs))(*[_d(t) for t in tabs])
+    nc, cs, off = ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    order = np.zeros(N_sym, dtype=np.intc)
+    partner = np.zeros(n, dtype=np.intc)
+    R = np.zeros(sum(d * d for d in dims))
+    check(lib.tdscha_symmetry_cosets(N_sym, len(tabs), _i(n_deg), ptrs, ctypes.byref(nc), ctypes.byref(cs), _i(order),
+                                     _i(partner), _d(R), ctypes.byref(off)))
+    if nc.value == 0:
+        return None
+    Rs, o = [], 0
+    for d in dims:
+        Rs.append(R[o:o + d * d].reshape(d, d).copy())
+        o += d * d
+    return dict(n_cosets=nc.value, coset_size=cs.value, order=order, partner=partner, R=Rs, offpattern=off.value)
 
 
 def symmetries_on_modes(pols, perm, rot, deg_space):
