@@ -20,12 +20,14 @@
 #include <algorithm>
 #include <atomic>
 #include <cstdint>
+#include <cstdio>
 #include <cstdlib>
 #include <functional>
 #include <map>
 #include <mutex>
 #include <tuple>
 #include <utility>
+#include <vector>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
@@ -491,6 +493,7 @@ static unsigned tile_sync_budget_ns() {
 struct Prepared {
     std::function<void(int)> launch;
     int num_m = 0;
+    int bn = 0;            // tile width (outputs per tile along N)
     long long tiles = 0;
 };
 
@@ -522,6 +525,7 @@ static int prepare_cfg(const GemmOperands &op, int M, int N, int K, float *D, lo
     const unsigned long long wait_ns = g_wait_budget_ns.load();
     unsigned *cnt = (sync_ns > 0 && tiles > grid.x) ? counter : nullptr;
     out->num_m = ceil_div(M, BM);
+    out->bn = BN;
     out->tiles = tiles;
     out->launch = [=](int gm) {
         if (cnt) cudaMemsetAsync(cnt, 0, sizeof(unsigned), st);
@@ -533,8 +537,10 @@ static int prepare_cfg(const GemmOperands &op, int M, int N, int K, float *D, lo
 
 // ---- tile-shape and tile-order autotuner -----------------------------------------------------------
 // On the first call for a (format, products, M, N, K) the launcher times every candidate (tile
-// configuration, tile-group size) on the caller's stream (fastest of two runs each; every run writes
-// the same D) and remembers the winner.  Tile configurations: 128 x 256 with the stage count that
+// configuration, tile-group size) on the caller's stream and remembers the winner: the candidates run
+// in turn, twice round (every run writes the same D), and each keeps its faster run, so that the clock
+// drift of a power-capped GPU over the trials does not favour the candidates timed first.
+// TDSCHA_AUTOTUNE_VERBOSE=1 prints every trial and the choice to stderr.  Tile configurations: 128 x 256 with the stage count that
 // fits (2 for the split modes, 4 otherwise) and 128 x 128 with more stages (3 / 6): the wide tile
 // reads each A panel half as often, the narrow one keeps a deeper copy pipeline.  Small problems,
 // launches that accumulate or are being captured, and TDSCHA_AUTOTUNE=0 use the wide tile in the
@@ -564,11 +570,10 @@ static int choose(int tf32, int nprod, int M, int N, int K, const Prepared *cfgs
     const char *env = getenv("TDSCHA_AUTOTUNE");
     const bool enabled = allow_trials && !(env && atoi(env) == 0);
     int best_c = 0, best_gm = cfgs[0].num_m;
+    const char *env_v = getenv("TDSCHA_AUTOTUNE_VERBOSE");
+    const bool verbose = env_v && atoi(env_v) == 1;
     if (enabled && cfgs[0].tiles >= 8LL * sms) {
-        cudaEvent_t e0, e1;
-        TD_CUDA(cudaEventCreate(&e0));
-        TD_CUDA(cudaEventCreate(&e1));
-        float best_ms = 1e30f;
+        std::vector<std::pair<int, int>> cands;   // (configuration, tile-group size)
         for (int c = 0; c < ncfg; ++c) {
             const int num_m = cfgs[c].num_m;
             const int cand_all[] = {num_m, 48, 24, 12, 6};
@@ -576,24 +581,38 @@ static int choose(int tf32, int nprod, int M, int N, int K, const Prepared *cfgs
                 const int cand = cand_all[ci];
                 bool dup = cand > num_m;
                 for (int cj = 0; cj < ci; ++cj) dup = dup || cand_all[cj] == cand;
-                if (dup) continue;
-                float t_min = 1e30f;
-                for (int rep = 0; rep < 2; ++rep) {
-                    TD_CUDA(cudaEventRecord(e0, st));
-                    cfgs[c].launch(cand);
-                    TD_CUDA(cudaGetLastError());
-                    TD_CUDA(cudaEventRecord(e1, st));
-                    TD_CUDA(cudaEventSynchronize(e1));
-                    float ms = 0.f;
-                    TD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-                    t_min = std::min(t_min, ms);
-                }
-                if (t_min < best_ms) { best_ms = t_min; best_c = c; best_gm = cand; }
+                if (!dup) cands.push_back({c, cand});
             }
         }
+        cudaEvent_t e0, e1;
+        TD_CUDA(cudaEventCreate(&e0));
+        TD_CUDA(cudaEventCreate(&e1));
+        std::vector<float> t_min(cands.size(), 1e30f);
+        for (int round = 0; round < 2; ++round)
+            for (size_t i = 0; i < cands.size(); ++i) {
+                TD_CUDA(cudaEventRecord(e0, st));
+                cfgs[cands[i].first].launch(cands[i].second);
+                TD_CUDA(cudaGetLastError());
+                TD_CUDA(cudaEventRecord(e1, st));
+                TD_CUDA(cudaEventSynchronize(e1));
+                float ms = 0.f;
+                TD_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                t_min[i] = std::min(t_min[i], ms);
+                if (verbose)
+                    fprintf(stderr, "[tc autotune] M=%d N=%d K=%d nprod=%d tile_n=%d group_m=%d round %d: %.3f ms\n", M, N, K,
+                            nprod, cfgs[cands[i].first].bn, cands[i].second, round, ms);
+            }
         cudaEventDestroy(e0);
         cudaEventDestroy(e1);
+        size_t bi = 0;
+        for (size_t i = 1; i < cands.size(); ++i)
+            if (t_min[i] < t_min[bi]) bi = i;
+        best_c = cands[bi].first;
+        best_gm = cands[bi].second;
     }
+    if (verbose)
+        fprintf(stderr, "[tc autotune] M=%d N=%d K=%d nprod=%d -> tile_n=%d group_m=%d\n", M, N, K, nprod, cfgs[best_c].bn,
+                best_gm);
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     if (allow_trials) g_tune_cfg[key] = {best_c, best_gm};
     *cfg_out = best_c;
