@@ -820,10 +820,13 @@ def main():
     value = applies / (ms_total / 1e3)
     launches = sum(c for _, c in prof.values()) + 3 * a.steps          # + 3 recurrence kernels per step
 
-    # roofline of the dominant contraction ([a | b] projection, K = n(n+1)/2)
+    # roofline of the dominant contraction ([a | b] projection, K = n(n+1)/2).  On the character-class
+    # path its executed work is flops_ratio x that of the contraction over every symmetry row.
     P = n * (n + 1) // 2
     ab_ms, ab_launches = prof["gemm_ab"]
-    flops_ab_per_apply = 2.0 * s.n_syms * (2 * a.N) * P                # = 2 N N_sym n(n+1) ~ 2 M n^2
+    cls = ens.classes()
+    ratio = cls["flops_ratio"] if cls["n_class"] else 1.0
+    flops_ab_per_apply = 2.0 * s.n_syms * (2 * a.N) * P * ratio        # = 2 N N_sym n(n+1) ~ 2 M n^2 (x ratio)
     flops_per_launch = flops_ab_per_apply * nb * a.steps / max(ab_launches, 1)
     t_launch = ab_ms / 1e3 / max(ab_launches, 1)
     peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json"))) if os.path.exists(
@@ -834,13 +837,21 @@ def main():
     nprod = 3 if a.precision.endswith("x3") else 1
     rate_div = {"bf16": 1.0, "tf32": 2.0}[a.precision[:4]] * nprod
     achieved = flops_per_launch / t_launch / 1e12
-    roofline = {"kernel": "tc_gemm_kernel ([a|b] = Y~ . V^T projection)", "bound": "tensor",
+    if cls["n_class"]:
+        kernel = (f"tc_gemm_kernel, grouped: [a|b] over {cls['n_class']} character classes of the translation subgroup "
+                  f"(executed work {ratio:.4f} x the contraction over all {s.n_syms} symmetry rows)")
+        traffic = MEASURED_TRAFFIC.get((a.L, a.N, a.chains, a.precision, "classes"))
+        tnote = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the grouped [a|b] launch (profiles/)"
+    else:
+        kernel = "tc_gemm_kernel ([a|b] = Y~ . V^T projection)"
+        traffic = MEASURED_TRAFFIC.get((a.L, a.N, a.chains, a.precision))
+        tnote = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of a reduced [a|b] launch (M 12288, N 5000, K 72832: "
+                 "9.3x its algorithmic bytes), scaled to this launch by algorithmic bytes "
+                 f"{(nb * s.n_syms + 2 * a.N) * P * 4 + nb * s.n_syms * 2 * a.N * 4:.3e}")
+    roofline = {"kernel": kernel, "bound": "tensor",
                 "achieved": achieved, "peak": bf16_peak / rate_div, "unit": "TFLOP/s",
                 "frac": achieved / (bf16_peak / rate_div),
-                "traffic": MEASURED_TRAFFIC.get((a.L, a.N, a.chains, a.precision)),
-                "traffic_note": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a reduced [a|b] launch (M 12288, "
-                                "N 5000, K 72832: 9.3x its algorithmic bytes), scaled to this launch by algorithmic bytes "
-                                f"{(nb * s.n_syms + 2 * a.N) * P * 4 + nb * s.n_syms * 2 * a.N * 4:.3e}",
+                "traffic": traffic, "traffic_note": tnote,
                 "peak_basis": f"{peak_src} bf16 dense sustained {bf16_peak} TFLOP/s / {rate_div:g} "
                               f"({nprod} product(s){', tf32 at half the bf16 rate' if a.precision.startswith('tf32') else ''})",
                 "algorithmic_flops_per_launch": flops_per_launch, "avg_launch_ms": t_launch * 1e3}
@@ -897,7 +908,7 @@ def main():
         ms_med = float(np.median(times))
         fp64_value = nb / (ms_med / 1e3)
         # the two big contractions ([a|b] and Z, cuBLAS DGEMM in this mode) per apply
-        flops_big = 2 * 2.0 * s.n_syms * (2 * a.N) * P
+        flops_big = 2 * 2.0 * s.n_syms * (2 * a.N) * P * ratio
         big_ms = (prof64["gemm_ab"][0] + prof64["gemm_z"][0]) / a.fp64_repeats
         fp64 = {"value": fp64_value, "unit": "apply_L/s", "applies_per_repeat": nb, "repeats": a.fp64_repeats,
                 "ms_per_repeat": [round(t, 2) for t in times], "ms_median": ms_med, "clocks": clocks64,
@@ -920,6 +931,8 @@ def main():
                 "data": "synthetic (seeded rock-salt ensemble)",
                 "config": {"workload": workload_name(a), "N": a.N, "n_modes": n, "N_sym": s.n_syms, "chains": nc,
                            "applies_per_step_per_gpu": nb, "precision": a.precision,
+                           "symmetry_path": (f"{cls['n_class']} character classes of the translation subgroup x coset "
+                                             "representatives" if cls["n_class"] else "every symmetry row"),
                            "l2": "inputs larger than L2 (ensemble operands several GB per precision)",
                            "parallelism": f"replicas x{world} (independent chains per GPU)"},
                 "roofline": roofline, "cpu_baseline": cpu_base, "e2e": e2e, "gpu_launches": launches,

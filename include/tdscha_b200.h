@@ -107,6 +107,33 @@ int tdscha_symmetry_cosets(int N_sym, int n_blocks, const int *n_deg, const doub
                            int *n_cosets, int *coset_size, int *order, int *partner, double *R,
                            double *offpattern);
 
+/*
+ * Character classes of the factorised path (no counterpart in the reference: its averaging loop runs
+ * over every symmetry).  On the factorised path the subgroup K is abelian, so every component of a
+ * symmetric matrix in the rotated basis is multiplied by a character of K under its matrices; the
+ * averages' two big contractions then run class by class over only that class's components, in
+ * every precision (TDSCHA_SYM_FREQ=0 at creation keeps the contractions over every symmetry row).
+ * n_class: classes in use (0 when the path is off); Kq / Kmq: padded pair / mode columns;
+ * flops_ratio: the class contractions' work relative to the same contractions over all symmetries
+ * and all pairs.  Any pointer may be NULL.
+ */
+int tdscha_ensemble_classes(const tdscha_ensemble *ens, int *n_class, int *Kq, int *Kmq, double *flops_ratio);
+
+/*
+ * The tables behind it, on host arrays (no device), for tests: sizes[4] = {n_class, Kq, Kmq, P}
+ * always; when cls is non-NULL also
+ *   cls (n_class x 5): real, pair-column offset, count, mode-column offset, count;
+ *   pcol_i (Kq x 5): mu0, nu0, mu1, nu1, partner;  pcol_d (Kq x 5): c0, c1, re, im, zc
+ *     (own value of a pair column on a symmetric matrix M: c0 M[mu0,nu0] + c1 M[mu1,nu1]; left
+ *     rows Re = re own(c), Im = im own(partner); outputs own(c) = O1[c] + zc O2[partner]);
+ *   pp_i (P x 2), pp_d (P x 2): entry (mu <= nu) of N from the outputs' own values;
+ *   mcol_i (Kmq x 2): mode, partner;  mcol_d (Kmq x 4): sign, re, im, zc;  mode_col (n).
+ * Returns sizes[0] = 0 when the group has no such structure.
+ */
+int tdscha_symmetry_classes(int N_sym, int n_blocks, const int *n_deg, const double *const *sym_blocks,
+                            int *sizes, double *flops_ratio, int *cls, int *pcol_i, double *pcol_d, int *pp_i,
+                            double *pp_d, int *mcol_i, double *mcol_d, int *mode_col);
+
 /* Device bytes the ensemble holds now (operands of every precision built so far included). */
 int tdscha_ensemble_device_bytes(const tdscha_ensemble *ens, long long *bytes);
 

@@ -9,6 +9,7 @@
 #include "apply.cuh"
 #include "common.cuh"
 #include "ensemble.cuh"
+#include "freq.cuh"
 #include "modes.cuh"
 #include "tc_gemm.cuh"
 
@@ -98,6 +99,74 @@ int tdscha_ensemble_cosets(const tdscha_ensemble *e, int *rotated, int *n_cosets
     if (n_cosets) *n_cosets = e->cosets ? e->cosets->n_cos : 0;
     if (coset_size) *coset_size = e->cosets ? e->cosets->sub : 0;
     if (offpattern) *offpattern = e->cosets ? e->cosets->offpattern : 0.0;
+    return 0;
+}
+
+int tdscha_ensemble_classes(const tdscha_ensemble *e, int *n_class, int *Kq, int *Kmq, double *flops_ratio) {
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    const FreqTables *f = e->freq;
+    if (n_class) *n_class = f ? f->n_class : 0;
+    if (Kq) *Kq = f ? f->Kq : 0;
+    if (Kmq) *Kmq = f ? f->Kmq : 0;
+    if (flops_ratio) *flops_ratio = f ? f->flops_ratio : 1.0;
+    return 0;
+}
+
+int tdscha_symmetry_classes(int N_sym, int n_blocks, const int *n_deg, const double *const *sym_blocks, int *sizes,
+                            double *flops_ratio, int *cls, int *pcol_i, double *pcol_d, int *pp_i, double *pp_d, int *mcol_i,
+                            double *mcol_d, int *mode_col) {
+    clear_error();
+    TD_CHECK(N_sym > 0 && n_blocks > 0 && n_deg && sym_blocks && sizes, TDSCHA_EINVAL, "bad arguments");
+    std::vector<int> dim(n_deg, n_deg + n_blocks), start(n_blocks);
+    int n = 0;
+    for (int b = 0; b < n_blocks; ++b) {
+        TD_CHECK(dim[b] > 0 && sym_blocks[b], TDSCHA_EINVAL, "block %d empty", b);
+        start[b] = n;
+        n += dim[b];
+    }
+    const long long P = (long long)n * (n + 1) / 2;
+    sizes[0] = sizes[1] = sizes[2] = 0;
+    sizes[3] = (int)P;
+    CosetAnalysis ca;
+    TD_TRY(analyse_cosets(N_sym, dim, sym_blocks, ca));
+    if (!ca.ok) {
+        set_error("%s", ca.why.c_str());
+        return 0;
+    }
+    FreqLayout L;
+    TD_TRY(build_freq_layout(n, dim, start, sym_blocks, ca, L));
+    if (!L.ok) return 0;
+    sizes[0] = L.n_class;
+    sizes[1] = L.Kq;
+    sizes[2] = L.Kmq;
+    if (flops_ratio) *flops_ratio = L.flops_ratio;
+    if (!cls) return 0;
+    for (int g = 0; g < L.n_class; ++g) {
+        const int v[5] = {L.cls_real[g], L.pcol_off[g], L.pcol_cnt[g], L.mcol_off[g], L.mcol_cnt[g]};
+        std::memcpy(cls + 5 * g, v, sizeof(v));
+    }
+    for (int c = 0; c < L.Kq; ++c) {
+        if (pcol_i) {
+            const int v[5] = {L.pc_mu0[c], L.pc_nu0[c], L.pc_mu1[c], L.pc_nu1[c], L.pc_partner[c]};
+            std::memcpy(pcol_i + 5 * c, v, sizeof(v));
+        }
+        if (pcol_d) {
+            const double v[5] = {L.pc_c0[c], L.pc_c1[c], L.pc_re[c], L.pc_im[c], L.pc_zc[c]};
+            std::memcpy(pcol_d + 5 * c, v, sizeof(v));
+        }
+    }
+    for (long long p = 0; p < P; ++p) {
+        if (pp_i) { pp_i[2 * p] = L.pp_col0[p]; pp_i[2 * p + 1] = L.pp_col1[p]; }
+        if (pp_d) { pp_d[2 * p] = L.pp_c0[p]; pp_d[2 * p + 1] = L.pp_c1[p]; }
+    }
+    for (int c = 0; c < L.Kmq; ++c) {
+        if (mcol_i) { mcol_i[2 * c] = L.mc_mode[c]; mcol_i[2 * c + 1] = L.mc_partner[c]; }
+        if (mcol_d) {
+            const double v[4] = {L.mc_sign[c], L.mc_re[c], L.mc_im[c], L.mc_zc[c]};
+            std::memcpy(mcol_d + 4 * c, v, sizeof(v));
+        }
+    }
+    if (mode_col) std::memcpy(mode_col, L.mode_col.data(), n * sizeof(int));
     return 0;
 }
 

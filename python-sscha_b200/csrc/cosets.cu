@@ -278,6 +278,7 @@ int analyse_cosets(int N_sym, const std::vector<int> &dim, const double *const *
         out.b0 = b0;
         out.sub = sub;
         out.n_cos = (int)members.size();
+        out.kset = K;
         out.order.clear();
         for (const auto &m : members) out.order.insert(out.order.end(), m.begin(), m.end());
         out.partner = partner;

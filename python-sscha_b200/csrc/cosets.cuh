@@ -27,6 +27,7 @@ struct CosetAnalysis {
     int sub = 0;                   // order of the subgroup = rows per coset
     int n_cos = 0;                 // number of cosets
     std::vector<int> order;        // internal symmetry row -> symmetry index (coset-major)
+    std::vector<int> kset;         // the subgroup's symmetry indices
     std::vector<int> partner;      // n: partner of each rotated mode (global index)
     std::vector<double> R;         // per block d x d, R_b[q'][q] = component q' of rotated mode q
     std::vector<long long> R_off;  // offset of block b's R_b in R
@@ -45,6 +46,8 @@ struct SymCosets {
     float *c1 = nullptr;           // (N_sym internal rows) x n: D_j[pi(q), q] (0 without a partner)
     float *repP = nullptr, *repPT = nullptr;   // padded fp32 tables of the representatives (as given / transposed)
     long long *d_offRep = nullptr;             // block offsets into repP / repPT
+    double *repS = nullptr;                    // FP64 tables of the representatives (n_cos, d, d) per block
+    long long *d_offRepS = nullptr;            // block offsets into repS
     double offpattern = 0;         // device check over all symmetries
 };
 

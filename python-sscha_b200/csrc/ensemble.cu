@@ -252,7 +252,7 @@ int symmetrize_device(int nb, int n, const double *Y, double *Ys, cudaStream_t s
 
 static void free_cosets(SymCosets *c) {
     if (!c) return;
-    void *ps[] = {c->order, c->partner, c->c0, c->c1, c->repP, c->repPT, c->d_offRep};
+    void *ps[] = {c->order, c->partner, c->c0, c->c1, c->repP, c->repPT, c->d_offRep, c->repS, c->d_offRepS};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete c;
@@ -262,6 +262,13 @@ static void free_cosets(SymCosets *c) {
 // symmetry kernels (read when an ensemble is created, and again by every averages call).
 static bool cosets_enabled() {
     const char *env = getenv("TDSCHA_SYM_COSETS");
+    return !(env && atoi(env) == 0);
+}
+
+// TDSCHA_SYM_FREQ=0 keeps the coset path's contractions over every symmetry row instead of the
+// character classes of freq.cuh (read when an ensemble is created, and again by every averages call).
+static bool freq_enabled() {
+    const char *env = getenv("TDSCHA_SYM_FREQ");
     return !(env && atoi(env) == 0);
 }
 
@@ -317,24 +324,28 @@ static int setup_cosets(tdscha_ensemble *e, const std::vector<int> &dim, const d
     std::memcpy(&c->offpattern, &bits, sizeof(double));
     if (!(c->offpattern <= 1e-7)) { free_cosets(c); return 0; }   // not a factorisation to working accuracy
     // the representatives' tables in the padded fp32 layouts of the tensor-core kernels
-    std::vector<long long> offR(nblk);
+    std::vector<long long> offR(nblk), offS(nblk);
     long long tot = 0, totd = 0;
     for (int b = 0; b < nblk; ++b) {
         const long long dp = (dim[b] + 3) & ~3;
         offR[b] = tot;
         tot += (long long)ca.n_cos * dp * dp;
-        totd = std::max<long long>(totd, (long long)ca.n_cos * dim[b] * dim[b]);
+        offS[b] = totd;
+        totd += (long long)ca.n_cos * dim[b] * dim[b];
     }
-    double *reps = nullptr;
     if (cudaMalloc(&c->repP, tot * sizeof(float)) != cudaSuccess || cudaMalloc(&c->repPT, tot * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&c->d_offRep, nblk * sizeof(long long)) != cudaSuccess || cudaMalloc(&reps, totd * sizeof(double)) != cudaSuccess) {
-        if (reps) cudaFree(reps);
+        cudaMalloc(&c->d_offRep, nblk * sizeof(long long)) != cudaSuccess ||
+        cudaMalloc(&c->repS, totd * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_offRepS, nblk * sizeof(long long)) != cudaSuccess) {
         set_error("allocation of the coset tables failed");
         return fail(TDSCHA_ENOMEM);
     }
     cudaMemcpy(c->d_offRep, offR.data(), nblk * sizeof(long long), cudaMemcpyHostToDevice);
+    cudaMemcpy(c->d_offRepS, offS.data(), nblk * sizeof(long long), cudaMemcpyHostToDevice);
     for (int b = 0; b < nblk; ++b) {
+        // the representatives' FP64 tables (rotated basis), then their padded fp32 copies
         const size_t blk = (size_t)dim[b] * dim[b];
+        double *reps = c->repS + offS[b];
         for (int p = 0; p < ca.n_cos; ++p)
             cudaMemcpy(reps + p * blk, e->sym + e->blk_sym_off[b] + (size_t)ca.order[(size_t)p * ca.sub] * blk, blk * sizeof(double),
                        cudaMemcpyDeviceToDevice);
@@ -342,13 +353,17 @@ static int setup_cosets(tdscha_ensemble *e, const std::vector<int> &dim, const d
         pad_sym_kernel<<<grid_for((long long)ca.n_cos * dp * dp), 256>>>(reps, ca.n_cos, dim[b], (int)dp, c->repP + offR[b],
                                                                          c->repPT + offR[b]);
         if (cudaDeviceSynchronize() != cudaSuccess) {
-            cudaFree(reps);
             set_error("coset tables: %s", cudaGetErrorString(cudaGetLastError()));
             return fail(TDSCHA_ECUDA);
         }
     }
-    cudaFree(reps);
     e->cosets = c;
+    // character classes of the subgroup: the big contractions class by class (freq.cuh)
+    if (freq_enabled()) {
+        FreqLayout fl;
+        TD_TRY(build_freq_layout(n, dim, e->blk_start, sym_blocks, ca, fl));
+        if (fl.ok) TD_TRY(freq_tables_create(fl, &e->freq));
+    }
     return 0;
 }
 
@@ -523,6 +538,9 @@ int ensemble_destroy(tdscha_ensemble *e) {
     }
     free_pair_classes(e->pairs);
     free_cosets(e->cosets);
+    freq_tables_destroy(e->freq);
+    for (auto &fo : e->fops)
+        if (fo.V_hi) cudaFree(fo.V_hi);   // one allocation per format, V_hi first
     sym_umma_destroy(e->umma);
     if (e->cublas) cublasDestroy(e->cublas);
     delete e;
@@ -717,6 +735,283 @@ static bool sym_umma_enabled() {
     return env && atoi(env) == 1;
 }
 
+// ------------------------------------------------------------------------------------------------
+// The averages on the character classes of the subgroup (freq.cuh): dense transform and fold over
+// the coset representatives, the four contractions class by class.
+// ------------------------------------------------------------------------------------------------
+static bool use_freq_path(const tdscha_ensemble *e, Format fmt) {
+    return e->freq && e->cosets && cosets_enabled() && freq_enabled() && !(fmt == FMT_BF16 && sym_umma_enabled());
+}
+
+// Resident character-basis operands of all configurations in format fmt (one allocation).
+static int ensure_freq_operands(tdscha_ensemble *e, Format fmt, bool lo, cudaStream_t st) {
+    FreqOps &o = e->fops[fmt];
+    if (o.built && (o.has_lo || !lo)) return 0;
+    if (o.V_hi) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(o.V_hi); o = FreqOps(); }
+    void *buf = nullptr;
+    TD_CUDA(cudaMalloc(&buf, freq_operand_bytes(*e->freq, e->N, fmt, lo)));
+    TD_TRY(ensure_XGT(e, st));
+    const int rc = freq_build_operands(*e->freq, e->X, e->G, e->Y, e->Xt, e->XGT, e->N, e->n, e->N, fmt, lo, buf, o, st);
+    if (rc) { cudaFree(buf); o = FreqOps(); return rc; }
+    return 0;
+}
+
+struct FreqWs {
+    size_t U, r1, Lab_hi, Lab_lo, Lcd_hi, Lcd_lo, H, Ch, Cw_hi, Cw_lo, AB_hi, AB_lo, O, OF, partD, partF, Ysr, R1r, rtmp;
+    size_t total;
+    long long ld1, ldz, ldf, N2pc;
+};
+
+static FreqWs freq_ws_layout(const tdscha_ensemble *e, int nb, int ncj, int nf_total, Format fmt, bool lo, long long Nc) {
+    const FreqTables &t = *e->freq;
+    FreqWs L{};
+    const size_t es = format_bytes(fmt), as = fmt == FMT_F64 ? 8 : 4;
+    const long long NR = (long long)nb * ncj, nC = t.n_class, Kmq = std::max(t.Kmq, 1);
+    L.N2pc = round_up(2 * Nc, 64);
+    L.ld1 = round_up(2 * Nc, 4);
+    L.ldz = round_up(e->P, 4);
+    L.ldf = round_up(e->n, 4);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += (bytes + 255) / 256 * 256; return o; };
+    L.U = take(NR * std::max<long long>(e->Kp, L.ldz) * as);
+    L.r1 = take(NR * std::max<long long>(e->np, L.ldf) * as);
+    L.Lab_hi = take(2 * NR * t.Kq * es);
+    L.Lab_lo = lo ? take(2 * NR * t.Kq * es) : 0;
+    L.Lcd_hi = take(2 * NR * Kmq * es);
+    L.Lcd_lo = lo ? take(2 * NR * Kmq * es) : 0;
+    L.H = take(nC * 2 * NR * L.ld1 * as);
+    L.Ch = take(nC * 2 * NR * L.ld1 * as);
+    L.Cw_hi = take(nC * 2 * NR * L.N2pc * es);
+    L.Cw_lo = lo ? take(nC * 2 * NR * L.N2pc * es) : 0;
+    L.AB_hi = take(nC * 2 * NR * L.N2pc * es);
+    L.AB_lo = lo ? take(nC * 2 * NR * L.N2pc * es) : 0;
+    L.O = take(2 * NR * t.Kq * as);
+    L.OF = take(2 * NR * Kmq * as);
+    L.partD = take((size_t)nb * nf_total * e->n * e->n * 8);
+    L.partF = take((size_t)nb * nf_total * e->n * 8);
+    L.Ysr = take((size_t)nb * e->n * e->n * 8);
+    L.R1r = take((size_t)nb * e->n * 8);
+    L.rtmp = take((size_t)nb * e->n * e->n * 8);
+    L.total = off;
+    return L;
+}
+
+// C (row-major) (+)= A . B^T for every group, FP64 (cuBLAS DGEMM per group)
+static int gemm_groups_f64(tdscha_ensemble *e, const std::vector<tc::GemmGroup> &gs, const double *A, long long lda,
+                           const double *B, long long ldb, double *C, long long ldc, bool accumulate, cudaStream_t st) {
+    const double one = 1.0, beta = accumulate ? 1.0 : 0.0;
+    cublasSetStream(e->cublas, st);
+    for (const auto &g : gs) {
+        cublasStatus_t s = cublasDgemm(e->cublas, CUBLAS_OP_T, CUBLAS_OP_N, g.N, g.M, g.K, &one, B + (long long)g.b_row * ldb + g.b_k,
+                                       (int)ldb, A + (long long)g.a_row * lda + g.a_k, (int)lda, &beta, C + g.d_off, (int)ldc);
+        TD_CHECK(s == CUBLAS_STATUS_SUCCESS, TDSCHA_ECUDA, "cublasDgemm failed (%d)", (int)s);
+    }
+    return 0;
+}
+
+static int gemm_groups(tdscha_ensemble *e, Format fmt, int nprod, const void *A_hi, const void *A_lo, long long a_rows,
+                       long long lda, const void *B_hi, const void *B_lo, long long b_rows, long long ldb,
+                       const std::vector<tc::GemmGroup> &gs, void *C, long long ldc, bool accumulate, cudaStream_t st) {
+    if (gs.empty()) return 0;
+    if (fmt == FMT_F64)
+        return gemm_groups_f64(e, gs, static_cast<const double *>(A_hi), lda, static_cast<const double *>(B_hi), ldb,
+                               static_cast<double *>(C), ldc, accumulate, st);
+    tc::GemmOperands op{fmt, nprod, A_hi, A_lo, lda, B_hi, B_lo, ldb};
+    op.accumulate = accumulate;
+    return tc::gemm_grouped(op, a_rows, lda, b_rows, ldb, gs.data(), (int)gs.size(), static_cast<float *>(C), ldc, st, e->d_err);
+}
+
+static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4, Format fmt,
+                                int nprod, bool lo, double *f_out, double *d_out, cudaStream_t st) {
+    const FreqTables &ft = *e->freq;
+    const SymCosets *cs = e->cosets;
+    const int n_cos = cs->n_cos, sub = cs->sub, nC = ft.n_class;
+    const int Jf = ceil_div(n_cos, 64);
+    const int nf_total = ceil_div(n_cos, Jf);
+    const size_t es = format_bytes(fmt);
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    TD_CUDA(cudaStreamIsCapturing(st, &cap));
+    long long Nc = e->N;
+    int ncj = 0;
+    FreqOps co;
+    if (cap != cudaStreamCaptureStatusNone) {
+        const AvgPlan &pl = e->plan;
+        TD_CHECK(pl.valid && pl.nb == nb && pl.fmt == (int)fmt && pl.lo == lo && pl.cosets && pl.freq, TDSCHA_EINVAL,
+                 "graph capture of the averages needs an earlier call with the same batch (%d) and precision", nb);
+        Nc = pl.Nc;
+        ncj = pl.Jc / sub;
+        if (Nc < e->N)
+            TD_CHECK(e->chunk_ops.bytes >= freq_operand_bytes(ft, Nc, fmt, lo), TDSCHA_EINVAL, "chunk buffer changed since the plan");
+        else {
+            TD_CHECK(e->fops[fmt].built && (e->fops[fmt].has_lo || !lo), TDSCHA_EINVAL, "operands released since the plan");
+            co = e->fops[fmt];
+        }
+    } else {
+        size_t free_b = 0, tot_b = 0;
+        TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+        const size_t avail = free_b + e->ws.bytes + e->chunk_ops.bytes;
+        const char *env_chunk = getenv("TDSCHA_CONFIG_CHUNK");
+        if (env_chunk && atoll(env_chunk) > 0 && atoll(env_chunk) < e->N) {
+            Nc = atoll(env_chunk);
+        } else if (!e->fops[fmt].built && freq_operand_bytes(ft, e->N, fmt, lo) > avail / 2) {
+            const long long per_conf = 4LL * (ft.Kq + ft.Kmq) * (long long)es * (lo ? 2 : 1);
+            const long long fit = (long long)(avail * 0.4) / per_conf;
+            Nc = std::min<long long>(e->N, std::max<long long>(32, fit / 32 * 32));
+        }
+        if (Nc < e->N) {
+            const size_t need = freq_operand_bytes(ft, Nc, fmt, lo);
+            if (e->chunk_ops.bytes < need) {
+                if (e->chunk_ops.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->chunk_ops.base); e->chunk_ops = Workspace(); }
+                TD_CUDA(cudaMalloc(&e->chunk_ops.base, need));
+                e->chunk_ops.bytes = need;
+            }
+        } else {
+            TD_TRY(ensure_freq_operands(e, fmt, lo, st));
+            co = e->fops[fmt];
+        }
+        TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+        // coset chunk: the largest multiple of Jf whose workspace fits in the budget
+        const size_t budget = std::max<size_t>((size_t)2 << 30, (size_t)((free_b + e->ws.bytes) * 0.6));
+        ncj = (int)round_up(n_cos, Jf);
+        while (ncj > Jf && freq_ws_layout(e, nb, ncj, nf_total, fmt, lo, Nc).total > budget) ncj -= Jf;
+        const char *env_sym = getenv("TDSCHA_SYM_CHUNK");   // in symmetries; forces a smaller chunk (tuning and tests)
+        if (env_sym && atoi(env_sym) > 0) ncj = std::min(ncj, std::max(Jf, atoi(env_sym) / sub / Jf * Jf));
+        e->plan.valid = true;
+        e->plan.nb = nb;
+        e->plan.fmt = (int)fmt;
+        e->plan.lo = lo;
+        e->plan.cosets = true;
+        e->plan.freq = true;
+        e->plan.Nc = Nc;
+        e->plan.Jc = ncj * sub;
+    }
+    const bool chunked = Nc < e->N;
+    const FreqWs L = freq_ws_layout(e, nb, ncj, nf_total, fmt, lo, Nc);
+    if (cap != cudaStreamCaptureStatusNone)
+        TD_CHECK(e->ws.bytes >= L.total, TDSCHA_EINVAL, "workspace changed since the plan");
+    else
+        TD_TRY(ensure_ws(e, L.total));
+    uint8_t *W = static_cast<uint8_t *>(e->ws.base);
+    auto at = [&](size_t off) -> void * { return W + off; };
+    void *U = at(L.U), *r1 = at(L.r1), *H = at(L.H), *Ch = at(L.Ch), *O = at(L.O), *OF = at(L.OF);
+    void *Lab_hi = at(L.Lab_hi), *Lab_lo = lo ? at(L.Lab_lo) : nullptr, *Lcd_hi = at(L.Lcd_hi), *Lcd_lo = lo ? at(L.Lcd_lo) : nullptr;
+    void *Cw_hi = at(L.Cw_hi), *Cw_lo = lo ? at(L.Cw_lo) : nullptr, *AB_hi = at(L.AB_hi), *AB_lo = lo ? at(L.AB_lo) : nullptr;
+    double *partD = static_cast<double *>(at(L.partD)), *partF = static_cast<double *>(at(L.partF));
+    double *Ysr = static_cast<double *>(at(L.Ysr)), *R1r = static_cast<double *>(at(L.R1r)), *rtmp = static_cast<double *>(at(L.rtmp));
+    const bool f64 = fmt == FMT_F64;
+    const size_t as = f64 ? 8 : 4;
+    {
+        StageScope sc(e, ST_OTHER, st, 3);
+        TD_TRY(rotate_mats(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Ys, rtmp, Ysr, true, st));
+        TD_TRY(rotate_rows_of(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, R1, R1r, true, st));
+    }
+    SymTables tr{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, cs->repP, cs->repPT, cs->d_offRep};
+    SymTables t64{cs->repS, cs->d_offRepS, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, nullptr, nullptr, nullptr};
+    int n_classes = 0;
+    for (int m = 1; m <= SYM_MT_MAX; ++m) n_classes += e->pairs.count[m] > 0 ? 1 : 0;
+    const long long Kmq1 = std::max(ft.Kmq, 1);
+    for (int p0 = 0; p0 < n_cos; p0 += ncj) {
+        const int nc = std::min(ncj, n_cos - p0);
+        const int NR = nb * nc;
+        {
+            StageScope sc(e, ST_TRANSFORM, st, n_classes + 3);
+            if (f64) {
+                TD_TRY(sym_transform(t64, e->pairs, nb, nc, p0, Ysr, R1r, e->ups, e->P, e->Kp, e->np, FMT_F64, U, nullptr, r1,
+                                     nullptr, false, st));
+                TD_TRY(freq_left<double>(ft, NR, e->n, (const double *)U, e->Kp, (const double *)r1, e->np, fmt, Lab_hi, Lab_lo,
+                                         Lcd_hi, Lcd_lo, st));
+            } else {
+                TD_TRY(sym_transform_tc(tr, e->pairs, nb, nc, p0, Ysr, R1r, e->ups, e->Kp, e->np, FMT_F32, U, nullptr, r1, nullptr,
+                                        st));
+                TD_TRY(freq_left<float>(ft, NR, e->n, (const float *)U, e->Kp, (const float *)r1, e->np, fmt, Lab_hi, Lab_lo,
+                                        Lcd_hi, Lcd_lo, st));
+            }
+        }
+        for (long long c0 = 0; c0 < e->N; c0 += Nc) {
+            const long long Ncur = std::min(Nc, e->N - c0);
+            const long long N2c = 2 * Ncur, N2pc = round_up(N2c, 64);   // the last chunk may be shorter
+            const bool acc = c0 > 0;
+            if (chunked) {
+                StageScope sc(e, ST_OTHER, st);
+                TD_TRY(ensure_XGT(e, st));
+                const int n = e->n;
+                TD_TRY(freq_build_operands(ft, e->X + c0 * n, e->G + c0 * n, e->Y + c0 * n, e->Xt + c0 * n, e->XGT + c0, e->N, n, Ncur,
+                                           fmt, lo, e->chunk_ops.base, co, st));
+            }
+            // per class: [a|b] and [c|d] in the character basis, (rows (comp, v, c), 2Nc columns)
+            std::vector<tc::GemmGroup> gab, gcd, gz, gf;
+            for (int g = 0; g < nC; ++g) {
+                const int Mg = ft.cls_real[g] ? NR : 2 * NR;
+                const long long hrow = (long long)g * 2 * NR;
+                gab.push_back({Mg, (int)N2c, ft.pcol_cnt[g], 0, ft.pcol_off[g], 0, ft.pcol_off[g], hrow * L.ld1});
+                gz.push_back({Mg, ft.pcol_cnt[g], (int)N2pc, (int)hrow, 0, ft.pcol_off[g], 0, (long long)ft.pcol_off[g]});
+                if (ft.mcol_cnt[g] > 0) {
+                    gcd.push_back({Mg, (int)N2c, ft.mcol_cnt[g], 0, ft.mcol_off[g], 0, ft.mcol_off[g], hrow * L.ld1});
+                    gf.push_back({Mg, ft.mcol_cnt[g], (int)N2pc, (int)hrow, 0, ft.mcol_off[g], 0, (long long)ft.mcol_off[g]});
+                } else {
+                    TD_CUDA(cudaMemsetAsync(static_cast<uint8_t *>(Ch) + hrow * L.ld1 * as, 0, (size_t)2 * NR * L.ld1 * as, st));
+                }
+            }
+            {
+                StageScope sc(e, ST_GEMM_AB, st);
+                TD_TRY(gemm_groups(e, fmt, nprod, Lab_hi, Lab_lo, 2LL * NR, ft.Kq, co.V_hi, co.V_lo, N2c, ft.Kq, gab, H, L.ld1, false,
+                                   st));
+            }
+            {
+                StageScope sc(e, ST_GEMM_CD, st);
+                TD_TRY(gemm_groups(e, fmt, nprod, Lcd_hi, Lcd_lo, 2LL * NR, Kmq1, co.XG_hi, co.XG_lo, N2c, Kmq1, gcd, Ch, L.ld1,
+                                   false, st));
+            }
+            {
+                StageScope sc(e, ST_WEIGHTS, st);
+                const long long M = (long long)nC * 2 * NR;
+                const long long per_row = Ncur + (N2pc - N2c);
+                if (f64)
+                    weights_kernel<double><<<grid_for(M * per_row), 256, 0, st>>>((const double *)H, (const double *)Ch, L.ld1,
+                                                                                 e->rho + c0, (int)Ncur, (int)M, N2pc, apply_d4,
+                                                                                 fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
+                else
+                    weights_kernel<float><<<grid_for(M * per_row), 256, 0, st>>>((const float *)H, (const float *)Ch, L.ld1,
+                                                                                e->rho + c0, (int)Ncur, (int)M, N2pc, apply_d4,
+                                                                                fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
+                TD_CUDA(cudaGetLastError());
+            }
+            {
+                StageScope sc(e, ST_GEMM_Z, st);
+                TD_TRY(gemm_groups(e, fmt, nprod, Cw_hi, Cw_lo, (long long)nC * 2 * NR, N2pc, co.VT_hi, co.VT_lo, ft.Kq, N2pc,
+                                   gz, O, ft.Kq, acc, st));
+            }
+            {
+                StageScope sc(e, ST_GEMM_F, st);
+                TD_TRY(gemm_groups(e, fmt, nprod, AB_hi, AB_lo, (long long)nC * 2 * NR, N2pc, co.YX_hi, co.YX_lo, Kmq1, N2pc,
+                                   gf, OF, Kmq1, acc, st));
+            }
+        }
+        {
+            StageScope sc(e, ST_FOLD, st, n_classes + 2);
+            if (f64) {
+                TD_TRY(freq_reconstruct<double>(ft, NR, e->n, e->P, e->d_pair_mu, e->d_pair_nu, (const double *)O, (const double *)OF,
+                                                (double *)U, L.ldz, (double *)r1, L.ldf, st));
+                TD_TRY(sym_fold<double>(t64, e->pairs, e->d_blocks_ids, nb, nc, p0, Jf, nf_total, (const double *)U, L.ldz,
+                                        (const double *)r1, L.ldf, e->ups, partD, partF, false, st));
+            } else {
+                TD_TRY(freq_reconstruct<float>(ft, NR, e->n, e->P, e->d_pair_mu, e->d_pair_nu, (const float *)O, (const float *)OF,
+                                               (float *)U, L.ldz, (float *)r1, L.ldf, st));
+                TD_TRY(sym_fold_tc(tr, e->pairs, nb, nc, p0, Jf, nf_total, (const float *)U, L.ldz, (const float *)r1, L.ldf, e->ups,
+                                   partD, partF, st));
+            }
+        }
+    }
+    const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
+    StageScope sc(e, ST_OTHER, st, 4);
+    fold_reduce_kernel<<<grid_for((long long)nb * e->n * e->n), 256, 0, st>>>(partD, partF, nf_total, e->n, nb, e->d_blocks_ids,
+                                                                               norm, Ysr, R1r);
+    TD_CUDA(cudaGetLastError());
+    TD_TRY(rotate_mats(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, Ysr, rtmp, d_out, false, st));
+    TD_TRY(rotate_rows_of(nb, e->n, e->dmax, e->Rrow, e->d_blocks_ids, e->d_blk_start, e->d_blk_dim, R1r, f_out, false, st));
+    return 0;
+}
+
 int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4, int precision,
                            double *f_out, double *d_out, cudaStream_t st) {
     TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
@@ -726,6 +1021,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     const Format fmt = format_of(precision);
     const int nprod = products_of(precision);
     const bool lo = needs_lo(precision);
+    if (use_freq_path(e, fmt)) return perturb_average_freq(e, nb, R1, Ys, apply_d4, fmt, nprod, lo, f_out, d_out, st);
     // factorised symmetry path (cosets.cuh) for the mixed formats, unless the tcgen05 symmetry
     // kernels are selected
     const bool use_cos = e->cosets && fmt != FMT_F64 && !(fmt == FMT_BF16 && sym_umma_enabled()) && cosets_enabled();
@@ -744,7 +1040,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
     if (cap != cudaStreamCaptureStatusNone) {
         // inside a CUDA graph capture: the plan and buffers of the previous (eager) call, unchanged
         const AvgPlan &pl = e->plan;
-        TD_CHECK(pl.valid && pl.nb == nb && pl.fmt == (int)fmt && pl.lo == lo && pl.cosets == use_cos, TDSCHA_EINVAL,
+        TD_CHECK(pl.valid && pl.nb == nb && pl.fmt == (int)fmt && pl.lo == lo && pl.cosets == use_cos && !pl.freq, TDSCHA_EINVAL,
                  "graph capture of the averages needs an earlier call with the same batch (%d) and precision", nb);
         Nc = pl.Nc;
         Jc = pl.Jc;
@@ -795,6 +1091,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
         e->plan.fmt = (int)fmt;
         e->plan.lo = lo;
         e->plan.cosets = use_cos;
+        e->plan.freq = false;
         e->plan.Nc = Nc;
         e->plan.Jc = Jc;
     }

@@ -25,6 +25,7 @@
 #include "common.cuh"
 #include "symmetry.cuh"
 #include "cosets.cuh"
+#include "freq.cuh"
 
 struct tdscha_ensemble;
 
@@ -52,6 +53,7 @@ struct AvgPlan {
     int nb = 0, fmt = -1;
     bool lo = false;
     bool cosets = false;
+    bool freq = false;
     long long Nc = 0;
     int Jc = 0;
 };
@@ -112,6 +114,8 @@ struct tdscha_ensemble {
     // rotate their inputs in and their outputs back.  nullptr: the basis as given.
     double *Rrow = nullptr;                        // n x dmax, Rrow[mu][q] = R_b[mu - s_b][q]
     tdscha::SymCosets *cosets = nullptr;           // factorised symmetry transform / fold (mixed formats)
+    tdscha::FreqTables *freq = nullptr;            // character classes of the subgroup (freq.cuh)
+    tdscha::FreqOps fops[3];                       // character-basis operands per storage format (resident)
     tdscha::Workspace rot_ws;                      // rotated inputs / outputs of the VJP
 };
 

@@ -1,0 +1,566 @@
+// freq.cu -- character classes of the symmetry subgroup (host) and the operand / left-operand /
+// reconstruction kernels of the averages in the character basis (device).  The algebra is stated in
+// freq.cuh.
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <map>
+#include <vector>
+
+#include "freq.cuh"
+
+namespace tdscha {
+
+// ================================================================================================
+// Host: classes and layouts
+// ================================================================================================
+namespace {
+
+using Chi = std::vector<std::complex<double>>;
+
+std::vector<long long> chi_key(const Chi &c, bool conj) {
+    std::vector<long long> k(2 * c.size());
+    for (size_t t = 0; t < c.size(); ++t) {
+        k[2 * t] = std::llround(c[t].real() * 1e6);
+        k[2 * t + 1] = std::llround((conj ? -c[t].imag() : c[t].imag()) * 1e6);
+    }
+    return k;
+}
+
+Chi chi_mul(const Chi &a, const Chi &b, bool conj_b) {
+    Chi r(a.size());
+    for (size_t t = 0; t < a.size(); ++t) r[t] = a[t] * (conj_b ? std::conj(b[t]) : b[t]);
+    return r;
+}
+
+struct Term {
+    int mu, nu;
+    double c;
+};
+
+// One component of the symmetric-matrix space: real part = sum re, imaginary part = sum im of the
+// matrix entries (im empty for a real scalar component), character chi, Frobenius multiplicity m.
+struct Comp {
+    int cls = -1;
+    bool conj = false;
+    double m = 1;
+    std::vector<Term> re, im;
+    int col = -1;   // first column (the imaginary part is at col + 1)
+};
+
+// M[mu, nu] += c * (part 0: real, 1: imaginary) of component k
+struct Recon {
+    int mu, nu, comp, part;
+    double c;
+};
+
+}  // namespace
+
+int build_freq_layout(int n, const std::vector<int> &dim, const std::vector<int> &blk_start, const double *const *sym_blocks,
+                      const CosetAnalysis &ca, FreqLayout &out) {
+    out = FreqLayout();
+    if (!ca.ok || (int)ca.kset.size() != ca.sub) return 0;
+    const int sub = ca.sub;
+    const int nblk = (int)dim.size();
+    // characters of every rotated mode on the subgroup: chi_q(t) = D_t[q, q] + i D_t[pi(q), q]
+    std::vector<Chi> chi(n, Chi(sub));
+    for (int b = 0; b < nblk; ++b) {
+        const int d = dim[b], s = blk_start[b];
+        const double *R = ca.R.data() + ca.R_off[b];
+        std::vector<double> T((size_t)d * d);
+        for (int t = 0; t < sub; ++t) {
+            const double *S = sym_blocks[b] + (size_t)ca.kset[t] * d * d;
+            for (int k = 0; k < d; ++k)
+                for (int q = 0; q < d; ++q) {
+                    double acc = 0.0;
+                    for (int l = 0; l < d; ++l) acc += S[(size_t)k * d + l] * R[(size_t)l * d + q];
+                    T[(size_t)k * d + q] = acc;
+                }
+            for (int q = 0; q < d; ++q) {
+                const int pq = ca.partner[s + q] - s;
+                double re = 0.0, im = 0.0;
+                for (int k = 0; k < d; ++k) re += R[(size_t)k * d + q] * T[(size_t)k * d + q];
+                if (pq != q)
+                    for (int k = 0; k < d; ++k) im += R[(size_t)k * d + pq] * T[(size_t)k * d + q];
+                chi[s + q][t] = {re, im};
+            }
+        }
+    }
+    std::map<std::vector<long long>, int> cls_of;
+    std::vector<int> cls_real;
+    auto classify = [&](const Chi &c, bool &conj) {
+        const auto kc = chi_key(c, false), kb = chi_key(c, true);
+        const bool real = kc == kb;
+        conj = !real && kb < kc;
+        const auto &canon = conj ? kb : kc;
+        auto it = cls_of.find(canon);
+        if (it != cls_of.end()) return it->second;
+        const int id = (int)cls_real.size();
+        cls_of.emplace(canon, id);
+        cls_real.push_back(real ? 1 : 0);
+        return id;
+    };
+    // orbits: a real mode, or a complex pair (lead, partner) with lead < partner
+    std::vector<std::pair<int, int>> orbits;
+    for (int q = 0; q < n; ++q) {
+        const int pq = ca.partner[q];
+        if (pq == q) orbits.push_back({q, -1});
+        else if (q < pq) orbits.push_back({q, pq});
+    }
+    // pair components and the reconstruction of every matrix entry from them
+    std::vector<Comp> comps;
+    std::vector<Recon> recon;
+    const Chi one(sub, {1.0, 0.0});
+    auto add = [&](const Chi &c, double m, std::vector<Term> re, std::vector<Term> im) {
+        Comp k;
+        k.cls = classify(c, k.conj);
+        k.m = m;
+        k.re = std::move(re);
+        k.im = std::move(im);
+        comps.push_back(std::move(k));
+        return (int)comps.size() - 1;
+    };
+    const int no = (int)orbits.size();
+    for (int a = 0; a < no; ++a)
+        for (int b = a; b < no; ++b) {
+            int q = orbits[a].first, qb = orbits[a].second, r = orbits[b].first, rb = orbits[b].second;
+            if (qb >= 0 && rb >= 0 && a != b) {
+                // 2 x 2 block: linear part (chi_q conj chi_r) and antilinear part (chi_q chi_r)
+                const int L = add(chi_mul(chi[q], chi[r], true), 4.0, {{q, r, 0.5}, {qb, rb, 0.5}}, {{qb, r, 0.5}, {q, rb, -0.5}});
+                const int A = add(chi_mul(chi[q], chi[r], false), 4.0, {{q, r, 0.5}, {qb, rb, -0.5}}, {{q, rb, 0.5}, {qb, r, 0.5}});
+                recon.push_back({q, r, L, 0, 1.0}); recon.push_back({q, r, A, 0, 1.0});
+                recon.push_back({qb, rb, L, 0, 1.0}); recon.push_back({qb, rb, A, 0, -1.0});
+                recon.push_back({qb, r, L, 1, 1.0}); recon.push_back({qb, r, A, 1, 1.0});
+                recon.push_back({q, rb, L, 1, -1.0}); recon.push_back({q, rb, A, 1, 1.0});
+            } else if (qb >= 0 && a == b) {
+                // diagonal 2 x 2 block: trace part (trivial character) and antilinear part (chi_q^2)
+                const int L = add(one, 2.0, {{q, q, 0.5}, {qb, qb, 0.5}}, {});
+                const int A = add(chi_mul(chi[q], chi[q], false), 2.0, {{q, q, 0.5}, {qb, qb, -0.5}}, {{q, qb, 1.0}});
+                recon.push_back({q, q, L, 0, 1.0}); recon.push_back({q, q, A, 0, 1.0});
+                recon.push_back({qb, qb, L, 0, 1.0}); recon.push_back({qb, qb, A, 0, -1.0});
+                recon.push_back({q, qb, A, 1, 1.0});
+            } else if (qb >= 0 || rb >= 0) {
+                if (qb >= 0) { std::swap(q, r); std::swap(qb, rb); }   // q real, (r, rb) complex
+                const int W = add(chi_mul(chi[q], chi[r], false), 2.0, {{q, r, 1.0}}, {{q, rb, 1.0}});
+                recon.push_back({q, r, W, 0, 1.0});
+                recon.push_back({q, rb, W, 1, 1.0});
+            } else {
+                const int S = add(chi_mul(chi[q], chi[r], false), q == r ? 1.0 : 2.0, {{q, r, 1.0}}, {});
+                recon.push_back({q, r, S, 0, 1.0});
+            }
+        }
+    const long long P = (long long)n * (n + 1) / 2;
+    // mode components (orbits) and their classes
+    struct ModeComp {
+        int cls;
+        bool conj;
+        int q, qb;
+        int col;
+    };
+    std::vector<ModeComp> mcomps;
+    for (auto [q, qb] : orbits) {
+        ModeComp mc{};
+        mc.cls = classify(chi[q], mc.conj);
+        mc.q = q;
+        mc.qb = qb;
+        mcomps.push_back(mc);
+    }
+    const int ncls = (int)cls_real.size();
+    std::vector<std::vector<int>> by_cls(ncls), mby_cls(ncls);
+    for (int k = 0; k < (int)comps.size(); ++k) by_cls[comps[k].cls].push_back(k);
+    for (int k = 0; k < (int)mcomps.size(); ++k) mby_cls[mcomps[k].cls].push_back(k);
+    // column layout, class by class (classes without pair components drop out: they carry nothing)
+    int kq = 0, kmq = 0;
+    std::vector<int> keep;
+    for (int g = 0; g < ncls; ++g) {
+        if (by_cls[g].empty()) continue;
+        const int id = (int)keep.size();
+        keep.push_back(g);
+        out.cls_real.push_back(cls_real[g]);
+        out.pcol_off.push_back(kq);
+        int cnt = 0;
+        for (int k : by_cls[g]) { comps[k].col = kq + cnt; cnt += comps[k].im.empty() ? 1 : 2; }
+        out.pcol_cnt.push_back((int)round_up(cnt, 64));
+        kq += out.pcol_cnt.back();
+        out.mcol_off.push_back(kmq);
+        int mcnt = 0;
+        for (int k : mby_cls[g]) { mcomps[k].col = kmq + mcnt; mcnt += mcomps[k].qb >= 0 ? 2 : 1; }
+        out.mcol_cnt.push_back(mcnt ? (int)round_up(mcnt, 64) : 0);
+        kmq += out.mcol_cnt.back();
+        (void)id;
+    }
+    out.n_class = (int)keep.size();
+    out.Kq = kq;
+    out.Kmq = kmq;
+    std::vector<int> new_id(ncls, -1);
+    for (int i = 0; i < out.n_class; ++i) new_id[keep[i]] = i;
+    // pair columns
+    out.pc_mu0.assign(kq, 0); out.pc_nu0.assign(kq, 0); out.pc_mu1.assign(kq, 0); out.pc_nu1.assign(kq, 0);
+    out.pc_c0.assign(kq, 0.0); out.pc_c1.assign(kq, 0.0);
+    out.pc_partner.assign(kq, -1);
+    out.pc_re.assign(kq, 0.0); out.pc_im.assign(kq, 0.0); out.pc_zc.assign(kq, 0.0);
+    long long total_cols = 0;
+    for (const Comp &k : comps) {
+        const int g = new_id[k.cls];
+        const bool real = out.cls_real[g] != 0;
+        const double sK = real ? (double)sub : 0.5 * sub;
+        const int ncol = k.im.empty() ? 1 : 2;
+        total_cols += ncol;
+        for (int part = 0; part < ncol; ++part) {
+            const int c = k.col + part;
+            const std::vector<Term> &tm = part ? k.im : k.re;
+            const double sg = (part && k.conj) ? -1.0 : 1.0;   // canonical = conjugate: imaginary part negated
+            if (tm.size() > 0) { out.pc_mu0[c] = tm[0].mu; out.pc_nu0[c] = tm[0].nu; out.pc_c0[c] = sg * tm[0].c; }
+            if (tm.size() > 1) { out.pc_mu1[c] = tm[1].mu; out.pc_nu1[c] = tm[1].nu; out.pc_c1[c] = sg * tm[1].c; }
+            const double s = part ? -1.0 : 1.0;
+            out.pc_partner[c] = ncol == 2 ? k.col + 1 - part : -1;
+            out.pc_re[c] = sK * k.m;
+            out.pc_im[c] = (real || ncol == 1) ? 0.0 : sK * k.m * s;
+            out.pc_zc[c] = (real || ncol == 1) ? 0.0 : -s;
+        }
+    }
+    if (total_cols != P) return 0;   // not a decomposition of the pair space (cannot happen for a valid analysis)
+    // reconstruction of every packed pair
+    auto packed = [n](int a, int b) {
+        const long long lo = std::min(a, b), hi = std::max(a, b);
+        return lo * n - lo * (lo - 1) / 2 + (hi - lo);
+    };
+    out.pp_col0.assign(P, 0); out.pp_col1.assign(P, 0);
+    out.pp_c0.assign(P, 0.0); out.pp_c1.assign(P, 0.0);
+    std::vector<int> nterm(P, 0);
+    for (const Recon &r : recon) {
+        const Comp &k = comps[r.comp];
+        const long long p = packed(r.mu, r.nu);
+        const int col = k.col + r.part;
+        const double c = r.c * ((r.part && k.conj) ? -1.0 : 1.0);
+        if (nterm[p] == 0) { out.pp_col0[p] = col; out.pp_c0[p] = c; }
+        else if (nterm[p] == 1) { out.pp_col1[p] = col; out.pp_c1[p] = c; }
+        else return 0;
+        ++nterm[p];
+    }
+    for (long long p = 0; p < P; ++p)
+        if (nterm[p] == 0) return 0;
+    // mode columns
+    out.mc_mode.assign(kmq, 0); out.mc_partner.assign(kmq, -1);
+    out.mc_sign.assign(kmq, 0.0); out.mc_re.assign(kmq, 0.0); out.mc_im.assign(kmq, 0.0); out.mc_zc.assign(kmq, 0.0);
+    out.mode_col.assign(n, -1);
+    for (const ModeComp &mc : mcomps) {
+        const int g = new_id[mc.cls];
+        if (g < 0) continue;   // a class without pair components: its averages' terms vanish
+        const bool real = out.cls_real[g] != 0;
+        const double sK = real ? (double)sub : 0.5 * sub;
+        const int ncol = mc.qb >= 0 ? 2 : 1;
+        for (int part = 0; part < ncol; ++part) {
+            const int c = mc.col + part;
+            const double s = part ? -1.0 : 1.0;
+            out.mc_mode[c] = part ? mc.qb : mc.q;
+            out.mc_sign[c] = (part && mc.conj) ? -1.0 : 1.0;
+            out.mc_partner[c] = ncol == 2 ? mc.col + 1 - part : -1;
+            out.mc_re[c] = sK;
+            out.mc_im[c] = (real || ncol == 1) ? 0.0 : sK * s;
+            out.mc_zc[c] = (real || ncol == 1) ? 0.0 : -s;
+            out.mode_col[out.mc_mode[c]] = c;
+        }
+    }
+    // work of the class contractions relative to one over every symmetry and all pairs
+    double work = 0.0;
+    for (int g = 0; g < out.n_class; ++g) work += (out.cls_real[g] ? 1.0 : 2.0) * out.pcol_cnt[g];
+    out.flops_ratio = work / ((double)sub * (double)P);
+    out.ok = true;
+    return 0;
+}
+
+}  // namespace tdscha
+
+// ================================================================================================
+// Device: tables, operands, left operands, reconstruction
+// ================================================================================================
+namespace tdscha {
+namespace {
+
+template <typename T>
+int upload(const std::vector<T> &v, T **dst, size_t *acc) {
+    *dst = nullptr;
+    if (v.empty()) return 0;
+    TD_CUDA(cudaMalloc(dst, v.size() * sizeof(T)));
+    TD_CUDA(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *acc += v.size() * sizeof(T);
+    return 0;
+}
+
+__device__ __forceinline__ long long packed_of(int a, int b, int n) {
+    const int lo = a < b ? a : b, hi = a < b ? b : a;
+    return (long long)lo * n - ((long long)lo * (lo - 1)) / 2 + (hi - lo);
+}
+
+unsigned grid1(long long work) { return (unsigned)std::max<long long>(1, std::min<long long>((work + 255) / 256, 148LL * 32)); }
+
+dim3 grid_rows(long long cols, long long rows) {
+    const long long gx = std::max<long long>(1, std::min<long long>(ceil_div(cols, 256), 64));
+    const long long gy = std::max<long long>(1, std::min<long long>(rows, 65535));
+    return dim3((unsigned)gx, (unsigned)gy);
+}
+
+// Vq (2Nc x Kq): row k < Nc: components of x x^T, row Nc + i: of sym(x g^T)
+__global__ void build_Vq_kernel(const double *__restrict__ X, const double *__restrict__ G, int n, long long Nc, int Kq,
+                                const int *__restrict__ mu0, const int *__restrict__ nu0, const int *__restrict__ mu1,
+                                const int *__restrict__ nu1, const double *__restrict__ c0, const double *__restrict__ c1,
+                                Format fmt, void *hi, void *lo) {
+    for (long long k = blockIdx.y; k < 2 * Nc; k += gridDim.y) {
+        const bool second = k >= Nc;
+        const double *x = X + (second ? k - Nc : k) * n;
+        const double *g = G + (second ? k - Nc : k) * n;
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Kq; c += gridDim.x * blockDim.x) {
+            const int a0 = mu0[c], b0 = nu0[c], a1 = mu1[c], b1 = nu1[c];
+            double v;
+            if (!second) v = c0[c] * x[a0] * x[b0] + c1[c] * x[a1] * x[b1];
+            else v = 0.5 * (c0[c] * (x[a0] * g[b0] + x[b0] * g[a0]) + c1[c] * (x[a1] * g[b1] + x[b1] * g[a1]));
+            store_split(fmt, hi, lo, k * Kq + c, v);
+        }
+    }
+}
+
+// VqT (Kq x N2pc) from XGT = [X^T ; G^T] (2n x ldT, configuration-contiguous): coalesced reads
+__global__ void build_VqT_kernel(const double *__restrict__ XGT, long long ldT, int n, long long Nc, long long N2pc, int Kq,
+                                 const int *__restrict__ mu0, const int *__restrict__ nu0, const int *__restrict__ mu1,
+                                 const int *__restrict__ nu1, const double *__restrict__ c0, const double *__restrict__ c1,
+                                 Format fmt, void *hi, void *lo) {
+    for (long long c = blockIdx.y; c < Kq; c += gridDim.y) {
+        const int a0 = mu0[c], b0 = nu0[c], a1 = mu1[c], b1 = nu1[c];
+        const double k0 = c0[c], k1 = c1[c];
+        const double *xa0 = XGT + (long long)a0 * ldT, *xb0 = XGT + (long long)b0 * ldT;
+        const double *xa1 = XGT + (long long)a1 * ldT, *xb1 = XGT + (long long)b1 * ldT;
+        const double *ga0 = XGT + (long long)(n + a0) * ldT, *gb0 = XGT + (long long)(n + b0) * ldT;
+        const double *ga1 = XGT + (long long)(n + a1) * ldT, *gb1 = XGT + (long long)(n + b1) * ldT;
+        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N2pc; k += (long long)gridDim.x * blockDim.x) {
+            double v = 0.0;
+            if (k < Nc) {
+                v = k0 * xa0[k] * xb0[k] + k1 * xa1[k] * xb1[k];
+            } else if (k < 2 * Nc) {
+                const long long i = k - Nc;
+                v = 0.5 * (k0 * (xa0[i] * gb0[i] + xb0[i] * ga0[i]) + k1 * (xa1[i] * gb1[i] + xb1[i] * ga1[i]));
+            }
+            store_split(fmt, hi, lo, c * N2pc + k, v);
+        }
+    }
+}
+
+// XGq (2Nc x Kmq): mode components of x (rows < Nc) and g
+__global__ void build_XGq_kernel(const double *__restrict__ X, const double *__restrict__ G, int n, long long Nc, int Kmq,
+                                 const int *__restrict__ mode, const double *__restrict__ sign, Format fmt, void *hi, void *lo) {
+    const long long total = 2 * Nc * Kmq;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+        const long long k = idx / Kmq;
+        const int c = (int)(idx - k * Kmq);
+        const double v = k < Nc ? X[k * n + mode[c]] : G[(k - Nc) * n + mode[c]];
+        store_split(fmt, hi, lo, idx, sign[c] * v);
+    }
+}
+
+// YXq (Kmq x N2pc): mode components of y (columns < Nc) and of x~, zero past 2Nc
+__global__ void build_YXq_kernel(const double *__restrict__ Y, const double *__restrict__ Xt, int n, long long Nc, long long N2pc,
+                                 int Kmq, const int *__restrict__ mode, const double *__restrict__ sign, Format fmt, void *hi,
+                                 void *lo) {
+    const long long total = (long long)Kmq * N2pc;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+        const long long c = idx / N2pc, k = idx - c * N2pc;
+        double v = 0.0;
+        if (k < Nc) v = Y[k * n + mode[c]];
+        else if (k < 2 * Nc) v = Xt[(k - Nc) * n + mode[c]];
+        store_split(fmt, hi, lo, idx, sign[c] * v);
+    }
+}
+
+// Lab rows r (real parts) and NR + r (imaginary parts) from the representatives' U rows
+template <typename InT>
+__global__ void left_ab_kernel(int NR, int n, int Kq, const InT *__restrict__ U, long long ldu, const int *__restrict__ mu0,
+                               const int *__restrict__ nu0, const int *__restrict__ mu1, const int *__restrict__ nu1,
+                               const double *__restrict__ c0, const double *__restrict__ c1, const int *__restrict__ partner,
+                               const double *__restrict__ re, const double *__restrict__ im, Format fmt, void *hi, void *lo) {
+    for (long long r = blockIdx.y; r < NR; r += gridDim.y) {
+        const InT *u = U + r * ldu;
+        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Kq; c += gridDim.x * blockDim.x) {
+            const double own = c0[c] * (double)u[packed_of(mu0[c], nu0[c], n)] + c1[c] * (double)u[packed_of(mu1[c], nu1[c], n)];
+            const int pc = partner[c];
+            double oth = 0.0;
+            if (pc >= 0 && im[c] != 0.0)
+                oth = c0[pc] * (double)u[packed_of(mu0[pc], nu0[pc], n)] + c1[pc] * (double)u[packed_of(mu1[pc], nu1[pc], n)];
+            store_split(fmt, hi, lo, r * Kq + c, re[c] * own);
+            store_split(fmt, hi, lo, (NR + r) * Kq + c, im[c] * oth);
+        }
+    }
+}
+
+template <typename InT>
+__global__ void left_cd_kernel(int NR, int Kmq, const InT *__restrict__ r1p, long long ldr, const int *__restrict__ mode,
+                               const double *__restrict__ sign, const int *__restrict__ partner, const double *__restrict__ re,
+                               const double *__restrict__ im, Format fmt, void *hi, void *lo) {
+    const long long total = (long long)NR * Kmq;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / Kmq;
+        const int c = (int)(idx - r * Kmq);
+        const InT *v = r1p + r * ldr;
+        const double own = sign[c] * (double)v[mode[c]];
+        const int pc = partner[c];
+        const double oth = (pc >= 0 && im[c] != 0.0) ? sign[pc] * (double)v[mode[pc]] : 0.0;
+        store_split(fmt, hi, lo, r * Kmq + c, re[c] * own);
+        store_split(fmt, hi, lo, (NR + r) * Kmq + c, im[c] * oth);
+    }
+}
+
+template <typename AccT>
+__device__ __forceinline__ double own_out(const AccT *o1, const AccT *o2, int c, const int *partner, const double *zc) {
+    double v = (double)o1[c];
+    const double z = zc[c];
+    if (z != 0.0) v += z * (double)o2[partner[c]];
+    return v;
+}
+
+template <typename AccT>
+__global__ void recon_z_kernel(int NR, long long P, int Kq, const AccT *__restrict__ O, const int *__restrict__ pmu,
+                               const int *__restrict__ pnu, const int *__restrict__ col0, const int *__restrict__ col1,
+                               const double *__restrict__ pc0, const double *__restrict__ pc1, const int *__restrict__ partner,
+                               const double *__restrict__ zc, AccT *__restrict__ Zs, long long ldz) {
+    for (long long r = blockIdx.y; r < NR; r += gridDim.y) {
+        const AccT *o1 = O + r * Kq, *o2 = O + (NR + r) * Kq;
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+            double v = pc0[p] * own_out(o1, o2, col0[p], partner, zc);
+            const double k1 = pc1[p];
+            if (k1 != 0.0) v += k1 * own_out(o1, o2, col1[p], partner, zc);
+            Zs[r * ldz + p] = (AccT)((pmu[p] == pnu[p] ? 1.0 : 2.0) * v);
+        }
+    }
+}
+
+template <typename AccT>
+__global__ void recon_f_kernel(int NR, int n, int Kmq, const AccT *__restrict__ OF, const int *__restrict__ mode_col,
+                               const double *__restrict__ sign, const int *__restrict__ partner, const double *__restrict__ zc,
+                               AccT *__restrict__ Fs, long long ldf) {
+    const long long total = (long long)NR * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+        const long long r = idx / n;
+        const int m = (int)(idx - r * n);
+        const int c = mode_col[m];
+        double v = 0.0;
+        if (c >= 0) v = sign[c] * own_out(OF + r * Kmq, OF + (NR + r) * Kmq, c, partner, zc);
+        Fs[r * ldf + m] = (AccT)v;
+    }
+}
+
+}  // namespace
+
+int freq_tables_create(const FreqLayout &L, FreqTables **out) {
+    *out = nullptr;
+    auto *t = new FreqTables();
+    t->n_class = L.n_class;
+    t->Kq = L.Kq;
+    t->Kmq = L.Kmq;
+    t->cls_real = L.cls_real;
+    t->pcol_off = L.pcol_off;
+    t->pcol_cnt = L.pcol_cnt;
+    t->mcol_off = L.mcol_off;
+    t->mcol_cnt = L.mcol_cnt;
+    t->flops_ratio = L.flops_ratio;
+    size_t acc = 0;
+    int rc = 0;
+    if ((rc = upload(L.pc_mu0, &t->pc_mu0, &acc)) || (rc = upload(L.pc_nu0, &t->pc_nu0, &acc)) ||
+        (rc = upload(L.pc_mu1, &t->pc_mu1, &acc)) || (rc = upload(L.pc_nu1, &t->pc_nu1, &acc)) ||
+        (rc = upload(L.pc_partner, &t->pc_partner, &acc)) || (rc = upload(L.pc_c0, &t->pc_c0, &acc)) ||
+        (rc = upload(L.pc_c1, &t->pc_c1, &acc)) || (rc = upload(L.pc_re, &t->pc_re, &acc)) ||
+        (rc = upload(L.pc_im, &t->pc_im, &acc)) || (rc = upload(L.pc_zc, &t->pc_zc, &acc)) ||
+        (rc = upload(L.pp_col0, &t->pp_col0, &acc)) || (rc = upload(L.pp_col1, &t->pp_col1, &acc)) ||
+        (rc = upload(L.pp_c0, &t->pp_c0, &acc)) || (rc = upload(L.pp_c1, &t->pp_c1, &acc)) ||
+        (rc = upload(L.mc_mode, &t->mc_mode, &acc)) || (rc = upload(L.mc_partner, &t->mc_partner, &acc)) ||
+        (rc = upload(L.mode_col, &t->mode_col, &acc)) || (rc = upload(L.mc_sign, &t->mc_sign, &acc)) ||
+        (rc = upload(L.mc_re, &t->mc_re, &acc)) || (rc = upload(L.mc_im, &t->mc_im, &acc)) ||
+        (rc = upload(L.mc_zc, &t->mc_zc, &acc))) {
+        freq_tables_destroy(t);
+        return rc;
+    }
+    t->bytes = acc;
+    *out = t;
+    return 0;
+}
+
+void freq_tables_destroy(FreqTables *t) {
+    if (!t) return;
+    void *ps[] = {t->pc_mu0, t->pc_nu0, t->pc_mu1, t->pc_nu1, t->pc_partner, t->pc_c0, t->pc_c1, t->pc_re, t->pc_im, t->pc_zc,
+                  t->pp_col0, t->pp_col1, t->pp_c0, t->pp_c1, t->mc_mode, t->mc_partner, t->mode_col, t->mc_sign, t->mc_re,
+                  t->mc_im, t->mc_zc};
+    for (void *p : ps)
+        if (p) cudaFree(p);
+    delete t;
+}
+
+size_t freq_operand_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo) {
+    const long long N2pc = round_up(2 * Nc, 64);
+    const size_t per = (size_t)(2 * Nc * t.Kq + (long long)t.Kq * N2pc + 2 * Nc * t.Kmq + (long long)t.Kmq * N2pc);
+    return per * format_bytes(fmt) * (lo ? 2 : 1) + 8 * 256;
+}
+
+int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt,
+                        const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
+                        cudaStream_t st) {
+    const size_t es = format_bytes(fmt);
+    const long long N2pc = round_up(2 * Nc, 64);
+    const long long nV = 2 * Nc * t.Kq, nVT = (long long)t.Kq * N2pc, nXG = 2 * Nc * t.Kmq, nYX = (long long)t.Kmq * N2pc;
+    uint8_t *b = static_cast<uint8_t *>(buf);
+    size_t off = 0;
+    auto take = [&](long long count) { void *p = b + off; off += ((size_t)count * es + 255) / 256 * 256; return p; };
+    o = FreqOps();
+    o.V_hi = take(nV);
+    o.VT_hi = take(nVT);
+    o.XG_hi = take(nXG);
+    o.YX_hi = take(nYX);
+    if (lo) {
+        o.V_lo = take(nV);
+        o.VT_lo = take(nVT);
+        o.XG_lo = take(nXG);
+        o.YX_lo = take(nYX);
+    }
+    build_Vq_kernel<<<grid_rows(t.Kq, 2 * Nc), 256, 0, st>>>(X, G, n, Nc, t.Kq, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0,
+                                                             t.pc_c1, fmt, o.V_hi, o.V_lo);
+    build_VqT_kernel<<<grid_rows(N2pc, t.Kq), 256, 0, st>>>(XGT, ldT, n, Nc, N2pc, t.Kq, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1,
+                                                            t.pc_c0, t.pc_c1, fmt, o.VT_hi, o.VT_lo);
+    build_XGq_kernel<<<grid1(nXG), 256, 0, st>>>(X, G, n, Nc, t.Kmq, t.mc_mode, t.mc_sign, fmt, o.XG_hi, o.XG_lo);
+    build_YXq_kernel<<<grid1(nYX), 256, 0, st>>>(Y, Xt, n, Nc, N2pc, t.Kmq, t.mc_mode, t.mc_sign, fmt, o.YX_hi, o.YX_lo);
+    TD_CUDA(cudaGetLastError());
+    o.built = true;
+    o.has_lo = lo;
+    o.bytes = off;
+    return 0;
+}
+
+template <typename InT>
+int freq_left(const FreqTables &t, int NR, int n, const InT *U, long long ldu, const InT *r1p, long long ldr, Format fmt,
+              void *Lab_hi, void *Lab_lo, void *Lcd_hi, void *Lcd_lo, cudaStream_t st) {
+    left_ab_kernel<InT><<<grid_rows(t.Kq, NR), 256, 0, st>>>(NR, n, t.Kq, U, ldu, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0,
+                                                             t.pc_c1, t.pc_partner, t.pc_re, t.pc_im, fmt, Lab_hi, Lab_lo);
+    if (t.Kmq > 0)
+        left_cd_kernel<InT><<<grid1((long long)NR * t.Kmq), 256, 0, st>>>(NR, t.Kmq, r1p, ldr, t.mc_mode, t.mc_sign, t.mc_partner,
+                                                                         t.mc_re, t.mc_im, fmt, Lcd_hi, Lcd_lo);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename AccT>
+int freq_reconstruct(const FreqTables &t, int NR, int n, long long P, const int *pmu, const int *pnu, const AccT *O,
+                     const AccT *OF, AccT *Zs, long long ldz, AccT *Fs, long long ldf, cudaStream_t st) {
+    recon_z_kernel<AccT><<<grid_rows(P, NR), 256, 0, st>>>(NR, P, t.Kq, O, pmu, pnu, t.pp_col0, t.pp_col1, t.pp_c0, t.pp_c1,
+                                                           t.pc_partner, t.pc_zc, Zs, ldz);
+    recon_f_kernel<AccT><<<grid1((long long)NR * n), 256, 0, st>>>(NR, n, t.Kmq, OF, t.mode_col, t.mc_sign, t.mc_partner,
+                                                                    t.mc_zc, Fs, ldf);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template int freq_left<float>(const FreqTables &, int, int, const float *, long long, const float *, long long, Format, void *,
+                              void *, void *, void *, cudaStream_t);
+template int freq_left<double>(const FreqTables &, int, int, const double *, long long, const double *, long long, Format,
+                               void *, void *, void *, void *, cudaStream_t);
+template int freq_reconstruct<float>(const FreqTables &, int, int, long long, const int *, const int *, const float *,
+                                     const float *, float *, long long, float *, long long, cudaStream_t);
+template int freq_reconstruct<double>(const FreqTables &, int, int, long long, const int *, const int *, const double *,
+                                      const double *, double *, long long, double *, long long, cudaStream_t);
+
+}  // namespace tdscha

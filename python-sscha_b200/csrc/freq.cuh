@@ -1,0 +1,106 @@
+// freq.cuh -- the two big contractions of the averages over the characters of the subgroup K.
+//
+// On the factorised symmetry path every symmetry is S_j = S_p D_t (p a coset representative, D_t in
+// the abelian subgroup K, 2 x 2 sparse in the rotated basis), and the per-row quantities only enter
+// through
+//     a_(p,t),i = <U_p, D_t M_i D_t^T>_F,   U_p = S_p^T Ys S_p,   M_i = x_i x_i^T or sym(x_i g_i^T)
+//     c_(p,t),i = r1_p . D_t x_i            (and b, d with g_i)
+//     N~_p = sum_t D_t (sum_i w_(p,t),i M_i) D_t^T,   F~_p = sum_t D_t (sum_i w'_(p,t),i v_i).
+// In the rotated basis symmetric matrices decompose into components xi_k, each a real number or a
+// complex number (a 2 x 2 block's linear / antilinear part, or a real mode times a complex pair)
+// that D_t multiplies by a character chi(t) of K.  Grouping the components by character class
+// (chi and its conjugate; the stored "canonical" component is conjugated where needed):
+//     a_(p,t) = sum_K Re( conj(chi_K(t)) H_K ),   H_K = sum_{k in K} m_k u_k conj(xi_k(M_i))
+// (m_k the Frobenius multiplicity of the component) and, because every weight is linear in a, b, c,
+// d with per-configuration coefficients, the weights' transforms over t are
+//     sum_t a_(p,t) chi_K(t) = s_K H_K,   s_K = |K| / 2 (complex class) or |K| Re (real class),
+// so the weights can be formed class by class without ever leaving the character basis, and
+//     xi_k(N~_p) = sum_i w^_K,i xi_k(M_i),     the same for the mode components of F~_p.
+// Each character class is one contraction over only its own components: the two big contractions
+// shrink from N_sym rows x all P pairs to (2 x cosets) rows per class x the class's pairs, about
+// |K| / 2 times fewer flops.  Layouts (NR = nb x cosets in the chunk):
+//   pair columns: the P components (complex ones as a real and an imaginary column) sorted by
+//     class, each class padded to a multiple of 64 columns (Kq in all);
+//   mode columns: the n mode components (complex orbits as two columns) by class, padded (Kmq);
+//   left operands / outputs: rows (comp, v, c) = comp * NR + v * ncos + c, comp 0 the real part.
+#pragma once
+#include <vector>
+#include "common.cuh"
+#include "cosets.cuh"
+
+namespace tdscha {
+
+// Host description of the character classes and the component layouts.
+struct FreqLayout {
+    bool ok = false;
+    int n_class = 0, Kq = 0, Kmq = 0;
+    std::vector<int> cls_real;                        // class is a real character
+    std::vector<int> pcol_off, pcol_cnt;              // pair columns of each class (padded)
+    std::vector<int> mcol_off, mcol_cnt;              // mode columns of each class (padded; 0 when none)
+    // per pair column: own value = c0 M[mu0, nu0] + c1 M[mu1, nu1] of a symmetric matrix M
+    std::vector<int> pc_mu0, pc_nu0, pc_mu1, pc_nu1;
+    std::vector<double> pc_c0, pc_c1;
+    std::vector<int> pc_partner;                      // the other column of a complex component (-1: none)
+    std::vector<double> pc_re, pc_im;                 // left rows: Re = pc_re own(c), Im = pc_im own(partner)
+    std::vector<double> pc_zc;                        // output: own(c) = O1[c] + pc_zc O2[partner]
+    // per packed pair (mu <= nu): N~[mu, nu] = pp_c0 own(pp_col0) + pp_c1 own(pp_col1)
+    std::vector<int> pp_col0, pp_col1;
+    std::vector<double> pp_c0, pp_c1;
+    // per mode column: own value of a mode vector v = mc_sign v[mc_mode]
+    std::vector<int> mc_mode, mc_partner;
+    std::vector<double> mc_sign, mc_re, mc_im, mc_zc;
+    std::vector<int> mode_col;                        // column of each mode
+    double flops_ratio = 0;                           // big-contraction work relative to all symmetries
+};
+
+// Classes and layouts from the analysis of the symmetry tables (sym_blocks as given, host).
+int build_freq_layout(int n, const std::vector<int> &dim, const std::vector<int> &blk_start, const double *const *sym_blocks,
+                      const CosetAnalysis &ca, FreqLayout &out);
+
+// Device copy of the layout tables.
+struct FreqTables {
+    int n_class = 0, Kq = 0, Kmq = 0;
+    std::vector<int> cls_real, pcol_off, pcol_cnt, mcol_off, mcol_cnt;
+    int *pc_mu0 = nullptr, *pc_nu0 = nullptr, *pc_mu1 = nullptr, *pc_nu1 = nullptr, *pc_partner = nullptr;
+    double *pc_c0 = nullptr, *pc_c1 = nullptr, *pc_re = nullptr, *pc_im = nullptr, *pc_zc = nullptr;
+    int *pp_col0 = nullptr, *pp_col1 = nullptr;
+    double *pp_c0 = nullptr, *pp_c1 = nullptr;
+    int *mc_mode = nullptr, *mc_partner = nullptr, *mode_col = nullptr;
+    double *mc_sign = nullptr, *mc_re = nullptr, *mc_im = nullptr, *mc_zc = nullptr;
+    double flops_ratio = 0;
+    size_t bytes = 0;
+};
+int freq_tables_create(const FreqLayout &L, FreqTables **out);
+void freq_tables_destroy(FreqTables *t);
+
+// Per-ensemble operands in the character basis, one storage format (hi, lo):
+//   Vq  (2Nc x Kq):  [xi(x x^T) ; xi(sym(x g^T))] rows per configuration
+//   VqT (Kq x N2pc): the same transposed (zero columns past 2Nc)
+//   XGq (2Nc x Kmq): [mode components of x ; of g]
+//   YXq (Kmq x N2pc): [mode components of y | of x~] transposed
+struct FreqOps {
+    bool built = false, has_lo = false;
+    void *V_hi = nullptr, *V_lo = nullptr, *VT_hi = nullptr, *VT_lo = nullptr;
+    void *XG_hi = nullptr, *XG_lo = nullptr, *YX_hi = nullptr, *YX_lo = nullptr;
+    size_t bytes = 0;
+};
+size_t freq_operand_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo);
+// Operands of configurations [c0, c0 + Nc) into caller-provided storage `buf` (freq_operand_bytes).
+// X, G, Y, Xt: (N x n) rotated-basis ensemble (row c0 first); XGT: [X^T; G^T] (2n x ldT).
+int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt,
+                        const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
+                        cudaStream_t st);
+
+// Left operands from the representatives' transforms (InT float or double):
+//   Lab (2 NR x Kq) from U (NR x ldu, packed pairs), Lcd (2 NR x Kmq) from r1p (NR x ldr).
+template <typename InT>
+int freq_left(const FreqTables &t, int NR, int n, const InT *U, long long ldu, const InT *r1p, long long ldr, Format fmt,
+              void *Lab_hi, void *Lab_lo, void *Lcd_hi, void *Lcd_lo, cudaStream_t st);
+
+// Back from the character basis: Zs (NR x ldz, packed c_p N~) from O (2 NR x Kq), Fs (NR x ldf)
+// from OF (2 NR x Kmq).
+template <typename AccT>
+int freq_reconstruct(const FreqTables &t, int NR, int n, long long P, const int *pmu, const int *pnu, const AccT *O,
+                     const AccT *OF, AccT *Zs, long long ldz, AccT *Fs, long long ldf, cudaStream_t st);
+
+}  // namespace tdscha

@@ -170,6 +170,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Sub-problems of one launch (a single contraction is one group): tile0 = tiles of the groups before.
+constexpr int MAX_GROUPS = 64;
+struct DevGroup {
+    int M, N, K, a_row, a_k, b_row, b_k, tile0, num_m, num_n;
+    long long d_off;
+};
+struct GroupTable {
+    int n, total_tiles;
+    DevGroup g[MAX_GROUPS];
+};
+
+__device__ __forceinline__ const DevGroup &group_of(const GroupTable &gt, int t) {
+    int g = 0;
+    while (g + 1 < gt.n && gt.g[g + 1].tile0 <= t) ++g;
+    return gt.g[g];
+}
+
 // Tile order of the persistent schedule: groups of `gm` M-tiles, N-tiles of a group in turn, M
 // fastest inside a group.  The ~148 tiles in flight then form a gm x (148/gm) block that shares its
 // A rows and B rows through L2, instead of one N column of tiles streaming all of A from HBM.
@@ -204,7 +221,7 @@ template <int BN, int STAGES, bool TF32, int NPROD>
 __global__ void __launch_bounds__(NUM_THREADS, 1)
 tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
-               int M, int N, int K, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err,
+               const __grid_constant__ GroupTable gt, int drain, int group_m, float *__restrict__ D, long long ldd, unsigned *err,
                unsigned *tile_sync, unsigned sync_ns, int accumulate, unsigned long long wait_ns, int stall) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     extern __shared__ uint8_t smem_raw[];
@@ -219,10 +236,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
-    const int num_kb = K / C::K_ELEMS;
-    const int num_m = (M + BM - 1) / BM, num_n = (N + BN - 1) / BN;
-    const int num_tiles = num_m * num_n;
-    const int chunks_per_tile = (num_kb + drain - 1) / drain;
+    const int num_tiles = gt.total_tiles;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -257,9 +271,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         for (int t = blockIdx.x, round = 0; t < num_tiles && !*abort_flag; t += gridDim.x, ++round) {
             target += (unsigned)min((int)gridDim.x, num_tiles - round * (int)gridDim.x);
             if (tile_sync) tile_start_sync(tile_sync, target, round > 0 ? sync_ns : 0ull);
+            const DevGroup &G = group_of(gt, t);
             int mb, nbk;
-            tile_coords(t, num_m, num_n, group_m, mb, nbk);
-            const int m0 = mb * BM, n0 = nbk * BN;
+            tile_coords(t - G.tile0, G.num_m, G.num_n, group_m, mb, nbk);
+            const int m0 = G.a_row + mb * BM, n0 = G.b_row + nbk * BN;
+            const int num_kb = G.K / C::K_ELEMS;
             for (int kb = 0; kb < num_kb; ++kb, ++g) {
                 const int s = (int)(g % STAGES);
                 const uint32_t ph = (uint32_t)(g / STAGES) & 1u;
@@ -268,11 +284,11 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
                 const uint32_t full = smem_u32(&bars[s]);
                 mbar_expect_tx(full, C::STAGE_BYTES);
                 const int kc = kb * C::K_ELEMS;
-                tma_load_2d(smem_u32(st), &tmA_hi, kc, m0, full);
-                tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES), &tmB_hi, kc, n0, full);
+                tma_load_2d(smem_u32(st), &tmA_hi, G.a_k + kc, m0, full);
+                tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES), &tmB_hi, G.b_k + kc, n0, full);
                 if constexpr (NPROD == 3) {
-                    tma_load_2d(smem_u32(st + C::A_BYTES), &tmA_lo, kc, m0, full);
-                    tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES), &tmB_lo, kc, n0, full);
+                    tma_load_2d(smem_u32(st + C::A_BYTES), &tmA_lo, G.a_k + kc, m0, full);
+                    tma_load_2d(smem_u32(st + C::NOPS * C::A_BYTES + C::B_BYTES), &tmB_lo, G.b_k + kc, n0, full);
                 }
                 issued = g + 1;
             }
@@ -283,6 +299,8 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         long long g = 0, ch = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+            const int num_kb = group_of(gt, t).K / C::K_ELEMS;
+            const int chunks_per_tile = (num_kb + drain - 1) / drain;
             for (int c = 0; c < chunks_per_tile && ok; ++c, ++ch) {
                 const int X = (int)(ch & 1);
                 const uint32_t use = (uint32_t)(ch >> 1);
@@ -326,9 +344,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         long long ch = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+            const DevGroup &G = group_of(gt, t);
             int mb, nbk;
-            tile_coords(t, num_m, num_n, group_m, mb, nbk);
+            tile_coords(t - G.tile0, G.num_m, G.num_n, group_m, mb, nbk);
             const int m0 = mb * BM, n0 = nbk * BN;
+            const int M = G.M, N = G.N;
+            const int chunks_per_tile = (G.K / C::K_ELEMS + drain - 1) / drain;
             float acc[C::EPI_COLS];
 #pragma unroll
             for (int i = 0; i < C::EPI_COLS; ++i) acc[i] = 0.f;
@@ -352,12 +373,12 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
             if (!ok) break;
             const long long grow = (long long)m0 + row;
             if (grow < M) {
-                float *drow = D + grow * ldd;
+                float *drow = D + G.d_off + grow * ldd;
                 const int cb0 = n0 + half * C::EPI_COLS;
 #pragma unroll
                 for (int v = 0; v < C::EPI_COLS / 4; ++v) {
                     const int cb = cb0 + 4 * v;
-                    if (cb + 4 <= N && ((ldd & 3) == 0)) {
+                    if (cb + 4 <= N && ((ldd & 3) == 0) && ((G.d_off & 3) == 0)) {
                         float4 o = make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
                         if (accumulate) {
                             const float4 old = *reinterpret_cast<const float4 *>(drow + cb);
@@ -454,8 +475,9 @@ static int default_drain(int nprod) {
 // Autotuner key: one choice per (format, products, M, N, K, device).
 struct TuneKey {
     int tf32, nprod, M, N, K, dev;
+    unsigned long long shape;   // hash of the sub-problems' shapes of a grouped launch (0: one problem)
     bool operator<(const TuneKey &o) const {
-        return std::tie(tf32, nprod, M, N, K, dev) < std::tie(o.tf32, o.nprod, o.M, o.N, o.K, o.dev);
+        return std::tie(tf32, nprod, M, N, K, dev, shape) < std::tie(o.tf32, o.nprod, o.M, o.N, o.K, o.dev, o.shape);
     }
 };
 static std::mutex g_tune_mutex;
@@ -497,39 +519,61 @@ struct Prepared {
     long long tiles = 0;
 };
 
+// Extents of the two operand buffers and the sub-problems of one contraction.
+struct Problem {
+    long long a_rows, a_cols, b_rows, b_cols;
+    std::vector<GemmGroup> groups;
+};
+
 template <int BN, int STAGES, bool TF32, int NPROD>
-static int prepare_cfg(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err,
-                       unsigned *counter, int stall, Prepared *out) {
+static int prepare_cfg(const GemmOperands &op, const Problem &pb, size_t g0, size_t g1, float *D, long long ldd,
+                       cudaStream_t st, unsigned *err, unsigned *counter, int stall, Prepared *out) {
     using C = Cfg<BN, STAGES, TF32, NPROD>;
     CUtensorMap a_hi, a_lo, b_hi, b_lo;
-    TD_TRY(make_map(&a_hi, op.A_hi, TF32, M, K, op.lda, BM));
-    TD_TRY(make_map(&b_hi, op.B_hi, TF32, N, K, op.ldb, BN));
+    TD_TRY(make_map(&a_hi, op.A_hi, TF32, pb.a_rows, pb.a_cols, op.lda, BM));
+    TD_TRY(make_map(&b_hi, op.B_hi, TF32, pb.b_rows, pb.b_cols, op.ldb, BN));
     if (NPROD == 3) {
-        TD_TRY(make_map(&a_lo, op.A_lo, TF32, M, K, op.lda, BM));
-        TD_TRY(make_map(&b_lo, op.B_lo, TF32, N, K, op.ldb, BN));
+        TD_TRY(make_map(&a_lo, op.A_lo, TF32, pb.a_rows, pb.a_cols, op.lda, BM));
+        TD_TRY(make_map(&b_lo, op.B_lo, TF32, pb.b_rows, pb.b_cols, op.ldb, BN));
     } else {
         a_lo = a_hi;
         b_lo = b_hi;
     }
+    GroupTable gt{};
+    gt.n = (int)(g1 - g0);
+    long long tiles = 0;
+    int max_m = 1;
+    for (size_t i = g0; i < g1; ++i) {
+        const GemmGroup &q = pb.groups[i];
+        DevGroup &d = gt.g[i - g0];
+        d.M = q.M; d.N = q.N; d.K = q.K;
+        d.a_row = q.a_row; d.a_k = q.a_k; d.b_row = q.b_row; d.b_k = q.b_k;
+        d.d_off = q.d_off;
+        d.num_m = ceil_div(q.M, BM);
+        d.num_n = ceil_div(q.N, BN);
+        d.tile0 = (int)tiles;
+        tiles += (long long)d.num_m * d.num_n;
+        max_m = std::max(max_m, d.num_m);
+    }
+    TD_CHECK(tiles < (1LL << 31), TDSCHA_EINVAL, "tc::gemm: %lld tiles exceed the schedule", tiles);
+    gt.total_tiles = (int)tiles;
     auto kern = tc_gemm_kernel<BN, STAGES, TF32, NPROD>;
     TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, C::SMEM_BYTES));
     int dev = 0, sms = 148;
     TD_CUDA(cudaGetDevice(&dev));
     TD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    const long long tiles = (long long)ceil_div(M, BM) * ceil_div(N, BN);
-    const int num_kb = K / C::K_ELEMS;
-    const int drain = op.drain_kb > 0 ? std::min(op.drain_kb, num_kb) : std::min(default_drain(NPROD), num_kb);
+    const int drain = op.drain_kb > 0 ? op.drain_kb : default_drain(NPROD);
     const dim3 grid((unsigned)std::min<long long>(tiles, sms));
     const unsigned sync_ns = tile_sync_budget_ns();
     const int accumulate = op.accumulate ? 1 : 0;
     const unsigned long long wait_ns = g_wait_budget_ns.load();
     unsigned *cnt = (sync_ns > 0 && tiles > grid.x) ? counter : nullptr;
-    out->num_m = ceil_div(M, BM);
+    out->num_m = max_m;
     out->bn = BN;
     out->tiles = tiles;
     out->launch = [=](int gm) {
         if (cnt) cudaMemsetAsync(cnt, 0, sizeof(unsigned), st);
-        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, M, N, K, drain, gm, D, ldd, err, cnt, sync_ns,
+        kern<<<grid, NUM_THREADS, C::SMEM_BYTES, st>>>(a_hi, a_lo, b_hi, b_lo, gt, drain, gm, D, ldd, err, cnt, sync_ns,
                                                         accumulate, wait_ns, stall);
     };
     return 0;
@@ -547,8 +591,8 @@ static int prepare_cfg(const GemmOperands &op, int M, int N, int K, float *D, lo
 // m-fastest order; TDSCHA_TILE_N (256 | 128) and TDSCHA_GROUP_M fix the choice.
 static std::map<TuneKey, std::pair<int, int>> g_tune_cfg;
 
-static int choose(int tf32, int nprod, int M, int N, int K, const Prepared *cfgs, int ncfg, cudaStream_t st, bool allow_trials,
-                  int *cfg_out, int *gm_out) {
+static int choose(int tf32, int nprod, int M, int N, int K, unsigned long long shape, const Prepared *cfgs, int ncfg,
+                  cudaStream_t st, bool allow_trials, int *cfg_out, int *gm_out) {
     int dev = 0, sms = 148;
     TD_CUDA(cudaGetDevice(&dev));
     TD_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
@@ -561,7 +605,7 @@ static int choose(int tf32, int nprod, int M, int N, int K, const Prepared *cfgs
         *gm_out = env_gm ? std::max(1, std::min(cfgs[c].num_m, atoi(env_gm))) : cfgs[c].num_m;
         return 0;
     }
-    const TuneKey key{tf32, nprod, M, N, K, dev};
+    const TuneKey key{tf32, nprod, M, N, K, dev, shape};
     {
         std::lock_guard<std::mutex> lock(g_tune_mutex);
         auto it = g_tune_cfg.find(key);
@@ -621,7 +665,7 @@ static int choose(int tf32, int nprod, int M, int N, int K, const Prepared *cfgs
 }
 
 template <bool TF32, int NPROD>
-static int launch_tuned(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+static int launch_tuned(const GemmOperands &op, const Problem &pb, float *D, long long ldd, cudaStream_t st, unsigned *err) {
     constexpr int S_WIDE = NPROD == 3 ? 2 : 4, S_NARROW = NPROD == 3 ? 3 : 6;
     int dev = 0;
     TD_CUDA(cudaGetDevice(&dev));
@@ -631,23 +675,47 @@ static int launch_tuned(const GemmOperands &op, int M, int N, int K, float *D, l
     unsigned *counter = nullptr;
     if (tile_sync_budget_ns() > 0) TD_TRY(tile_sync_counter(dev, st, capturing, &counter));
     const int stall = g_stall_next.exchange(0);
-    Prepared cfgs[2];
-    TD_TRY((prepare_cfg<256, S_WIDE, TF32, NPROD>(op, M, N, K, D, ldd, st, err, counter, stall, &cfgs[0])));
-    TD_TRY((prepare_cfg<128, S_NARROW, TF32, NPROD>(op, M, N, K, D, ldd, st, err, counter, stall, &cfgs[1])));
-    int c = 0, gm = cfgs[0].num_m;
-    if (!stall) {   // abort-path test: one launch of the wide tile, no tuning trials
-        // trial runs write D, so an accumulating launch only reuses a choice tuned earlier (and a
-        // launch being captured into a CUDA graph runs nothing, so it cannot time trials)
-        TD_TRY(choose(TF32 ? 1 : 0, NPROD, M, N, K, cfgs, 2, st, !op.accumulate && !capturing, &c, &gm));
+    for (size_t g0 = 0; g0 < pb.groups.size(); g0 += MAX_GROUPS) {
+        const size_t g1 = std::min(pb.groups.size(), g0 + MAX_GROUPS);
+        Prepared cfgs[2];
+        TD_TRY((prepare_cfg<256, S_WIDE, TF32, NPROD>(op, pb, g0, g1, D, ldd, st, err, counter, stall, &cfgs[0])));
+        TD_TRY((prepare_cfg<128, S_NARROW, TF32, NPROD>(op, pb, g0, g1, D, ldd, st, err, counter, stall, &cfgs[1])));
+        // tuning key: the one problem's shape, or the groups' shapes hashed (FNV-1a)
+        int kM = pb.groups[g0].M, kN = pb.groups[g0].N, kK = pb.groups[g0].K;
+        unsigned long long shape = 0;
+        if (g1 - g0 > 1) {
+            shape = 1469598103934665603ull;
+            for (size_t i = g0; i < g1; ++i)
+                for (long long v : {(long long)pb.groups[i].M, (long long)pb.groups[i].N, (long long)pb.groups[i].K}) {
+                    shape ^= (unsigned long long)v;
+                    shape *= 1099511628211ull;
+                }
+            kM = (int)(g1 - g0);
+        }
+        int c = 0, gm = cfgs[0].num_m;
+        if (!stall) {   // abort-path test: one launch of the wide tile, no tuning trials
+            // trial runs write D, so an accumulating launch only reuses a choice tuned earlier (and a
+            // launch being captured into a CUDA graph runs nothing, so it cannot time trials)
+            TD_TRY(choose(TF32 ? 1 : 0, NPROD, kM, kN, kK, shape, cfgs, 2, st, !op.accumulate && !capturing, &c, &gm));
+        }
+        cfgs[c].launch(gm);
+        TD_CUDA(cudaGetLastError());
     }
-    cfgs[c].launch(gm);
-    TD_CUDA(cudaGetLastError());
     return 0;
 }
 
 void set_wait_budget_ns(unsigned long long ns) { g_wait_budget_ns.store(ns); }
 unsigned long long wait_budget_ns() { return g_wait_budget_ns.load(); }
 void stall_next_launch() { g_stall_next.store(1); }
+
+static int dispatch(const GemmOperands &op, const Problem &pb, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+    if (op.fmt == FMT_TF32) {
+        if (op.nprod == 3) return launch_tuned<true, 3>(op, pb, D, ldd, st, err);
+        return launch_tuned<true, 1>(op, pb, D, ldd, st, err);
+    }
+    if (op.nprod == 3) return launch_tuned<false, 3>(op, pb, D, ldd, st, err);
+    return launch_tuned<false, 1>(op, pb, D, ldd, st, err);
+}
 
 int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, cudaStream_t st, unsigned *err) {
     TD_CHECK(M > 0 && N > 0 && K > 0, TDSCHA_EINVAL, "tc::gemm: empty problem %d x %d x %d", M, N, K);
@@ -659,12 +727,34 @@ int gemm(const GemmOperands &op, int M, int N, int K, float *D, long long ldd, c
     TD_CHECK(op.lda >= K && op.ldb >= K && ldd >= N && op.lda < LD_MAX && op.ldb < LD_MAX && ldd < LD_MAX, TDSCHA_EINVAL,
              "tc::gemm: leading dimensions lda=%lld ldb=%lld ldd=%lld inconsistent with K=%d N=%d", op.lda, op.ldb, ldd, K, N);
     TD_CHECK(op.A_hi && op.B_hi && D && (op.nprod == 1 || (op.A_lo && op.B_lo)), TDSCHA_EINVAL, "tc::gemm: NULL operand");
-    if (tf32) {
-        if (op.nprod == 3) return launch_tuned<true, 3>(op, M, N, K, D, ldd, st, err);
-        return launch_tuned<true, 1>(op, M, N, K, D, ldd, st, err);
+    Problem pb{M, K, N, K, {GemmGroup{M, N, K, 0, 0, 0, 0, 0}}};
+    return dispatch(op, pb, D, ldd, st, err);
+}
+
+int gemm_grouped(const GemmOperands &op, long long a_rows, long long a_cols, long long b_rows, long long b_cols,
+                 const GemmGroup *groups, int n_groups, float *D, long long ldd, cudaStream_t st, unsigned *err) {
+    TD_CHECK(n_groups > 0 && groups, TDSCHA_EINVAL, "tc::gemm_grouped: no groups");
+    const bool tf32 = op.fmt == FMT_TF32;
+    TD_CHECK(op.fmt == FMT_TF32 || op.fmt == FMT_BF16, TDSCHA_EINVAL, "tc::gemm_grouped: operand format must be bf16 or tf32");
+    TD_CHECK(op.nprod == 1 || op.nprod == 3, TDSCHA_EINVAL, "tc::gemm_grouped: nprod must be 1 or 3");
+    const int kblk = tf32 ? 32 : 64;
+    constexpr long long LD_MAX = 1LL << 31;
+    TD_CHECK(op.lda >= a_cols && op.ldb >= b_cols && op.lda < LD_MAX && op.ldb < LD_MAX && ldd < LD_MAX && a_rows < LD_MAX &&
+                 b_rows < LD_MAX && a_cols < LD_MAX && b_cols < LD_MAX,
+             TDSCHA_EINVAL, "tc::gemm_grouped: operand extents inconsistent with their leading dimensions");
+    TD_CHECK(op.A_hi && op.B_hi && D && (op.nprod == 1 || (op.A_lo && op.B_lo)), TDSCHA_EINVAL, "tc::gemm_grouped: NULL operand");
+    Problem pb{a_rows, a_cols, b_rows, b_cols, {}};
+    for (int i = 0; i < n_groups; ++i) {
+        const GemmGroup &g = groups[i];
+        TD_CHECK(g.M > 0 && g.N > 0 && g.K > 0 && g.K % kblk == 0 && g.a_k % kblk == 0 && g.b_k % kblk == 0, TDSCHA_EINVAL,
+                 "tc::gemm_grouped: group %d: M=%d N=%d K=%d a_k=%d b_k=%d (K and offsets multiples of %d)", i, g.M, g.N, g.K,
+                 g.a_k, g.b_k, kblk);
+        TD_CHECK(g.a_row >= 0 && g.b_row >= 0 && g.a_row < a_rows && g.b_row < b_rows && g.a_k + (long long)g.K <= a_cols &&
+                     g.b_k + (long long)g.K <= b_cols && g.N <= ldd && g.d_off >= 0,
+                 TDSCHA_EINVAL, "tc::gemm_grouped: group %d outside its operands", i);
+        pb.groups.push_back(g);
     }
-    if (op.nprod == 3) return launch_tuned<false, 3>(op, M, N, K, D, ldd, st, err);
-    return launch_tuned<false, 1>(op, M, N, K, D, ldd, st, err);
+    return dispatch(op, pb, D, ldd, st, err);
 }
 
 }  // namespace tc

@@ -61,6 +61,9 @@ def load():
     lib.tdscha_ensemble_device_bytes.argtypes = [vp, ctypes.POINTER(ctypes.c_longlong)]
     lib.tdscha_ensemble_cosets.argtypes = [vp, ip, ip, ip, dp]
     lib.tdscha_symmetry_cosets.argtypes = [ctypes.c_int, ctypes.c_int, ip, ctypes.POINTER(dp), ip, ip, ip, ip, dp, dp]
+    lib.tdscha_ensemble_classes.argtypes = [vp, ip, ip, ip, dp]
+    lib.tdscha_symmetry_classes.argtypes = [ctypes.c_int, ctypes.c_int, ip, ctypes.POINTER(dp), ip, dp, ip, ip, dp, ip, dp,
+                                            ip, dp, ip]
     lib.tdscha_perturb_average_sym.argtypes = [vp, dp, dp, ctypes.c_int, ctypes.c_int, dp, dp]
     lib.tdscha_perturb_average_sym_device.argtypes = [vp, ctypes.c_int, vp, vp, ctypes.c_int, ctypes.c_int, vp, vp, vp]
     lib.tdscha_GetPerturbAverageSym.argtypes = [dp, dp, dp, dp, dp, dp, ctypes.c_double, ctypes.c_int, ctypes.c_int,
@@ -148,6 +151,11 @@ class DeviceEnsemble:
             self.close()
         except Exception:
             pass
+
+    def classes(self):
+        """dict(n_class, Kq, Kmq, flops_ratio) of the character-class contractions (n_class 0: off)."""
+        nc, kq, kmq, r = ensemble_classes(self.handle)
+        return dict(n_class=nc, Kq=kq, Kmq=kmq, flops_ratio=r)
 
     def device_bytes(self):
         b = ctypes.c_longlong()
@@ -405,6 +413,45 @@ def symmetry_cosets(symmetries):
         Rs.append(R[o:o + d * d].reshape(d, d).copy())
         o += d * d
     return dict(n_cosets=nc.value, coset_size=cs.value, order=order, partner=partner, R=Rs, offpattern=off.value)
+
+
+def symmetry_classes(symmetries):
+    """Character classes of the factorised path on per-block symmetry tables (host, no device):
+    tdscha_symmetry_classes.  None when the group has no such structure, else a dict of the layout
+    arrays (see include/tdscha_b200.h)."""
+    lib = load()
+    tabs = [np.ascontiguousarray(t, dtype=np.float64) for t in symmetries]
+    N_sym = tabs[0].shape[0]
+    n_deg = np.array([t.shape[1] for t in tabs], dtype=np.intc)
+    n = int(n_deg.sum())
+    ptrs = (dp * len(tabs))(*[_d(t) for t in tabs])
+    sizes = np.zeros(4, dtype=np.intc)
+    ratio = ctypes.c_double()
+    check(lib.tdscha_symmetry_classes(N_sym, len(tabs), _i(n_deg), ptrs, _i(sizes), ctypes.byref(ratio), None, None, None,
+                                      None, None, None, None, None))
+    nC, Kq, Kmq, P = (int(x) for x in sizes)
+    if nC == 0:
+        return None
+    cls = np.zeros((nC, 5), dtype=np.intc)
+    pcol_i = np.zeros((Kq, 5), dtype=np.intc)
+    pcol_d = np.zeros((Kq, 5))
+    pp_i = np.zeros((P, 2), dtype=np.intc)
+    pp_d = np.zeros((P, 2))
+    mcol_i = np.zeros((max(Kmq, 1), 2), dtype=np.intc)
+    mcol_d = np.zeros((max(Kmq, 1), 4))
+    mode_col = np.zeros(n, dtype=np.intc)
+    check(lib.tdscha_symmetry_classes(N_sym, len(tabs), _i(n_deg), ptrs, _i(sizes), ctypes.byref(ratio), _i(cls), _i(pcol_i),
+                                      _d(pcol_d), _i(pp_i), _d(pp_d), _i(mcol_i), _d(mcol_d), _i(mode_col)))
+    return dict(n_class=nC, Kq=Kq, Kmq=Kmq, flops_ratio=ratio.value, cls=cls, pcol_i=pcol_i, pcol_d=pcol_d, pp_i=pp_i,
+                pp_d=pp_d, mcol_i=mcol_i[:Kmq], mcol_d=mcol_d[:Kmq], mode_col=mode_col)
+
+
+def ensemble_classes(handle):
+    """(n_class, Kq, Kmq, flops_ratio) of a resident ensemble (tdscha_ensemble_classes)."""
+    lib = load()
+    nc, kq, kmq, r = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_double()
+    check(lib.tdscha_ensemble_classes(handle, ctypes.byref(nc), ctypes.byref(kq), ctypes.byref(kmq), ctypes.byref(r)))
+    return nc.value, kq.value, kmq.value, r.value
 
 
 def symmetries_on_modes(pols, perm, rot, deg_space):
