@@ -319,9 +319,19 @@ int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, con
  *   tdscha_debug_stall_next_contraction  the next contraction launch issues no operand copy, so that
  *                                        its first wait can only end by running out (tests of the
  *                                        abort path); one-shot, process-wide
+ *   tdscha_set_error_check               per_call = 1 (default): every device entry point that runs
+ *                                        tensor-core kernels reads the ensemble's error word when its
+ *                                        work is done (one stream synchronisation per call);
+ *                                        per_call = 0: the calls return as soon as their work is
+ *                                        queued and the error word keeps every expiry until
+ *                                        tdscha_check_errors reads it; process-wide
+ *   tdscha_check_errors                  waits for `stream`, returns TDSCHA_ETIMEOUT (and clears the
+ *                                        word) when a wait of an earlier call on this ensemble ran out
  */
 int tdscha_set_wait_budget(double seconds);
 int tdscha_debug_stall_next_contraction(void);
+int tdscha_set_error_check(int per_call);
+int tdscha_check_errors(tdscha_ensemble *ens, void *stream);
 
 /*
  * Vector-Jacobian product of the averages (the outputs of tdscha_perturb_average_sym_device)

@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points declared in include/tdscha_b200.h.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -51,7 +52,10 @@ static int scratch_get(int slot, size_t bytes, cudaStream_t st, void **out) {
     return 0;
 }
 
-static int check_err_word(tdscha_ensemble *e, cudaStream_t st) {
+// Per-call reading of the error word (tdscha_set_error_check); off: tdscha_check_errors reads it.
+static std::atomic<int> g_check_per_call{1};
+
+static int read_err_word(tdscha_ensemble *e, cudaStream_t st) {
     unsigned h = 0;
     TD_CUDA(cudaMemcpyAsync(&h, e->d_err, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
     TD_CUDA(cudaStreamSynchronize(st));
@@ -61,6 +65,10 @@ static int check_err_word(tdscha_ensemble *e, cudaStream_t st) {
         return TDSCHA_ETIMEOUT;
     }
     return 0;
+}
+
+static int check_err_word(tdscha_ensemble *e, cudaStream_t st) {
+    return g_check_per_call.load() ? read_err_word(e, st) : 0;
 }
 
 }  // namespace tdscha
@@ -371,6 +379,19 @@ int tdscha_debug_stall_next_contraction(void) {
     clear_error();
     tc::stall_next_launch();
     return 0;
+}
+
+int tdscha_set_error_check(int per_call) {
+    clear_error();
+    g_check_per_call.store(per_call ? 1 : 0);
+    return 0;
+}
+
+int tdscha_check_errors(tdscha_ensemble *e, void *stream) {
+    clear_error();
+    TD_CHECK(e != nullptr, TDSCHA_EINVAL, "NULL ensemble");
+    TD_CUDA(cudaSetDevice(e->device));
+    return read_err_word(e, static_cast<cudaStream_t>(stream));
 }
 
 int tdscha_tc_contract(int precision, int M, int N, int K, const void *A_hi, const void *A_lo, long long lda,

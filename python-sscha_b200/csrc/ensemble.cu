@@ -750,8 +750,7 @@ static int ensure_freq_operands(tdscha_ensemble *e, Format fmt, bool lo, cudaStr
     if (o.V_hi) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(o.V_hi); o = FreqOps(); }
     void *buf = nullptr;
     TD_CUDA(cudaMalloc(&buf, freq_operand_bytes(*e->freq, e->N, fmt, lo)));
-    TD_TRY(ensure_XGT(e, st));
-    const int rc = freq_build_operands(*e->freq, e->X, e->G, e->Y, e->Xt, e->XGT, e->N, e->n, e->N, fmt, lo, buf, o, st);
+    const int rc = freq_build_operands(*e->freq, e->X, e->G, e->Y, e->Xt, e->n, e->N, fmt, lo, buf, o, st);
     if (rc) { cudaFree(buf); o = FreqOps(); return rc; }
     return 0;
 }
@@ -933,10 +932,9 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
             const bool acc = c0 > 0;
             if (chunked) {
                 StageScope sc(e, ST_OTHER, st);
-                TD_TRY(ensure_XGT(e, st));
                 const int n = e->n;
-                TD_TRY(freq_build_operands(ft, e->X + c0 * n, e->G + c0 * n, e->Y + c0 * n, e->Xt + c0 * n, e->XGT + c0, e->N, n, Ncur,
-                                           fmt, lo, e->chunk_ops.base, co, st));
+                TD_TRY(freq_build_operands(ft, e->X + c0 * n, e->G + c0 * n, e->Y + c0 * n, e->Xt + c0 * n, n, Ncur, fmt, lo,
+                                           e->chunk_ops.base, co, st));
             }
             // per class: [a|b] and [c|d] in the character basis, (rows (comp, v, c), 2Nc columns)
             std::vector<tc::GemmGroup> gab, gcd, gz, gf;
@@ -964,16 +962,12 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
             }
             {
                 StageScope sc(e, ST_WEIGHTS, st);
-                const long long M = (long long)nC * 2 * NR;
-                const long long per_row = Ncur + (N2pc - N2c);
                 if (f64)
-                    weights_kernel<double><<<grid_for(M * per_row), 256, 0, st>>>((const double *)H, (const double *)Ch, L.ld1,
-                                                                                 e->rho + c0, (int)Ncur, (int)M, N2pc, apply_d4,
-                                                                                 fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
+                    TD_TRY(freq_weights<double>(ft, (const double *)H, (const double *)Ch, L.ld1, e->rho + c0, Ncur, NR, N2pc,
+                                                apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo, st));
                 else
-                    weights_kernel<float><<<grid_for(M * per_row), 256, 0, st>>>((const float *)H, (const float *)Ch, L.ld1,
-                                                                                e->rho + c0, (int)Ncur, (int)M, N2pc, apply_d4,
-                                                                                fmt, Cw_hi, Cw_lo, AB_hi, AB_lo);
+                    TD_TRY(freq_weights<float>(ft, (const float *)H, (const float *)Ch, L.ld1, e->rho + c0, Ncur, NR, N2pc,
+                                               apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo, st));
                 TD_CUDA(cudaGetLastError());
             }
             {

@@ -301,48 +301,109 @@ dim3 grid_rows(long long cols, long long rows) {
     return dim3((unsigned)gx, (unsigned)gy);
 }
 
-// Vq (2Nc x Kq): row k < Nc: components of x x^T, row Nc + i: of sym(x g^T)
-__global__ void build_Vq_kernel(const double *__restrict__ X, const double *__restrict__ G, int n, long long Nc, int Kq,
-                                const int *__restrict__ mu0, const int *__restrict__ nu0, const int *__restrict__ mu1,
-                                const int *__restrict__ nu1, const double *__restrict__ c0, const double *__restrict__ c1,
-                                Format fmt, void *hi, void *lo) {
-    for (long long k = blockIdx.y; k < 2 * Nc; k += gridDim.y) {
-        const bool second = k >= Nc;
-        const double *x = X + (second ? k - Nc : k) * n;
-        const double *g = G + (second ? k - Nc : k) * n;
-        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Kq; c += gridDim.x * blockDim.x) {
+// Vq (2Nc x Kq) and VqT (Kq x N2pc) together: one CTA per 64 x 64 tile of (configuration rows,
+// component columns) computes the tile once into shared memory (hi, lo) and writes it row-major and
+// transposed, 128 bytes or more per warp on both sides.  Rows k >= 2Nc (up to N2pc) are zero in VqT.
+template <typename T>
+__device__ __forceinline__ void split_to(Format fmt, double v, T &h, T &l);
+template <>
+__device__ __forceinline__ void split_to<uint16_t>(Format, double v, uint16_t &h, uint16_t &l) {
+    h = bf16_bits_rn((float)v);
+    l = bf16_bits_rn((float)(v - (double)bf16_bits_to_float(h)));
+}
+template <>
+__device__ __forceinline__ void split_to<float>(Format, double v, float &h, float &l) {
+    h = tf32_round((float)v);
+    l = tf32_round((float)(v - (double)h));
+}
+template <>
+__device__ __forceinline__ void split_to<double>(Format, double v, double &h, double &l) {
+    h = v;
+    l = 0.0;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) build_Vq_tiles_kernel(const double *__restrict__ X, const double *__restrict__ G, int n,
+                                                             long long Nc, long long N2pc, int Kq, const int *__restrict__ mu0,
+                                                             const int *__restrict__ nu0, const int *__restrict__ mu1,
+                                                             const int *__restrict__ nu1, const double *__restrict__ c0,
+                                                             const double *__restrict__ c1, Format fmt, T *__restrict__ V_hi,
+                                                             T *__restrict__ V_lo, T *__restrict__ VT_hi, T *__restrict__ VT_lo) {
+    constexpr int LO_ROWS = sizeof(T) == 8 ? 1 : 64;   // FP64 has no lo part
+    __shared__ T th[64][65];
+    __shared__ T tl[LO_ROWS][65];
+    const long long k0 = (long long)blockIdx.y * 64;   // configuration rows (of [x x^T ; sym(x g^T)])
+    const int cb = blockIdx.x * 64;                     // component columns
+    const int tid = threadIdx.y * 32 + threadIdx.x;
+    const bool lo = V_lo != nullptr;
+    for (int e = tid; e < 64 * 64; e += 256) {
+        const int r = e >> 6, cc = e & 63;
+        const long long k = k0 + r;
+        const int c = cb + cc;
+        double v = 0.0;
+        if (k < 2 * Nc && c < Kq) {
+            const bool second = k >= Nc;
+            const double *x = X + (second ? k - Nc : k) * n;
             const int a0 = mu0[c], b0 = nu0[c], a1 = mu1[c], b1 = nu1[c];
-            double v;
-            if (!second) v = c0[c] * x[a0] * x[b0] + c1[c] * x[a1] * x[b1];
-            else v = 0.5 * (c0[c] * (x[a0] * g[b0] + x[b0] * g[a0]) + c1[c] * (x[a1] * g[b1] + x[b1] * g[a1]));
-            store_split(fmt, hi, lo, k * Kq + c, v);
+            if (!second) {
+                v = c0[c] * x[a0] * x[b0] + c1[c] * x[a1] * x[b1];
+            } else {
+                const double *g = G + (k - Nc) * n;
+                v = 0.5 * (c0[c] * (x[a0] * g[b0] + x[b0] * g[a0]) + c1[c] * (x[a1] * g[b1] + x[b1] * g[a1]));
+            }
+        }
+        T h, l;
+        split_to<T>(fmt, v, h, l);
+        th[r][cc] = h;
+        if constexpr (LO_ROWS == 64) tl[r][cc] = l;
+    }
+    __syncthreads();
+    // row-major: rows k < 2Nc, 64 columns
+    constexpr int EPW = sizeof(T) == 2 ? 2 : 1;   // elements per store word
+    constexpr int WPR = 64 / EPW;                  // words per tile row
+    for (int w = tid; w < 64 * WPR; w += 256) {
+        const int r = w / WPR, j = (w % WPR) * EPW;
+        const long long k = k0 + r;
+        if (k >= 2 * Nc || cb + j >= Kq) continue;
+        if constexpr (EPW == 2) {
+            const uint32_t ph = (uint32_t)th[r][j] | ((uint32_t)th[r][j + 1] << 16);
+            *reinterpret_cast<uint32_t *>(V_hi + k * Kq + cb + j) = ph;
+            if (lo) *reinterpret_cast<uint32_t *>(V_lo + k * Kq + cb + j) = (uint32_t)tl[r][j] | ((uint32_t)tl[r][j + 1] << 16);
+        } else {
+            V_hi[k * Kq + cb + j] = th[r][j];
+            if constexpr (LO_ROWS == 64)
+                if (lo) V_lo[k * Kq + cb + j] = tl[r][j];
+        }
+    }
+    // transposed: rows c (64), columns k0 .. k0 + 63 (< N2pc)
+    for (int w = tid; w < 64 * WPR; w += 256) {
+        const int cr = w / WPR, j = (w % WPR) * EPW;
+        const int c = cb + cr;
+        const long long k = k0 + j;
+        if (c >= Kq || k >= N2pc) continue;
+        if constexpr (EPW == 2) {
+            *reinterpret_cast<uint32_t *>(VT_hi + (long long)c * N2pc + k) = (uint32_t)th[j][cr] | ((uint32_t)th[j + 1][cr] << 16);
+            if (lo)
+                *reinterpret_cast<uint32_t *>(VT_lo + (long long)c * N2pc + k) =
+                    (uint32_t)tl[j][cr] | ((uint32_t)tl[j + 1][cr] << 16);
+        } else {
+            VT_hi[(long long)c * N2pc + k] = th[j][cr];
+            if constexpr (LO_ROWS == 64)
+                if (lo) VT_lo[(long long)c * N2pc + k] = tl[j][cr];
         }
     }
 }
 
-// VqT (Kq x N2pc) from XGT = [X^T ; G^T] (2n x ldT, configuration-contiguous): coalesced reads
-__global__ void build_VqT_kernel(const double *__restrict__ XGT, long long ldT, int n, long long Nc, long long N2pc, int Kq,
-                                 const int *__restrict__ mu0, const int *__restrict__ nu0, const int *__restrict__ mu1,
-                                 const int *__restrict__ nu1, const double *__restrict__ c0, const double *__restrict__ c1,
-                                 Format fmt, void *hi, void *lo) {
-    for (long long c = blockIdx.y; c < Kq; c += gridDim.y) {
-        const int a0 = mu0[c], b0 = nu0[c], a1 = mu1[c], b1 = nu1[c];
-        const double k0 = c0[c], k1 = c1[c];
-        const double *xa0 = XGT + (long long)a0 * ldT, *xb0 = XGT + (long long)b0 * ldT;
-        const double *xa1 = XGT + (long long)a1 * ldT, *xb1 = XGT + (long long)b1 * ldT;
-        const double *ga0 = XGT + (long long)(n + a0) * ldT, *gb0 = XGT + (long long)(n + b0) * ldT;
-        const double *ga1 = XGT + (long long)(n + a1) * ldT, *gb1 = XGT + (long long)(n + b1) * ldT;
-        for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < N2pc; k += (long long)gridDim.x * blockDim.x) {
-            double v = 0.0;
-            if (k < Nc) {
-                v = k0 * xa0[k] * xb0[k] + k1 * xa1[k] * xb1[k];
-            } else if (k < 2 * Nc) {
-                const long long i = k - Nc;
-                v = 0.5 * (k0 * (xa0[i] * gb0[i] + xb0[i] * ga0[i]) + k1 * (xa1[i] * gb1[i] + xb1[i] * ga1[i]));
-            }
-            store_split(fmt, hi, lo, c * N2pc + k, v);
-        }
-    }
+template <typename T>
+int build_Vq_tiles(const FreqTables &t, const double *X, const double *G, int n, long long Nc, long long N2pc, Format fmt,
+                   void *V_hi, void *V_lo, void *VT_hi, void *VT_lo, cudaStream_t st) {
+    TD_CHECK(N2pc % 64 == 0 && N2pc / 64 <= 65535 && t.Kq % 64 == 0, TDSCHA_EINVAL, "operand tiles: %lld x %d", N2pc, t.Kq);
+    const dim3 grid((unsigned)(t.Kq / 64), (unsigned)(N2pc / 64));
+    build_Vq_tiles_kernel<T><<<grid, dim3(32, 8), 0, st>>>(X, G, n, Nc, N2pc, t.Kq, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0,
+                                                           t.pc_c1, fmt, static_cast<T *>(V_hi), static_cast<T *>(V_lo),
+                                                           static_cast<T *>(VT_hi), static_cast<T *>(VT_lo));
+    TD_CUDA(cudaGetLastError());
+    return 0;
 }
 
 // XGq (2Nc x Kmq): mode components of x (rows < Nc) and g
@@ -447,7 +508,105 @@ __global__ void recon_f_kernel(int NR, int n, int Kmq, const AccT *__restrict__ 
     }
 }
 
+// 4 consecutive values into an operand slot of format fmt (fp32 arithmetic; idx a multiple of 4)
+__device__ __forceinline__ void store4_split(Format fmt, void *hi, void *lo, long long idx, const float (&v)[4]) {
+    if (fmt == FMT_BF16) {
+        __nv_bfloat16 h[4], l[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            h[e] = __float2bfloat16_rn(v[e]);
+            l[e] = __float2bfloat16_rn(v[e] - __bfloat162float(h[e]));
+        }
+        *reinterpret_cast<uint2 *>(static_cast<__nv_bfloat16 *>(hi) + idx) = *reinterpret_cast<const uint2 *>(h);
+        if (lo) *reinterpret_cast<uint2 *>(static_cast<__nv_bfloat16 *>(lo) + idx) = *reinterpret_cast<const uint2 *>(l);
+    } else {
+        float4 h, l;
+        h.x = tf32_round(v[0]); h.y = tf32_round(v[1]); h.z = tf32_round(v[2]); h.w = tf32_round(v[3]);
+        l.x = tf32_round(v[0] - h.x); l.y = tf32_round(v[1] - h.y); l.z = tf32_round(v[2] - h.z); l.w = tf32_round(v[3] - h.w);
+        *reinterpret_cast<float4 *>(static_cast<float *>(hi) + idx) = h;
+        if (lo) *reinterpret_cast<float4 *>(static_cast<float *>(lo) + idx) = l;
+    }
+}
+
+// One CTA row per operand row (grid-stride), threads over quads of configurations.  vec: fp32
+// accumulators, a split format and Nc a multiple of 4 (aligned vector loads and stores).
+template <typename AccT, bool VEC>
+__global__ void __launch_bounds__(256) freq_weights_kernel(const AccT *__restrict__ H, const AccT *__restrict__ Ch, long long ld,
+                                                           const double *__restrict__ rho, long long Nc, int NR, long long rows,
+                                                           const int *__restrict__ cls_real, long long N2pc, int d4, Format fmt,
+                                                           void *Cw_hi, void *Cw_lo, void *AB_hi, void *AB_lo) {
+    for (long long r = blockIdx.y; r < rows; r += gridDim.y) {
+        const long long g = r / (2LL * NR);
+        if (r - g * 2LL * NR >= NR && cls_real[g]) continue;   // imaginary row of a real class
+        const AccT *h = H + r * ld, *c = Ch + r * ld;
+        const long long o = r * N2pc;
+        if constexpr (VEC) {
+            const float k4 = d4 ? 1.f : 0.f;
+            for (long long i0 = 4LL * (blockIdx.x * (long long)blockDim.x + threadIdx.x); i0 < Nc;
+                 i0 += 4LL * gridDim.x * blockDim.x) {
+                const float4 a = *reinterpret_cast<const float4 *>(h + i0), b = *reinterpret_cast<const float4 *>(h + Nc + i0);
+                const float4 cc = *reinterpret_cast<const float4 *>(c + i0), dd = *reinterpret_cast<const float4 *>(c + Nc + i0);
+                const float av[4] = {a.x, a.y, a.z, a.w}, bv[4] = {b.x, b.y, b.z, b.w};
+                const float cv[4] = {cc.x, cc.y, cc.z, cc.w}, dv[4] = {dd.x, dd.y, dd.z, dd.w};
+                float half_delta[4], gamma[4], alpha[4], beta[4];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float rh = (float)rho[i0 + e];
+                    gamma[e] = rh * (-cv[e] * (1.f / 3.f) + k4 * av[e] * 0.125f);
+                    half_delta[e] = 0.5f * rh * (-dv[e] * (1.f / 3.f) + k4 * bv[e] * 0.25f);
+                    alpha[e] = -rh * av[e] * (1.f / 6.f);
+                    beta[e] = -rh * bv[e] * (1.f / 3.f);
+                }
+                store4_split(fmt, Cw_hi, Cw_lo, o + i0, half_delta);
+                store4_split(fmt, Cw_hi, Cw_lo, o + Nc + i0, gamma);
+                store4_split(fmt, AB_hi, AB_lo, o + i0, alpha);
+                store4_split(fmt, AB_hi, AB_lo, o + Nc + i0, beta);
+            }
+        } else {
+            for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < Nc; i += (long long)gridDim.x * blockDim.x) {
+                const double a = (double)h[i], b = (double)h[Nc + i], cv = (double)c[i], dv = (double)c[Nc + i];
+                const double rh = rho[i];
+                const double gam = rh * (-cv / 3.0 + (d4 ? a / 8.0 : 0.0));
+                const double del = rh * (-dv / 3.0 + (d4 ? b / 4.0 : 0.0));
+                store_split(fmt, Cw_hi, Cw_lo, o + i, 0.5 * del);
+                store_split(fmt, Cw_hi, Cw_lo, o + Nc + i, gam);
+                store_split(fmt, AB_hi, AB_lo, o + i, -rh * a / 6.0);
+                store_split(fmt, AB_hi, AB_lo, o + Nc + i, -rh * b / 3.0);
+            }
+        }
+        // zero columns past 2Nc (the contractions' K runs to N2pc)
+        if (blockIdx.x == 0)
+            for (long long k = 2 * Nc + threadIdx.x; k < N2pc; k += blockDim.x) {
+                store_split(fmt, Cw_hi, Cw_lo, o + k, 0.0);
+                store_split(fmt, AB_hi, AB_lo, o + k, 0.0);
+            }
+    }
+}
+
 }  // namespace
+
+template <typename AccT>
+int freq_weights(const FreqTables &t, const AccT *H, const AccT *Ch, long long ld, const double *rho, long long Nc, int NR,
+                 long long N2pc, int d4, Format fmt, void *Cw_hi, void *Cw_lo, void *AB_hi, void *AB_lo, cudaStream_t st) {
+    const long long rows = (long long)t.n_class * 2 * NR;
+    const bool vec = sizeof(AccT) == 4 && fmt != FMT_F64 && Nc % 4 == 0 && ld % 4 == 0;
+    const long long per = vec ? ceil_div(Nc, 4) : Nc;
+    const dim3 grid((unsigned)std::max<long long>(1, std::min<long long>(ceil_div(per, 256), 64)),
+                    (unsigned)std::max<long long>(1, std::min<long long>(rows, 65535)));
+    if (vec)
+        freq_weights_kernel<AccT, true><<<grid, 256, 0, st>>>(H, Ch, ld, rho, Nc, NR, rows, t.d_cls_real, N2pc, d4, fmt, Cw_hi,
+                                                              Cw_lo, AB_hi, AB_lo);
+    else
+        freq_weights_kernel<AccT, false><<<grid, 256, 0, st>>>(H, Ch, ld, rho, Nc, NR, rows, t.d_cls_real, N2pc, d4, fmt, Cw_hi,
+                                                               Cw_lo, AB_hi, AB_lo);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template int freq_weights<float>(const FreqTables &, const float *, const float *, long long, const double *, long long, int,
+                                 long long, int, Format, void *, void *, void *, void *, cudaStream_t);
+template int freq_weights<double>(const FreqTables &, const double *, const double *, long long, const double *, long long,
+                                  int, long long, int, Format, void *, void *, void *, void *, cudaStream_t);
 
 int freq_tables_create(const FreqLayout &L, FreqTables **out) {
     *out = nullptr;
@@ -473,7 +632,7 @@ int freq_tables_create(const FreqLayout &L, FreqTables **out) {
         (rc = upload(L.mc_mode, &t->mc_mode, &acc)) || (rc = upload(L.mc_partner, &t->mc_partner, &acc)) ||
         (rc = upload(L.mode_col, &t->mode_col, &acc)) || (rc = upload(L.mc_sign, &t->mc_sign, &acc)) ||
         (rc = upload(L.mc_re, &t->mc_re, &acc)) || (rc = upload(L.mc_im, &t->mc_im, &acc)) ||
-        (rc = upload(L.mc_zc, &t->mc_zc, &acc))) {
+        (rc = upload(L.mc_zc, &t->mc_zc, &acc)) || (rc = upload(L.cls_real, &t->d_cls_real, &acc))) {
         freq_tables_destroy(t);
         return rc;
     }
@@ -486,7 +645,7 @@ void freq_tables_destroy(FreqTables *t) {
     if (!t) return;
     void *ps[] = {t->pc_mu0, t->pc_nu0, t->pc_mu1, t->pc_nu1, t->pc_partner, t->pc_c0, t->pc_c1, t->pc_re, t->pc_im, t->pc_zc,
                   t->pp_col0, t->pp_col1, t->pp_c0, t->pp_c1, t->mc_mode, t->mc_partner, t->mode_col, t->mc_sign, t->mc_re,
-                  t->mc_im, t->mc_zc};
+                  t->mc_im, t->mc_zc, t->d_cls_real};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete t;
@@ -498,9 +657,8 @@ size_t freq_operand_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo
     return per * format_bytes(fmt) * (lo ? 2 : 1) + 8 * 256;
 }
 
-int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt,
-                        const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
-                        cudaStream_t st) {
+int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt, int n,
+                        long long Nc, Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st) {
     const size_t es = format_bytes(fmt);
     const long long N2pc = round_up(2 * Nc, 64);
     const long long nV = 2 * Nc * t.Kq, nVT = (long long)t.Kq * N2pc, nXG = 2 * Nc * t.Kmq, nYX = (long long)t.Kmq * N2pc;
@@ -518,10 +676,14 @@ int freq_build_operands(const FreqTables &t, const double *X, const double *G, c
         o.XG_lo = take(nXG);
         o.YX_lo = take(nYX);
     }
-    build_Vq_kernel<<<grid_rows(t.Kq, 2 * Nc), 256, 0, st>>>(X, G, n, Nc, t.Kq, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0,
-                                                             t.pc_c1, fmt, o.V_hi, o.V_lo);
-    build_VqT_kernel<<<grid_rows(N2pc, t.Kq), 256, 0, st>>>(XGT, ldT, n, Nc, N2pc, t.Kq, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1,
-                                                            t.pc_c0, t.pc_c1, fmt, o.VT_hi, o.VT_lo);
+    // Vq and its transpose from shared-memory tiles (gathering the transpose from the ensemble per
+    // component would re-read the ensemble rows once per component)
+    if (fmt == FMT_BF16)
+        TD_TRY(build_Vq_tiles<uint16_t>(t, X, G, n, Nc, N2pc, fmt, o.V_hi, o.V_lo, o.VT_hi, o.VT_lo, st));
+    else if (fmt == FMT_F64)
+        TD_TRY(build_Vq_tiles<double>(t, X, G, n, Nc, N2pc, fmt, o.V_hi, nullptr, o.VT_hi, nullptr, st));
+    else
+        TD_TRY(build_Vq_tiles<float>(t, X, G, n, Nc, N2pc, fmt, o.V_hi, o.V_lo, o.VT_hi, o.VT_lo, st));
     build_XGq_kernel<<<grid1(nXG), 256, 0, st>>>(X, G, n, Nc, t.Kmq, t.mc_mode, t.mc_sign, fmt, o.XG_hi, o.XG_lo);
     build_YXq_kernel<<<grid1(nYX), 256, 0, st>>>(Y, Xt, n, Nc, N2pc, t.Kmq, t.mc_mode, t.mc_sign, fmt, o.YX_hi, o.YX_lo);
     TD_CUDA(cudaGetLastError());

@@ -67,6 +67,7 @@ struct FreqTables {
     double *pp_c0 = nullptr, *pp_c1 = nullptr;
     int *mc_mode = nullptr, *mc_partner = nullptr, *mode_col = nullptr;
     double *mc_sign = nullptr, *mc_re = nullptr, *mc_im = nullptr, *mc_zc = nullptr;
+    int *d_cls_real = nullptr;
     double flops_ratio = 0;
     size_t bytes = 0;
 };
@@ -86,16 +87,23 @@ struct FreqOps {
 };
 size_t freq_operand_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo);
 // Operands of configurations [c0, c0 + Nc) into caller-provided storage `buf` (freq_operand_bytes).
-// X, G, Y, Xt: (N x n) rotated-basis ensemble (row c0 first); XGT: [X^T; G^T] (2n x ldT).
-int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt,
-                        const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
-                        cudaStream_t st);
+// X, G, Y, Xt: (N x n) rotated-basis ensemble (row c0 first).
+int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt, int n,
+                        long long Nc, Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st);
 
 // Left operands from the representatives' transforms (InT float or double):
 //   Lab (2 NR x Kq) from U (NR x ldu, packed pairs), Lcd (2 NR x Kmq) from r1p (NR x ldr).
 template <typename InT>
 int freq_left(const FreqTables &t, int NR, int n, const InT *U, long long ldu, const InT *r1p, long long ldr, Format fmt,
               void *Lab_hi, void *Lab_lo, void *Lcd_hi, void *Lcd_lo, cudaStream_t st);
+
+// Weights of the character basis, class by class: from [a|b] (H) and [c|d] (Ch), rows
+// g * 2NR + (comp, v, c) with ld, columns i < Nc and Nc + i, write Cw = [delta/2 | gamma] and
+// AB = [alpha | beta] (ld N2pc, zero columns from 2Nc on); the imaginary rows of real classes are
+// skipped (their contractions never read them).
+template <typename AccT>
+int freq_weights(const FreqTables &t, const AccT *H, const AccT *Ch, long long ld, const double *rho, long long Nc, int NR,
+                 long long N2pc, int d4, Format fmt, void *Cw_hi, void *Cw_lo, void *AB_hi, void *AB_lo, cudaStream_t st);
 
 // Back from the character basis: Zs (NR x ldz, packed c_p N~) from O (2 NR x Kq), Fs (NR x ldf)
 // from OF (2 NR x Kmq).

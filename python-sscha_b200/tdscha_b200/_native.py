@@ -91,6 +91,8 @@ def load():
     lib.tdscha_lanczos_run_device.argtypes = [ctypes.c_int, ctypes.POINTER(RunSystem), ctypes.c_int, ctypes.c_int, vp]
     lib.tdscha_set_wait_budget.argtypes = [ctypes.c_double]
     lib.tdscha_debug_stall_next_contraction.argtypes = []
+    lib.tdscha_set_error_check.argtypes = [ctypes.c_int]
+    lib.tdscha_check_errors.argtypes = [vp, vp]
     lib.tdscha_set_profiling.argtypes = [vp, ctypes.c_int]
     lib.tdscha_read_profile.argtypes = [vp, dp, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
     for name in ("tdscha_perturb_average_vjp_precision_device", "tdscha_set_wait_budget", "tdscha_debug_stall_next_contraction", "tdscha_apply_L1_static_device", "tdscha_apply_static_L_device", "tdscha_lanczos_run_device", "tdscha_lanczos_step_device_noalloc", "tdscha_apply_prologue_device", "tdscha_apply_epilogue_device", "tdscha_set_profiling", "tdscha_read_profile", "tdscha_tc_contract", "tdscha_ensemble_create", "tdscha_ensemble_destroy", "tdscha_ensemble_info",
@@ -334,6 +336,17 @@ def tc_contract(precision, A_hi, A_lo, B_hi, B_lo, D, stream=None):
 def set_wait_budget(seconds):
     """Budget of every bounded wait of the tensor-core kernels launched afterwards (default 4 s)."""
     check(load().tdscha_set_wait_budget(float(seconds)))
+
+
+def set_error_check(per_call):
+    """tdscha_set_error_check: read the error word after every device call (True, default) or only
+    in check_errors (False)."""
+    check(load().tdscha_set_error_check(1 if per_call else 0))
+
+
+def check_errors(handle, stream=None):
+    """tdscha_check_errors: wait for the stream, raise on a bounded wait that ran out since the last check."""
+    check(load().tdscha_check_errors(handle, _stream_ptr(stream)))
 
 
 def debug_stall_next_contraction():

@@ -73,3 +73,28 @@ def test_wait_budget_rejects_out_of_range(cuda):
         _native.set_wait_budget(0.0)
     with pytest.raises(_native.TdschaError, match="EINVAL"):
         _native.set_wait_budget(1e3)
+
+
+def test_deferred_error_check_reports_the_expiry_later(cuda, rocksalt_l2):
+    """With the per-call check off (tdscha_set_error_check(0)) the stalled averages call returns at
+    once; tdscha_check_errors reports the expiry afterwards, clears it, and later calls are exact."""
+    from tdscha_b200 import _native
+    d = rocksalt_l2
+    ens = _native.DeviceEnsemble(d["X"], d["Y"], d["w"], d["rho"], d["T"], d["syms"], d["blocks"], d["blocks_ids"])
+    f0, dv0 = ens.perturb_average(d["case0_R1"], d["case0_Y1"], 1, "bf16x3")
+    try:
+        _native.set_error_check(False)
+        _native.set_wait_budget(0.02)
+        _native.debug_stall_next_contraction()
+        ens.perturb_average(d["case0_R1"], d["case0_Y1"], 1, "bf16x3")      # no error at return
+        with pytest.raises(_native.TdschaError, match="ETIMEOUT"):
+            _native.check_errors(ens.handle)
+        _native.check_errors(ens.handle)                                      # cleared
+        _native.set_wait_budget(4.0)
+        f, dv = ens.perturb_average(d["case0_R1"], d["case0_Y1"], 1, "bf16x3")
+        _native.check_errors(ens.handle)
+    finally:
+        _native.set_wait_budget(4.0)
+        _native.set_error_check(True)
+    assert np.array_equal(f, f0) and np.array_equal(dv, dv0)
+    ens.close()
