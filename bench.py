@@ -32,7 +32,10 @@ for _p in (REPO, os.path.join(REPO, "python-sscha_b200")):
 # of 768, 16 vectors: M = 12288, N = 5000, K = 72832; 4.92e10 B read + written against 5.29e9 B of
 # algorithmic operand and output bytes, 9.3x) and scaled to the full launch by its algorithmic bytes
 # (2.406e10 B x 9.3).
-MEASURED_TRAFFIC = {(4, 10000, 8, "bf16x3"): 2.24e11}
+# On the character-class path: the grouped [a|b] launch of the same system with N = 2500 moved
+# 3.05e9 B against 2.92e9 B of algorithmic bytes (1.04x); scaled by the algorithmic bytes of the
+# N = 10000 launch (1.033e10 B).
+MEASURED_TRAFFIC = {(4, 10000, 8, "bf16x3"): 2.24e11, (4, 10000, 8, "bf16x3", "classes"): 1.08e10}
 METRIC = "apply_L/s at 128 atoms N=1e4: mixed+batched vs FP64 GPU at G(w) rel err <=1e-5"
 
 
@@ -845,7 +848,8 @@ def main():
         kernel = (f"tc_gemm_kernel, grouped: [a|b] over {cls['n_class']} character classes of the translation subgroup "
                   f"(executed work {ratio:.4f} x the contraction over all {s.n_syms} symmetry rows)")
         traffic = MEASURED_TRAFFIC.get((a.L, a.N, a.chains, a.precision, "classes"))
-        tnote = "ncu dram__bytes_read.sum + dram__bytes_write.sum of the grouped [a|b] launch (profiles/)"
+        tnote = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of the grouped [a|b] launch at N = 2500 (1.04x its "
+                 "algorithmic bytes), scaled by the algorithmic bytes of this launch")
     else:
         kernel = "tc_gemm_kernel ([a|b] = Y~ . V^T projection)"
         traffic = MEASURED_TRAFFIC.get((a.L, a.N, a.chains, a.precision))

@@ -292,8 +292,9 @@ int tdscha_continued_fraction_device(int n_iter, const double *a, const double *
  * apply, DynamicalLanczos.py:3521-3551).  When enabled, every averages call records CUDA events on
  * its launching stream around each stage.  tdscha_read_profile synchronises, returns the summed
  * milliseconds and the launch counts of the n_stages stages (0 transform, 1 contraction [a|b],
- * 2 contraction [c|d], 3 weights, 4 contraction Z, 5 contraction F, 6 fold, 7 other) since the
- * last read, and resets them.  Launch counts are kept even with profiling disabled.
+ * 2 contraction [c|d], 3 weights, 4 contraction Z, 5 contraction F, 6 fold, 7 other, 8 the
+ * operand rebuilds of configuration-chunked ensembles) since the last read, and resets them.
+ * Launch counts are kept even with profiling disabled.
  */
 int tdscha_set_profiling(tdscha_ensemble *ens, int enable);
 int tdscha_read_profile(tdscha_ensemble *ens, double *ms, long long *launches, int n_stages);

@@ -2,6 +2,7 @@
 // orchestration of the symmetrised perturbed averages (the algebra is in ensemble.cuh).
 #include <cublas_v2.h>
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -541,6 +542,10 @@ int ensemble_destroy(tdscha_ensemble *e) {
     freq_tables_destroy(e->freq);
     for (auto &fo : e->fops)
         if (fo.V_hi) cudaFree(fo.V_hi);   // one allocation per format, V_hi first
+    for (int f = 0; f < 3; ++f) {
+        if (e->fyx_hi[f]) cudaFree(e->fyx_hi[f]);
+        if (e->fyx_lo[f]) cudaFree(e->fyx_lo[f]);
+    }
     sym_umma_destroy(e->umma);
     if (e->cublas) cublasDestroy(e->cublas);
     delete e;
@@ -739,6 +744,25 @@ static bool sym_umma_enabled() {
 // The averages on the character classes of the subgroup (freq.cuh): dense transform and fold over
 // the coset representatives, the four contractions class by class.
 // ------------------------------------------------------------------------------------------------
+// k-blocks accumulated in tensor memory per drain of the class [a|b] contraction.  Its K is one
+// class's components (a few thousand), so its tiles are short and a drain after every k-block leaves
+// the tile's final store exposed; four k-blocks per drain overlap it with the next tile's MMAs at
+// the split modes' accuracy of single-k-block drains (measured on the 4x4x4 benchmark system).
+// TDSCHA_FREQ_DRAIN_AB overrides (0: the contraction default).
+static int freq_ab_drain() {
+    const char *env = getenv("TDSCHA_FREQ_DRAIN_AB");
+    return env ? std::max(0, atoi(env)) : 4;
+}
+
+// TDSCHA_FREQ_FUSED_CD=1 forms the thin [c|d] contraction of the split formats inside the weights
+// kernel instead of a grouped contraction plus a separate weights kernel (read at every call).  Off
+// by default: on the 4x4x4 benchmark system the fused kernel takes 6.7 ms per 16-vector step against
+// 2.1 + 3.1 ms for the two launches (same results).
+static bool fused_cd_enabled() {
+    const char *env = getenv("TDSCHA_FREQ_FUSED_CD");
+    return env && atoi(env) == 1;
+}
+
 static bool use_freq_path(const tdscha_ensemble *e, Format fmt) {
     return e->freq && e->cosets && cosets_enabled() && freq_enabled() && !(fmt == FMT_BF16 && sym_umma_enabled());
 }
@@ -750,7 +774,8 @@ static int ensure_freq_operands(tdscha_ensemble *e, Format fmt, bool lo, cudaStr
     if (o.V_hi) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(o.V_hi); o = FreqOps(); }
     void *buf = nullptr;
     TD_CUDA(cudaMalloc(&buf, freq_operand_bytes(*e->freq, e->N, fmt, lo)));
-    const int rc = freq_build_operands(*e->freq, e->X, e->G, e->Y, e->Xt, e->n, e->N, fmt, lo, buf, o, st);
+    TD_TRY(ensure_XGT(e, st));
+    const int rc = freq_build_operands(*e->freq, e->X, e->G, e->Y, e->Xt, e->XGT, e->N, e->n, e->N, fmt, lo, buf, o, st);
     if (rc) { cudaFree(buf); o = FreqOps(); return rc; }
     return 0;
 }
@@ -810,13 +835,15 @@ static int gemm_groups_f64(tdscha_ensemble *e, const std::vector<tc::GemmGroup> 
 
 static int gemm_groups(tdscha_ensemble *e, Format fmt, int nprod, const void *A_hi, const void *A_lo, long long a_rows,
                        long long lda, const void *B_hi, const void *B_lo, long long b_rows, long long ldb,
-                       const std::vector<tc::GemmGroup> &gs, void *C, long long ldc, bool accumulate, cudaStream_t st) {
+                       const std::vector<tc::GemmGroup> &gs, void *C, long long ldc, bool accumulate, cudaStream_t st,
+                       int drain_kb = 0) {
     if (gs.empty()) return 0;
     if (fmt == FMT_F64)
         return gemm_groups_f64(e, gs, static_cast<const double *>(A_hi), lda, static_cast<const double *>(B_hi), ldb,
                                static_cast<double *>(C), ldc, accumulate, st);
     tc::GemmOperands op{fmt, nprod, A_hi, A_lo, lda, B_hi, B_lo, ldb};
     op.accumulate = accumulate;
+    op.drain_kb = drain_kb;
     return tc::gemm_grouped(op, a_rows, lda, b_rows, ldb, gs.data(), (int)gs.size(), static_cast<float *>(C), ldc, st, e->d_err);
 }
 
@@ -909,6 +936,8 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
     int n_classes = 0;
     for (int m = 1; m <= SYM_MT_MAX; ++m) n_classes += e->pairs.count[m] > 0 ? 1 : 0;
     const long long Kmq1 = std::max(ft.Kmq, 1);
+    bool fused_cd = !f64 && ft.Kmq > 0 && fused_cd_enabled();
+    for (int u : ft.mcol_used) fused_cd = fused_cd && u <= 64;
     for (int p0 = 0; p0 < n_cos; p0 += ncj) {
         const int nc = std::min(ncj, n_cos - p0);
         const int NR = nb * nc;
@@ -931,10 +960,11 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
             const long long N2c = 2 * Ncur, N2pc = round_up(N2c, 64);   // the last chunk may be shorter
             const bool acc = c0 > 0;
             if (chunked) {
-                StageScope sc(e, ST_OTHER, st);
+                StageScope sc(e, ST_OPERANDS, st, 3);
                 const int n = e->n;
-                TD_TRY(freq_build_operands(ft, e->X + c0 * n, e->G + c0 * n, e->Y + c0 * n, e->Xt + c0 * n, n, Ncur, fmt, lo,
-                                           e->chunk_ops.base, co, st));
+                TD_TRY(ensure_XGT(e, st));
+                TD_TRY(freq_build_operands(ft, e->X + c0 * n, e->G + c0 * n, e->Y + c0 * n, e->Xt + c0 * n, e->XGT + c0, e->N, n,
+                                           Ncur, fmt, lo, e->chunk_ops.base, co, st));
             }
             // per class: [a|b] and [c|d] in the character basis, (rows (comp, v, c), 2Nc columns)
             std::vector<tc::GemmGroup> gab, gcd, gz, gf;
@@ -946,21 +976,26 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
                 if (ft.mcol_cnt[g] > 0) {
                     gcd.push_back({Mg, (int)N2c, ft.mcol_cnt[g], 0, ft.mcol_off[g], 0, ft.mcol_off[g], hrow * L.ld1});
                     gf.push_back({Mg, ft.mcol_cnt[g], (int)N2pc, (int)hrow, 0, ft.mcol_off[g], 0, (long long)ft.mcol_off[g]});
-                } else {
+                } else if (!fused_cd) {
                     TD_CUDA(cudaMemsetAsync(static_cast<uint8_t *>(Ch) + hrow * L.ld1 * as, 0, (size_t)2 * NR * L.ld1 * as, st));
                 }
             }
             {
                 StageScope sc(e, ST_GEMM_AB, st);
                 TD_TRY(gemm_groups(e, fmt, nprod, Lab_hi, Lab_lo, 2LL * NR, ft.Kq, co.V_hi, co.V_lo, N2c, ft.Kq, gab, H, L.ld1, false,
-                                   st));
+                                   st, freq_ab_drain()));
             }
-            {
-                StageScope sc(e, ST_GEMM_CD, st);
-                TD_TRY(gemm_groups(e, fmt, nprod, Lcd_hi, Lcd_lo, 2LL * NR, Kmq1, co.XG_hi, co.XG_lo, N2c, Kmq1, gcd, Ch, L.ld1,
-                                   false, st));
-            }
-            {
+            if (fused_cd) {
+                // [c|d] formed inside the weights kernel (the class's few mode columns)
+                StageScope sc(e, ST_WEIGHTS, st);
+                TD_TRY(freq_weights_cd(ft, (const float *)H, L.ld1, Lcd_hi, Lcd_lo, co.XG_hi, co.XG_lo, e->rho + c0, Ncur, NR, N2pc,
+                                       apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo, st));
+            } else {
+                {
+                    StageScope sc(e, ST_GEMM_CD, st);
+                    TD_TRY(gemm_groups(e, fmt, nprod, Lcd_hi, Lcd_lo, 2LL * NR, Kmq1, co.XG_hi, co.XG_lo, N2c, Kmq1, gcd, Ch, L.ld1,
+                                       false, st));
+                }
                 StageScope sc(e, ST_WEIGHTS, st);
                 if (f64)
                     TD_TRY(freq_weights<double>(ft, (const double *)H, (const double *)Ch, L.ld1, e->rho + c0, Ncur, NR, N2pc,
@@ -968,7 +1003,6 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
                 else
                     TD_TRY(freq_weights<float>(ft, (const float *)H, (const float *)Ch, L.ld1, e->rho + c0, Ncur, NR, N2pc,
                                                apply_d4, fmt, Cw_hi, Cw_lo, AB_hi, AB_lo, st));
-                TD_CUDA(cudaGetLastError());
             }
             {
                 StageScope sc(e, ST_GEMM_Z, st);
@@ -1167,7 +1201,7 @@ int perturb_average_device(tdscha_ensemble *e, int nb, const double *R1, const d
             const long long N2c = 2 * Ncur, N2pc = round_up(N2c, 64);
             const bool acc = c0 > 0;
             if (chunked) {
-                StageScope sc(e, ST_OTHER, st);
+                StageScope sc(e, ST_OPERANDS, st, 4);
                 TD_TRY(build_chunk_operands(e, c0, Ncur, fmt, lo, e->chunk_ops.base, co, st));
             }
             // GEMM1: [a | b] = B1 . V^T      (M x 2Nc, K = Kp)
@@ -1563,9 +1597,228 @@ static int perturb_average_vjp_mixed(tdscha_ensemble *e, int nb, const double *R
     return 0;
 }
 
+// TDSCHA_VJP_FREQ=0 keeps the averages' VJP on the rows over every symmetry (read at every call).
+static bool vjp_freq_enabled() {
+    const char *env = getenv("TDSCHA_VJP_FREQ");
+    return !(env && atoi(env) == 0);
+}
+
+// ------------------------------------------------------------------------------------------------
+// The averages' VJP on the character classes (freq.cuh): the forward quantities and the cotangent
+// transforms class by class, coefficients in the character basis, transposed contractions over the
+// class rows.  Inputs in the ensemble's rotated basis; resident class operands (no configuration
+// chunks).
+// ------------------------------------------------------------------------------------------------
+static int ensure_freq_yx_rows(tdscha_ensemble *e, Format fmt, bool lo, cudaStream_t st) {
+    const FreqTables &ft = *e->freq;
+    if (ft.Kmq == 0) return 0;
+    if (e->fyx_hi[fmt] && (!lo || e->fyx_lo[fmt])) return 0;
+    const size_t bytes = (size_t)e->N2 * ft.Kmq * format_bytes(fmt);
+    if (!e->fyx_hi[fmt]) TD_CUDA(cudaMalloc(&e->fyx_hi[fmt], bytes));
+    if (lo && !e->fyx_lo[fmt]) TD_CUDA(cudaMalloc(&e->fyx_lo[fmt], bytes));
+    return freq_build_mode_rows(ft, e->Y, e->Xt, e->n, e->N, fmt, e->fyx_hi[fmt], lo ? e->fyx_lo[fmt] : nullptr, st);
+}
+
+static int perturb_average_vjp_freq(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
+                                    const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
+                                    Format fmt, int nprod, bool lo) {
+    const FreqTables &ft = *e->freq;
+    const SymCosets *cs = e->cosets;
+    const int n_cos = cs->n_cos, sub = cs->sub, nC = ft.n_class, N = e->N, n = e->n;
+    const bool f64 = fmt == FMT_F64;
+    const size_t es = format_bytes(fmt), as = f64 ? 8 : 4, nh = lo ? 2 : 1;
+    const long long Kq = ft.Kq, Kmq1 = std::max(ft.Kmq, 1), ld1 = round_up(e->N2, 4);
+    TD_TRY(ensure_freq_operands(e, fmt, lo, st));
+    TD_TRY(ensure_freq_yx_rows(e, fmt, lo, st));
+    const FreqOps &co = e->fops[fmt];
+    // workspace: fixed part, then per coset (NR = nb * cosets of the chunk, NRp = NR rounded to 64)
+    const size_t fixed = as * ((size_t)N * Kq + 2 * (size_t)N * Kmq1 + (size_t)N * e->Kp + 2 * (size_t)N * e->np) +
+                         8 * ((size_t)N + (size_t)nb * n + (size_t)nb * n * n) + 32 * 256;
+    auto per_chunk = [&](int ncj) {
+        const size_t NR = (size_t)nb * ncj, NRp = round_up(NR, 64), rows = (size_t)nC * 2 * NR;
+        size_t b = 2 * as * (NR * e->Kp + NR * e->np);                      // U, r1, Q, phi
+        b += 2 * es * nh * (2 * NR * Kq + 2 * NR * Kmq1);                    // Lab, LQ, Lcd, Lphi
+        if (!f64) b += 2 * es * nh * ((size_t)Kq * 2 * NRp + (size_t)Kmq1 * 2 * NRp);   // their transposes
+        b += 4 * as * rows * ld1;                                            // H, Ch, HQ, Cp
+        b += f64 ? 4 * 8 * rows * ld1 : 4 * es * nh * (size_t)N * nC * 2 * NRp;   // K1..K4
+        b += 8 * rows * (size_t)N;                                           // BR
+        return b + 32 * 256;
+    };
+    size_t free_b = 0, tot_b = 0;
+    TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
+    const size_t budget = std::max<size_t>((size_t)1 << 30, (size_t)((free_b + e->vjp_ws.bytes) * 0.5));
+    TD_CHECK(budget > fixed + per_chunk(1), TDSCHA_ENOMEM, "not enough device memory for the averages' VJP");
+    int ncj = n_cos;
+    while (ncj > 1 && fixed + per_chunk(ncj) > budget) ncj = (ncj + 1) / 2;
+    const size_t need = fixed + per_chunk(ncj);
+    if (e->vjp_ws.bytes < need) {
+        if (e->vjp_ws.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->vjp_ws.base); e->vjp_ws = Workspace(); }
+        TD_CUDA(cudaMalloc(&e->vjp_ws.base, need));
+        e->vjp_ws.bytes = need;
+    }
+    uint8_t *W = static_cast<uint8_t *>(e->vjp_ws.base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { void *p = W + off; off += (bytes + 255) / 256 * 256; return p; };
+    const long long NRmax = (long long)nb * ncj, NRpmax = round_up(NRmax, 64), rowsmax = (long long)nC * 2 * NRmax;
+    void *VbarQ = take(as * (size_t)N * Kq), *GQ = take(as * (size_t)N * Kmq1), *YQ = take(as * (size_t)N * Kmq1);
+    void *Vbar = take(as * (size_t)N * e->Kp), *gbar = take(as * (size_t)N * e->np), *ypart = take(as * (size_t)N * e->np);
+    double *colsum = static_cast<double *>(take(8 * (size_t)N));
+    double *Rq = static_cast<double *>(take(8 * (size_t)nb * n)), *Dq = static_cast<double *>(take(8 * (size_t)nb * n * n));
+    void *U = take(as * NRmax * e->Kp), *r1 = take(as * NRmax * e->np), *Q = take(as * NRmax * e->Kp), *phi = take(as * NRmax * e->np);
+    auto pair_of = [&](size_t count) { void *h = take(count * es); void *l = lo ? take(count * es) : nullptr; return std::make_pair(h, l); };
+    auto Lab = pair_of(2 * NRmax * Kq), LQ = pair_of(2 * NRmax * Kq), Lcd = pair_of(2 * NRmax * Kmq1), Lph = pair_of(2 * NRmax * Kmq1);
+    std::pair<void *, void *> LabT{nullptr, nullptr}, LQT{nullptr, nullptr}, LcdT{nullptr, nullptr}, LphT{nullptr, nullptr};
+    if (!f64) {
+        LabT = pair_of((size_t)Kq * 2 * NRpmax);
+        LQT = pair_of((size_t)Kq * 2 * NRpmax);
+        LcdT = pair_of((size_t)Kmq1 * 2 * NRpmax);
+        LphT = pair_of((size_t)Kmq1 * 2 * NRpmax);
+    }
+    void *H = take(as * rowsmax * ld1), *Ch = take(as * rowsmax * ld1), *HQ = take(as * rowsmax * ld1), *Cp = take(as * rowsmax * ld1);
+    std::pair<void *, void *> Ks[4];
+    for (auto &k : Ks) k = f64 ? std::make_pair(take(8 * rowsmax * ld1), (void *)nullptr) : pair_of((size_t)N * nC * 2 * NRpmax);
+    double *BR = static_cast<double *>(take(8 * rowsmax * (size_t)N));
+    TD_CHECK(off <= e->vjp_ws.bytes, TDSCHA_EINVAL, "VJP workspace layout exceeds its allocation");
+    TD_CUDA(cudaMemsetAsync(colsum, 0, 8 * (size_t)N, st));
+    vjp_cotangent_kernel<<<grid_for((long long)nb * n * n), 256, 0, st>>>(nb, n, fbar, Dbar, e->ups, Rq, Dq);
+    TD_CUDA(cudaGetLastError());
+    SymTables tr{e->sym, e->d_blk_sym_off, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, cs->repP, cs->repPT, cs->d_offRep};
+    SymTables t64{cs->repS, cs->d_offRepS, e->d_blk_start, e->d_blk_dim, e->n_blocks, e->n, e->dmax, nullptr, nullptr, nullptr};
+    bool first = true;
+    for (int p0 = 0; p0 < n_cos; p0 += ncj) {
+        const int nc = std::min(ncj, n_cos - p0);
+        const int NR = nb * nc, NRp = (int)round_up(NR, 64);
+        const long long RT = (long long)nC * 2 * NRp, rows = (long long)nC * 2 * NR;
+        // transforms over the representatives and left operands
+        if (f64) {
+            TD_TRY(sym_transform(t64, e->pairs, nb, nc, p0, Ys, R1, e->ups, e->P, e->Kp, e->np, FMT_F64, U, nullptr, r1, nullptr, false, st));
+            TD_TRY(sym_transform(t64, e->pairs, nb, nc, p0, Dq, Rq, e->ups, e->P, e->Kp, e->np, FMT_F64, Q, nullptr, phi, nullptr, false, st));
+            TD_TRY(freq_left<double>(ft, NR, n, (const double *)U, e->Kp, (const double *)r1, e->np, fmt, Lab.first, Lab.second,
+                                     Lcd.first, Lcd.second, st));
+            TD_TRY(freq_left<double>(ft, NR, n, (const double *)Q, e->Kp, (const double *)phi, e->np, fmt, LQ.first, LQ.second,
+                                     Lph.first, Lph.second, st));
+        } else {
+            TD_TRY(sym_transform_tc(tr, e->pairs, nb, nc, p0, Ys, R1, e->ups, e->Kp, e->np, FMT_F32, U, nullptr, r1, nullptr, st));
+            TD_TRY(sym_transform_tc(tr, e->pairs, nb, nc, p0, Dq, Rq, e->ups, e->Kp, e->np, FMT_F32, Q, nullptr, phi, nullptr, st));
+            TD_TRY(freq_left<float>(ft, NR, n, (const float *)U, e->Kp, (const float *)r1, e->np, fmt, Lab.first, Lab.second,
+                                    Lcd.first, Lcd.second, st));
+            TD_TRY(freq_left<float>(ft, NR, n, (const float *)Q, e->Kp, (const float *)phi, e->np, fmt, LQ.first, LQ.second,
+                                    Lph.first, Lph.second, st));
+        }
+        // forward class contractions: [a|b], [c|d] of (U, r1) and [A'|B'], [C'|D'] of (Q, phi)
+        std::vector<tc::GemmGroup> gab, gcd;
+        for (int g = 0; g < nC; ++g) {
+            const int Mg = ft.cls_real[g] ? NR : 2 * NR;
+            const long long hrow = (long long)g * 2 * NR;
+            gab.push_back({Mg, (int)e->N2, ft.pcol_cnt[g], 0, ft.pcol_off[g], 0, ft.pcol_off[g], hrow * ld1});
+            if (ft.mcol_cnt[g] > 0) {
+                gcd.push_back({Mg, (int)e->N2, ft.mcol_cnt[g], 0, ft.mcol_off[g], 0, ft.mcol_off[g], hrow * ld1});
+            } else {
+                TD_CUDA(cudaMemsetAsync(static_cast<uint8_t *>(Ch) + hrow * ld1 * as, 0, (size_t)2 * NR * ld1 * as, st));
+                TD_CUDA(cudaMemsetAsync(static_cast<uint8_t *>(Cp) + hrow * ld1 * as, 0, (size_t)2 * NR * ld1 * as, st));
+            }
+        }
+        TD_TRY(gemm_groups(e, fmt, nprod, Lab.first, Lab.second, 2LL * NR, Kq, co.V_hi, co.V_lo, e->N2, Kq, gab, H, ld1, false, st));
+        TD_TRY(gemm_groups(e, fmt, nprod, LQ.first, LQ.second, 2LL * NR, Kq, co.V_hi, co.V_lo, e->N2, Kq, gab, HQ, ld1, false, st));
+        TD_TRY(gemm_groups(e, fmt, nprod, Lcd.first, Lcd.second, 2LL * NR, Kmq1, co.XG_hi, co.XG_lo, e->N2, Kmq1, gcd, Ch, ld1, false, st));
+        TD_TRY(gemm_groups(e, fmt, nprod, Lph.first, Lph.second, 2LL * NR, Kmq1, e->fyx_hi[fmt], lo ? e->fyx_lo[fmt] : nullptr,
+                           e->N2, Kmq1, gcd, Cp, ld1, false, st));
+        // coefficients and the rho pairing
+        void *Kh[4] = {Ks[0].first, Ks[1].first, Ks[2].first, Ks[3].first};
+        void *Kl[4] = {Ks[0].second, Ks[1].second, Ks[2].second, Ks[3].second};
+        if (f64) {
+            TD_TRY(freq_vjp_coef<double>(ft, sub, (const double *)H, (const double *)Ch, (const double *)HQ, (const double *)Cp, ld1,
+                                         N, NR, NRp, apply_d4, false, fmt, Kh, Kl, ld1, BR, st));
+        } else {
+            for (int q = 0; q < 4; ++q) {
+                TD_CUDA(cudaMemsetAsync(Kh[q], 0, (size_t)N * RT * es, st));
+                if (lo) TD_CUDA(cudaMemsetAsync(Kl[q], 0, (size_t)N * RT * es, st));
+            }
+            TD_TRY(freq_vjp_coef<float>(ft, sub, (const float *)H, (const float *)Ch, (const float *)HQ, (const float *)Cp, ld1, N,
+                                        NR, NRp, apply_d4, true, fmt, Kh, Kl, RT, BR, st));
+        }
+        vjp_colsum_kernel<<<ceil_div(N, 256), 256, 0, st>>>(rows, N, BR, colsum);
+        TD_CUDA(cudaGetLastError());
+        // transposed contractions over the class rows
+        if (f64) {
+            std::vector<std::array<long long, 5>> gp, gm;
+            for (int g = 0; g < nC; ++g) {
+                const long long row0 = (long long)g * 2 * NR, nr = ft.cls_real[g] ? NR : 2 * NR;
+                gp.push_back({row0, nr, ft.pcol_off[g], ft.pcol_cnt[g], 0});
+                if (ft.mcol_cnt[g] > 0) gm.push_back({row0, nr, ft.mcol_off[g], ft.mcol_cnt[g], 0});
+            }
+            // the left operands' rows start at 0 for every class: offset K by the class block, R by 0
+            auto run = [&](const std::vector<std::array<long long, 5>> &gs, const double *K, const void *R, long long ldr, void *C,
+                           long long ldc, bool acc) {
+                const double one = 1.0, beta = acc ? 1.0 : 0.0;
+                cublasSetStream(e->cublas, st);
+                for (const auto &g : gs) {
+                    cublasStatus_t s2 = cublasDgemm(e->cublas, CUBLAS_OP_N, CUBLAS_OP_T, (int)g[3], N, (int)g[1], &one,
+                                                    static_cast<const double *>(R) + g[2], (int)ldr, K + g[0] * ld1, (int)ld1, &beta,
+                                                    static_cast<double *>(C) + g[2], (int)ldc);
+                    TD_CHECK(s2 == CUBLAS_STATUS_SUCCESS, TDSCHA_ECUDA, "cublasDgemm failed (%d)", (int)s2);
+                }
+                return 0;
+            };
+            TD_TRY(run(gp, (const double *)Kh[0], Lab.first, Kq, VbarQ, Kq, !first));
+            TD_TRY(run(gp, (const double *)Kh[1], LQ.first, Kq, VbarQ, Kq, true));
+            TD_TRY(run(gm, (const double *)Kh[2], Lcd.first, Kmq1, GQ, Kmq1, !first));
+            TD_TRY(run(gm, (const double *)Kh[3], Lph.first, Kmq1, YQ, Kmq1, !first));
+        } else {
+            TD_TRY(freq_transpose_left(fmt, Lab.first, NR, NRp, Kq, LabT.first, st));
+            TD_TRY(freq_transpose_left(fmt, LQ.first, NR, NRp, Kq, LQT.first, st));
+            TD_TRY(freq_transpose_left(fmt, Lcd.first, NR, NRp, Kmq1, LcdT.first, st));
+            TD_TRY(freq_transpose_left(fmt, Lph.first, NR, NRp, Kmq1, LphT.first, st));
+            if (lo) {
+                TD_TRY(freq_transpose_left(fmt, Lab.second, NR, NRp, Kq, LabT.second, st));
+                TD_TRY(freq_transpose_left(fmt, LQ.second, NR, NRp, Kq, LQT.second, st));
+                TD_TRY(freq_transpose_left(fmt, Lcd.second, NR, NRp, Kmq1, LcdT.second, st));
+                TD_TRY(freq_transpose_left(fmt, Lph.second, NR, NRp, Kmq1, LphT.second, st));
+            }
+            std::vector<tc::GemmGroup> gp, gm;
+            for (int g = 0; g < nC; ++g) {
+                const int Kg = ft.cls_real[g] ? NRp : 2 * NRp;
+                const int a_k = g * 2 * NRp;
+                gp.push_back({N, ft.pcol_cnt[g], Kg, 0, a_k, ft.pcol_off[g], 0, (long long)ft.pcol_off[g]});
+                if (ft.mcol_cnt[g] > 0) gm.push_back({N, ft.mcol_cnt[g], Kg, 0, a_k, ft.mcol_off[g], 0, (long long)ft.mcol_off[g]});
+            }
+            TD_TRY(gemm_groups(e, fmt, nprod, Kh[0], Kl[0], N, RT, LabT.first, LabT.second, Kq, 2LL * NRp, gp, VbarQ, Kq, !first, st));
+            TD_TRY(gemm_groups(e, fmt, nprod, Kh[1], Kl[1], N, RT, LQT.first, LQT.second, Kq, 2LL * NRp, gp, VbarQ, Kq, true, st));
+            TD_TRY(gemm_groups(e, fmt, nprod, Kh[2], Kl[2], N, RT, LcdT.first, LcdT.second, Kmq1, 2LL * NRp, gm, GQ, Kmq1, !first, st));
+            TD_TRY(gemm_groups(e, fmt, nprod, Kh[3], Kl[3], N, RT, LphT.first, LphT.second, Kmq1, 2LL * NRp, gm, YQ, Kmq1, !first, st));
+        }
+        first = false;
+    }
+    const double norm = 1.0 / (e->N_eff * (double)e->N_sym);
+    if (f64) {
+        TD_TRY(freq_vjp_reconstruct<double>(ft, N, n, e->P, (const double *)VbarQ, (const double *)GQ, (const double *)YQ,
+                                            (double *)Vbar, e->Kp, (double *)gbar, (double *)ypart, e->np, st));
+        vjp_matvec_kernel<double><<<N, 256, (size_t)n * sizeof(double), st>>>(N, n, e->Kp, e->np, (const double *)Vbar, e->X, (double *)gbar);
+        vjp_final_kernel<double><<<grid_for((long long)N * n), 256, 0, st>>>(N, n, e->np, norm, e->rho, e->psi, (const double *)gbar,
+                                                                             (const double *)ypart, Ybar);
+    } else {
+        TD_TRY(freq_vjp_reconstruct<float>(ft, N, n, e->P, (const float *)VbarQ, (const float *)GQ, (const float *)YQ,
+                                           (float *)Vbar, e->Kp, (float *)gbar, (float *)ypart, e->np, st));
+        vjp_matvec_kernel<float><<<N, 256, (size_t)n * sizeof(double), st>>>(N, n, e->Kp, e->np, (const float *)Vbar, e->X, (float *)gbar);
+        vjp_final_kernel<float><<<grid_for((long long)N * n), 256, 0, st>>>(N, n, e->np, norm, e->rho, e->psi, (const float *)gbar,
+                                                                            (const float *)ypart, Ybar);
+    }
+    vjp_rho_kernel<<<1, 256, 0, st>>>(N, norm, e->N_eff, e->rho, colsum, rhobar);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 static int vjp_in_ensemble_basis(tdscha_ensemble *e, int nb, const double *R1, const double *Ys, int apply_d4,
                                  const double *fbar, const double *Dbar, double *Ybar, double *rhobar, cudaStream_t st,
                                  int precision) {
+    if (e->freq && use_freq_path(e, format_of(precision)) && vjp_freq_enabled()) {
+        TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
+        TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);
+        TD_CHECK(R1 && Ys && fbar && Dbar && Ybar && rhobar, TDSCHA_EINVAL, "NULL argument");
+        TD_CHECK(precision >= 0 && precision <= TDSCHA_PREC_BF16, TDSCHA_EINVAL, "unknown precision %d", precision);
+        return perturb_average_vjp_freq(e, nb, R1, Ys, apply_d4, fbar, Dbar, Ybar, rhobar, st, format_of(precision),
+                                        products_of(precision), needs_lo(precision));
+    }
     if (precision != TDSCHA_PREC_FP64) {
         TD_CHECK(nb > 0, TDSCHA_EINVAL, "nb must be positive");
         TD_CHECK(apply_d4 == 0 || apply_d4 == 1, TDSCHA_EINVAL, "apply_D4 must be 0 or 1 (got %d)", apply_d4);

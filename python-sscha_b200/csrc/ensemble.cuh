@@ -59,7 +59,7 @@ struct AvgPlan {
 };
 
 // Stages of one averages call, for the optional CUDA-event profile.
-enum Stage : int { ST_TRANSFORM = 0, ST_GEMM_AB, ST_GEMM_CD, ST_WEIGHTS, ST_GEMM_Z, ST_GEMM_F, ST_FOLD, ST_OTHER, ST_COUNT };
+enum Stage : int { ST_TRANSFORM = 0, ST_GEMM_AB, ST_GEMM_CD, ST_WEIGHTS, ST_GEMM_Z, ST_GEMM_F, ST_FOLD, ST_OTHER, ST_OPERANDS, ST_COUNT };
 
 struct ProfRec {
     int stage;
@@ -116,6 +116,8 @@ struct tdscha_ensemble {
     tdscha::SymCosets *cosets = nullptr;           // factorised symmetry transform / fold (mixed formats)
     tdscha::FreqTables *freq = nullptr;            // character classes of the subgroup (freq.cuh)
     tdscha::FreqOps fops[3];                       // character-basis operands per storage format (resident)
+    void *fyx_hi[3] = {nullptr, nullptr, nullptr};  // [Y; X~] mode components (2N x Kmq) per format (class VJP)
+    void *fyx_lo[3] = {nullptr, nullptr, nullptr};
     tdscha::Workspace rot_ws;                      // rotated inputs / outputs of the VJP
 };
 

@@ -186,6 +186,7 @@ int build_freq_layout(int n, const std::vector<int> &dim, const std::vector<int>
         int mcnt = 0;
         for (int k : mby_cls[g]) { mcomps[k].col = kmq + mcnt; mcnt += mcomps[k].qb >= 0 ? 2 : 1; }
         out.mcol_cnt.push_back(mcnt ? (int)round_up(mcnt, 64) : 0);
+        out.mcol_used.push_back(mcnt);
         kmq += out.mcol_cnt.back();
         (void)id;
     }
@@ -394,6 +395,95 @@ __global__ void __launch_bounds__(256) build_Vq_tiles_kernel(const double *__res
     }
 }
 
+// The same from the transposed ensemble XGT = [X^T ; G^T] (2n x ldT, configuration-contiguous): one
+// CTA per (COLS component columns, 256 configuration rows of [x x^T ; sym(x g^T)]), one thread per
+// configuration row; every read of XGT is a coalesced row segment, and consecutive CTAs share the
+// same 256 configurations (x fastest), whose XGT block (2n x 256) stays in L2 while every column
+// tile is built from it.  VqT rows go out directly (512 B per warp), Vq rows through shared memory.
+template <typename T>
+__global__ void __launch_bounds__(256) build_Vq_cols_kernel(const double *__restrict__ XGT, long long ldT, int n, long long Nc,
+                                                            long long N2pc, int Kq, const int *__restrict__ mu0,
+                                                            const int *__restrict__ nu0, const int *__restrict__ mu1,
+                                                            const int *__restrict__ nu1, const double *__restrict__ c0,
+                                                            const double *__restrict__ c1, Format fmt, T *__restrict__ V_hi,
+                                                            T *__restrict__ V_lo, T *__restrict__ VT_hi, T *__restrict__ VT_lo) {
+    constexpr int COLS = sizeof(T) == 2 ? 64 : 32;   // 128 bytes of a Vq row
+    constexpr int LDS = 257;                          // shared row length (conflict-free column reads)
+    extern __shared__ __align__(16) uint8_t smem_raw[];
+    T *th = reinterpret_cast<T *>(smem_raw);          // [COLS][LDS]
+    T *tl = th + COLS * LDS;
+    const int cb = blockIdx.x * COLS;
+    const long long k0 = (long long)blockIdx.y * 256;
+    const int t = threadIdx.x;
+    const long long k = k0 + t;
+    const bool lo = V_lo != nullptr;
+    const bool second = k >= Nc && k < 2 * Nc;
+    const bool live = k < 2 * Nc;
+    const long long i = second ? k - Nc : k;
+    for (int cc = 0; cc < COLS; ++cc) {
+        const int c = cb + cc;
+        double v = 0.0;
+        if (live) {
+            const int a0 = __ldg(mu0 + c), b0 = __ldg(nu0 + c), a1 = __ldg(mu1 + c), b1 = __ldg(nu1 + c);
+            const double f0 = __ldg(c0 + c), f1 = __ldg(c1 + c);
+            const double xa0 = XGT[(long long)a0 * ldT + i], xb0 = XGT[(long long)b0 * ldT + i];
+            const double xa1 = XGT[(long long)a1 * ldT + i], xb1 = XGT[(long long)b1 * ldT + i];
+            if (!second) {
+                v = f0 * xa0 * xb0 + f1 * xa1 * xb1;
+            } else {
+                const double *G = XGT + (long long)n * ldT;
+                v = 0.5 * (f0 * (xa0 * G[(long long)b0 * ldT + i] + xb0 * G[(long long)a0 * ldT + i]) +
+                           f1 * (xa1 * G[(long long)b1 * ldT + i] + xb1 * G[(long long)a1 * ldT + i]));
+            }
+        }
+        T h, l;
+        split_to<T>(fmt, v, h, l);
+        if (k < N2pc) {
+            VT_hi[(long long)c * N2pc + k] = h;
+            if (lo) VT_lo[(long long)c * N2pc + k] = l;
+        }
+        th[cc * LDS + t] = h;
+        tl[cc * LDS + t] = l;
+    }
+    __syncthreads();
+    // Vq rows k < 2Nc: one warp per row and pass, COLS columns as 32-bit words
+    constexpr int EPW = sizeof(T) == 2 ? 2 : 1;
+    constexpr int WPR = COLS / EPW;   // = 32
+    const int warp = t >> 5, lane = t & 31;
+    for (int r = warp; r < 256; r += 8) {
+        const long long kr = k0 + r;
+        if (kr >= 2 * Nc) break;
+        const int j = lane * EPW;
+        if constexpr (EPW == 2) {
+            *reinterpret_cast<uint32_t *>(V_hi + kr * Kq + cb + j) =
+                (uint32_t)th[j * LDS + r] | ((uint32_t)th[(j + 1) * LDS + r] << 16);
+            if (lo)
+                *reinterpret_cast<uint32_t *>(V_lo + kr * Kq + cb + j) =
+                    (uint32_t)tl[j * LDS + r] | ((uint32_t)tl[(j + 1) * LDS + r] << 16);
+        } else {
+            V_hi[kr * Kq + cb + j] = th[j * LDS + r];
+            if (lo) V_lo[kr * Kq + cb + j] = tl[j * LDS + r];
+        }
+        static_assert(WPR == 32, "one warp per Vq row");
+    }
+}
+
+template <typename T>
+int build_Vq_cols(const FreqTables &t, const double *XGT, long long ldT, int n, long long Nc, long long N2pc, Format fmt,
+                  void *V_hi, void *V_lo, void *VT_hi, void *VT_lo, cudaStream_t st) {
+    constexpr int COLS = sizeof(T) == 2 ? 64 : 32;
+    TD_CHECK(t.Kq % COLS == 0 && N2pc % 64 == 0 && ceil_div(N2pc, 256) <= 65535, TDSCHA_EINVAL, "operand build: %lld x %d",
+             N2pc, t.Kq);
+    const size_t smem = (size_t)2 * COLS * 257 * sizeof(T);
+    auto kern = build_Vq_cols_kernel<T>;
+    TD_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const dim3 grid((unsigned)(t.Kq / COLS), (unsigned)ceil_div(N2pc, 256));
+    kern<<<grid, 256, smem, st>>>(XGT, ldT, n, Nc, N2pc, t.Kq, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0, t.pc_c1, fmt,
+                                  static_cast<T *>(V_hi), static_cast<T *>(V_lo), static_cast<T *>(VT_hi), static_cast<T *>(VT_lo));
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 template <typename T>
 int build_Vq_tiles(const FreqTables &t, const double *X, const double *G, int n, long long Nc, long long N2pc, Format fmt,
                    void *V_hi, void *V_lo, void *VT_hi, void *VT_lo, cudaStream_t st) {
@@ -583,6 +673,98 @@ __global__ void __launch_bounds__(256) freq_weights_kernel(const AccT *__restric
     }
 }
 
+template <Format FMT>
+__device__ __forceinline__ float split_value(const void *hi, const void *lo, long long idx) {
+    if constexpr (FMT == FMT_BF16) {
+        float v = bf16_bits_to_float(static_cast<const uint16_t *>(hi)[idx]);
+        if (lo) v += bf16_bits_to_float(static_cast<const uint16_t *>(lo)[idx]);
+        return v;
+    } else {
+        float v = static_cast<const float *>(hi)[idx];
+        if (lo) v += static_cast<const float *>(lo)[idx];
+        return v;
+    }
+}
+
+// One CTA per (32 rows of one class, 128 configurations): the class's mode components of the
+// configurations (x and g) and of the rows' left operands in shared memory (fp32, padded to 65
+// columns), then per (row, configuration) the dot products c, d and the weights.
+template <Format FMT>
+__global__ void __launch_bounds__(256) weights_cd_kernel(const float *__restrict__ H, long long ld, const void *Lcd_hi,
+                                                         const void *Lcd_lo, const void *XG_hi, const void *XG_lo, int Kmq,
+                                                         const double *__restrict__ rho, long long Nc, int NR, int tiles_per_class,
+                                                         const int *__restrict__ cls_real, const int *__restrict__ mcol_off,
+                                                         const int *__restrict__ mcol_used, long long N2pc, int d4, void *Cw_hi,
+                                                         void *Cw_lo, void *AB_hi, void *AB_lo) {
+    extern __shared__ __align__(16) float wsm[];
+    float *Xs = wsm;                   // [128][65]
+    float *Gs = Xs + 128 * 65;         // [128][65]
+    float *Ls = Gs + 128 * 65;         // [32][65]
+    const int g = blockIdx.y;
+    const int Kc = mcol_used[g], moff = mcol_off[g];
+    const bool real_cls = cls_real[g] != 0;
+    const int rows_cls = real_cls ? NR : 2 * NR;
+    const long long i0 = (long long)blockIdx.x * 128;
+    const int tid = threadIdx.x;
+    for (int e = tid; e < 128 * 64; e += 256) {
+        const int ii = e >> 6, cc = e & 63;
+        const long long i = i0 + ii;
+        float xv = 0.f, gv = 0.f;
+        if (cc < Kc && i < Nc) {
+            xv = split_value<FMT>(XG_hi, XG_lo, i * Kmq + moff + cc);
+            gv = split_value<FMT>(XG_hi, XG_lo, (Nc + i) * Kmq + moff + cc);
+        }
+        Xs[ii * 65 + cc] = xv;
+        Gs[ii * 65 + cc] = gv;
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    const float k4 = d4 ? 1.f : 0.f;
+    // the configuration slice stays in shared memory while the CTA walks every row tile of the class
+    for (int tb = 0; tb * 32 < rows_cls; ++tb) {
+    __syncthreads();
+    for (int e = tid; e < 32 * 64; e += 256) {
+        const int rr = e >> 6, cc = e & 63;
+        const int lr = tb * 32 + rr;   // row inside the class: comp * NR + j
+        float v = 0.f;
+        if (cc < Kc && lr < rows_cls) v = split_value<FMT>(Lcd_hi, Lcd_lo, (long long)lr * Kmq + moff + cc);
+        Ls[rr * 65 + cc] = v;
+    }
+    __syncthreads();
+    for (int rr = warp; rr < 32; rr += 8) {
+        const int lr = tb * 32 + rr;
+        if (lr >= rows_cls) break;
+        const long long r = (long long)g * 2 * NR + lr;
+        const float *h = H + r * ld;
+        const float *l = Ls + rr * 65;
+        for (int q = 0; q < 4; ++q) {
+            const int ii = lane + 32 * q;
+            const long long i = i0 + ii;
+            if (i >= Nc) break;
+            const float *xs = Xs + ii * 65, *gs = Gs + ii * 65;
+            float c = 0.f, d = 0.f;
+            for (int cc = 0; cc < Kc; ++cc) {
+                c = fmaf(l[cc], xs[cc], c);
+                d = fmaf(l[cc], gs[cc], d);
+            }
+            const float a = h[i], b = h[Nc + i];
+            const float rh = (float)rho[i];
+            const float gam = rh * (-c * (1.f / 3.f) + k4 * a * 0.125f);
+            const float hdel = 0.5f * rh * (-d * (1.f / 3.f) + k4 * b * 0.25f);
+            const long long o = r * N2pc;
+            store_split(FMT, Cw_hi, Cw_lo, o + i, (double)hdel);
+            store_split(FMT, Cw_hi, Cw_lo, o + Nc + i, (double)gam);
+            store_split(FMT, AB_hi, AB_lo, o + i, (double)(-rh * a * (1.f / 6.f)));
+            store_split(FMT, AB_hi, AB_lo, o + Nc + i, (double)(-rh * b * (1.f / 3.f)));
+        }
+        if (blockIdx.x == 0)
+            for (long long k = 2 * Nc + lane; k < N2pc; k += 32) {
+                store_split(FMT, Cw_hi, Cw_lo, r * N2pc + k, 0.0);
+                store_split(FMT, AB_hi, AB_lo, r * N2pc + k, 0.0);
+            }
+    }
+    }
+}
+
 }  // namespace
 
 template <typename AccT>
@@ -603,6 +785,30 @@ int freq_weights(const FreqTables &t, const AccT *H, const AccT *Ch, long long l
     return 0;
 }
 
+int freq_weights_cd(const FreqTables &t, const float *H, long long ld, const void *Lcd_hi, const void *Lcd_lo, const void *XG_hi,
+                    const void *XG_lo, const double *rho, long long Nc, int NR, long long N2pc, int d4, Format fmt, void *Cw_hi,
+                    void *Cw_lo, void *AB_hi, void *AB_lo, cudaStream_t st) {
+    TD_CHECK(fmt == FMT_BF16 || fmt == FMT_TF32, TDSCHA_EINVAL, "fused weights need a split format");
+    TD_CHECK(t.Kmq > 0, TDSCHA_EINVAL, "fused weights need mode columns");
+    const int tiles_per_class = ceil_div(2 * NR, 32);
+    const long long gy = t.n_class;
+    const size_t smem = (size_t)(2 * 128 + 32) * 65 * sizeof(float);
+    const dim3 grid((unsigned)ceil_div(Nc, 128), (unsigned)gy);
+    if (fmt == FMT_BF16) {
+        TD_CUDA(cudaFuncSetAttribute(weights_cd_kernel<FMT_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        weights_cd_kernel<FMT_BF16><<<grid, 256, smem, st>>>(H, ld, Lcd_hi, Lcd_lo, XG_hi, XG_lo, t.Kmq, rho, Nc, NR, tiles_per_class,
+                                                             t.d_cls_real, t.d_mcol_off, t.d_mcol_used, N2pc, d4, Cw_hi, Cw_lo,
+                                                             AB_hi, AB_lo);
+    } else {
+        TD_CUDA(cudaFuncSetAttribute(weights_cd_kernel<FMT_TF32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        weights_cd_kernel<FMT_TF32><<<grid, 256, smem, st>>>(H, ld, Lcd_hi, Lcd_lo, XG_hi, XG_lo, t.Kmq, rho, Nc, NR, tiles_per_class,
+                                                             t.d_cls_real, t.d_mcol_off, t.d_mcol_used, N2pc, d4, Cw_hi, Cw_lo,
+                                                             AB_hi, AB_lo);
+    }
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
 template int freq_weights<float>(const FreqTables &, const float *, const float *, long long, const double *, long long, int,
                                  long long, int, Format, void *, void *, void *, void *, cudaStream_t);
 template int freq_weights<double>(const FreqTables &, const double *, const double *, long long, const double *, long long,
@@ -619,6 +825,7 @@ int freq_tables_create(const FreqLayout &L, FreqTables **out) {
     t->pcol_cnt = L.pcol_cnt;
     t->mcol_off = L.mcol_off;
     t->mcol_cnt = L.mcol_cnt;
+    t->mcol_used = L.mcol_used;
     t->flops_ratio = L.flops_ratio;
     size_t acc = 0;
     int rc = 0;
@@ -632,7 +839,8 @@ int freq_tables_create(const FreqLayout &L, FreqTables **out) {
         (rc = upload(L.mc_mode, &t->mc_mode, &acc)) || (rc = upload(L.mc_partner, &t->mc_partner, &acc)) ||
         (rc = upload(L.mode_col, &t->mode_col, &acc)) || (rc = upload(L.mc_sign, &t->mc_sign, &acc)) ||
         (rc = upload(L.mc_re, &t->mc_re, &acc)) || (rc = upload(L.mc_im, &t->mc_im, &acc)) ||
-        (rc = upload(L.mc_zc, &t->mc_zc, &acc)) || (rc = upload(L.cls_real, &t->d_cls_real, &acc))) {
+        (rc = upload(L.mc_zc, &t->mc_zc, &acc)) || (rc = upload(L.cls_real, &t->d_cls_real, &acc)) ||
+        (rc = upload(L.mcol_off, &t->d_mcol_off, &acc)) || (rc = upload(L.mcol_used, &t->d_mcol_used, &acc))) {
         freq_tables_destroy(t);
         return rc;
     }
@@ -645,7 +853,7 @@ void freq_tables_destroy(FreqTables *t) {
     if (!t) return;
     void *ps[] = {t->pc_mu0, t->pc_nu0, t->pc_mu1, t->pc_nu1, t->pc_partner, t->pc_c0, t->pc_c1, t->pc_re, t->pc_im, t->pc_zc,
                   t->pp_col0, t->pp_col1, t->pp_c0, t->pp_c1, t->mc_mode, t->mc_partner, t->mode_col, t->mc_sign, t->mc_re,
-                  t->mc_im, t->mc_zc, t->d_cls_real};
+                  t->mc_im, t->mc_zc, t->d_cls_real, t->d_mcol_off, t->d_mcol_used};
     for (void *p : ps)
         if (p) cudaFree(p);
     delete t;
@@ -657,8 +865,9 @@ size_t freq_operand_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo
     return per * format_bytes(fmt) * (lo ? 2 : 1) + 8 * 256;
 }
 
-int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt, int n,
-                        long long Nc, Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st) {
+int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt,
+                        const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
+                        cudaStream_t st) {
     const size_t es = format_bytes(fmt);
     const long long N2pc = round_up(2 * Nc, 64);
     const long long nV = 2 * Nc * t.Kq, nVT = (long long)t.Kq * N2pc, nXG = 2 * Nc * t.Kmq, nYX = (long long)t.Kmq * N2pc;
@@ -678,7 +887,13 @@ int freq_build_operands(const FreqTables &t, const double *X, const double *G, c
     }
     // Vq and its transpose from shared-memory tiles (gathering the transpose from the ensemble per
     // component would re-read the ensemble rows once per component)
-    if (fmt == FMT_BF16)
+    // (from the transposed ensemble XGT when given: coalesced, L2-resident reads per configuration
+    // block; else gathering from the ensemble rows)
+    if (XGT && fmt == FMT_BF16)
+        TD_TRY(build_Vq_cols<uint16_t>(t, XGT, ldT, n, Nc, N2pc, fmt, o.V_hi, o.V_lo, o.VT_hi, o.VT_lo, st));
+    else if (XGT && fmt == FMT_TF32)
+        TD_TRY(build_Vq_cols<float>(t, XGT, ldT, n, Nc, N2pc, fmt, o.V_hi, o.V_lo, o.VT_hi, o.VT_lo, st));
+    else if (fmt == FMT_BF16)
         TD_TRY(build_Vq_tiles<uint16_t>(t, X, G, n, Nc, N2pc, fmt, o.V_hi, o.V_lo, o.VT_hi, o.VT_lo, st));
     else if (fmt == FMT_F64)
         TD_TRY(build_Vq_tiles<double>(t, X, G, n, Nc, N2pc, fmt, o.V_hi, nullptr, o.VT_hi, nullptr, st));
@@ -724,5 +939,206 @@ template int freq_reconstruct<float>(const FreqTables &, int, int, long long, co
                                      const float *, float *, long long, float *, long long, cudaStream_t);
 template int freq_reconstruct<double>(const FreqTables &, int, int, long long, const int *, const int *, const double *,
                                       const double *, double *, long long, double *, long long, cudaStream_t);
+
+}  // namespace tdscha
+
+// ================================================================================================
+// The averages' VJP in the character basis (device)
+// ================================================================================================
+namespace tdscha {
+namespace {
+
+template <typename T>
+__global__ void transpose_left_kernel(const T *__restrict__ L, int NR, int NRp, long long cols, T *__restrict__ out) {
+    __shared__ T tile[32][33];
+    const long long c0 = (long long)blockIdx.x * 32;
+    const int q0 = blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int q = q0 + j, comp = q / NRp, jj = q - comp * NRp;
+        const long long c = c0 + threadIdx.x;
+        T v = T(0);
+        if (comp < 2 && jj < NR && c < cols) v = L[(long long)(comp * NR + jj) * cols + c];
+        tile[j][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long c = c0 + j;
+        const int q = q0 + threadIdx.x;
+        if (c < cols && q < 2 * NRp) out[c * (2LL * NRp) + q] = tile[threadIdx.x][j];
+    }
+}
+
+// One thread per (row r, configuration i) of a 32 x 32 tile; TRANS: the K's go out transposed
+// through shared memory (coalesced along the rows).
+template <typename AccT, bool TRANS>
+__global__ void __launch_bounds__(256) vjp_coef_class_kernel(const AccT *__restrict__ H, const AccT *__restrict__ Ch,
+                                                             const AccT *__restrict__ HQ, const AccT *__restrict__ Cp,
+                                                             long long ld, int N, long long rows, int NR, int NRp,
+                                                             const int *__restrict__ cls_real, double inv_s_real,
+                                                             double inv_s_cplx, int d4, Format fmt, void *K1h, void *K1l,
+                                                             void *K2h, void *K2l, void *K3h, void *K3l, void *K4h, void *K4l,
+                                                             long long ldk, double *__restrict__ BR) {
+    __shared__ double ts[4][32][33];
+    const long long r0 = (long long)blockIdx.y * 32;
+    const int i0 = blockIdx.x * 32;
+    const double k4 = d4 ? 1.0 : 0.0;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long r = r0 + j;
+        const int i = i0 + threadIdx.x;
+        double v[4] = {0.0, 0.0, 0.0, 0.0};
+        if (r < rows && i < N) {
+            const long long g = r / (2LL * NR);
+            const long long rem = r - g * 2LL * NR;
+            const bool imag = rem >= NR;
+            const bool real_cls = cls_real[g] != 0;
+            if (!(imag && real_cls)) {
+                const long long o = r * ld;
+                const double a = (double)H[o + i], b = (double)H[o + N + i], c = (double)Ch[o + i], d = (double)Ch[o + N + i];
+                const double Ap = (double)HQ[o + i], Bp = (double)HQ[o + N + i], Cq = (double)Cp[o + i], Dq = (double)Cp[o + N + i];
+                const double kk2 = -c / 3.0 + k4 * a / 8.0;
+                v[0] = k4 * Ap / 8.0 - Dq / 3.0;
+                v[1] = kk2;
+                v[2] = -Ap / 6.0;
+                v[3] = -a / 6.0;
+                const double br = 0.5 * (-d / 3.0 + k4 * b / 4.0) * Ap + kk2 * Bp - a / 6.0 * Cq - b / 3.0 * Dq;
+                BR[r * N + i] = br * (real_cls ? inv_s_real : inv_s_cplx);
+            } else {
+                BR[r * N + i] = 0.0;
+            }
+            if constexpr (!TRANS) {
+                store_split(fmt, K1h, K1l, r * ldk + i, v[0]);
+                store_split(fmt, K2h, K2l, r * ldk + i, v[1]);
+                store_split(fmt, K3h, K3l, r * ldk + i, v[2]);
+                store_split(fmt, K4h, K4l, r * ldk + i, v[3]);
+            }
+        }
+        if constexpr (TRANS) {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ts[q][j][threadIdx.x] = v[q];
+        }
+    }
+    if constexpr (TRANS) {
+        __syncthreads();
+        void *hs[4] = {K1h, K2h, K3h, K4h}, *ls[4] = {K1l, K2l, K3l, K4l};
+        for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+            const int i = i0 + j;
+            const long long r = r0 + threadIdx.x;
+            if (i >= N || r >= rows) continue;
+            const long long g = r / (2LL * NR);
+            const long long rem = r - g * 2LL * NR;
+            const long long comp = rem / NR, jj = rem - comp * NR;
+            if (comp == 1 && cls_real[g]) continue;   // stays zero
+            const long long col = g * 2LL * NRp + comp * NRp + jj;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) store_split(fmt, hs[q], ls[q], (long long)i * ldk + col, ts[q][threadIdx.x][j]);
+        }
+    }
+}
+
+template <typename T>
+__global__ void vjp_recon_pairs_kernel(int N, long long P, int Kq, const T *__restrict__ VbarQ, const int *__restrict__ col0,
+                                       const int *__restrict__ col1, const double *__restrict__ pc0, const double *__restrict__ pc1,
+                                       const double *__restrict__ pre, T *__restrict__ Vbar, long long ldv) {
+    for (long long i = blockIdx.y; i < N; i += gridDim.y) {
+        const T *q = VbarQ + i * Kq;
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
+            const int a = col0[p];
+            double v = pc0[p] * (double)q[a] / pre[a];
+            const double k1 = pc1[p];
+            if (k1 != 0.0) {
+                const int b = col1[p];
+                v += k1 * (double)q[b] / pre[b];
+            }
+            Vbar[i * ldv + p] = (T)v;
+        }
+    }
+}
+
+template <typename T>
+__global__ void vjp_recon_modes_kernel(int N, int n, int Kmq, const T *__restrict__ GQ, const T *__restrict__ YQ,
+                                       const int *__restrict__ mode_col, const double *__restrict__ sign,
+                                       const double *__restrict__ mre, T *__restrict__ gbar, T *__restrict__ ypart, long long ldg) {
+    const long long total = (long long)N * n;
+    for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total; idx += (long long)gridDim.x * blockDim.x) {
+        const long long i = idx / n;
+        const int m = (int)(idx - i * n);
+        const int c = mode_col[m];
+        double g = 0.0, y = 0.0;
+        if (c >= 0) {
+            const double f = sign[c] / mre[c];
+            g = f * (double)GQ[i * Kmq + c];
+            y = f * (double)YQ[i * Kmq + c];
+        }
+        gbar[i * ldg + m] = (T)g;
+        ypart[i * ldg + m] = (T)y;
+    }
+}
+
+}  // namespace
+
+int freq_build_mode_rows(const FreqTables &t, const double *A, const double *B, int n, long long Nc, Format fmt, void *hi,
+                         void *lo, cudaStream_t st) {
+    if (t.Kmq == 0) return 0;
+    build_XGq_kernel<<<grid1(2 * Nc * t.Kmq), 256, 0, st>>>(A, B, n, Nc, t.Kmq, t.mc_mode, t.mc_sign, fmt, hi, lo);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+int freq_transpose_left(Format fmt, const void *L, int NR, int NRp, long long cols, void *out, cudaStream_t st) {
+    if (!L || cols <= 0) return 0;
+    TD_CHECK(NRp % 32 == 0 && NR <= NRp && 2LL * NRp / 32 <= 65535 && ceil_div(cols, 32) <= 2147483647LL, TDSCHA_EINVAL,
+             "left-operand transpose of %d rows x %lld", NR, cols);
+    const dim3 grid((unsigned)ceil_div(cols, 32), (unsigned)(2 * NRp / 32)), block(32, 8);
+    if (fmt == FMT_BF16)
+        transpose_left_kernel<uint16_t><<<grid, block, 0, st>>>(static_cast<const uint16_t *>(L), NR, NRp, cols, static_cast<uint16_t *>(out));
+    else if (fmt == FMT_F64)
+        transpose_left_kernel<double><<<grid, block, 0, st>>>(static_cast<const double *>(L), NR, NRp, cols, static_cast<double *>(out));
+    else
+        transpose_left_kernel<float><<<grid, block, 0, st>>>(static_cast<const float *>(L), NR, NRp, cols, static_cast<float *>(out));
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename AccT>
+int freq_vjp_coef(const FreqTables &t, int sub, const AccT *H, const AccT *Ch, const AccT *HQ, const AccT *Cp, long long ld,
+                  int N, int NR, int NRp, int d4, bool trans, Format fmt, void *const *K_hi, void *const *K_lo, long long ldk,
+                  double *BR, cudaStream_t st) {
+    const long long rows = (long long)t.n_class * 2 * NR;
+    TD_CHECK(ceil_div(rows, 32) <= 65535, TDSCHA_EINVAL, "VJP coefficient grid: %lld rows", rows);
+    const dim3 grid((unsigned)ceil_div(N, 32), (unsigned)ceil_div(rows, 32)), block(32, 8);
+    const double inv_r = 1.0 / (double)sub, inv_c = 2.0 / (double)sub;
+    if (trans)
+        vjp_coef_class_kernel<AccT, true><<<grid, block, 0, st>>>(H, Ch, HQ, Cp, ld, N, rows, NR, NRp, t.d_cls_real, inv_r, inv_c, d4,
+                                                                  fmt, K_hi[0], K_lo[0], K_hi[1], K_lo[1], K_hi[2], K_lo[2], K_hi[3],
+                                                                  K_lo[3], ldk, BR);
+    else
+        vjp_coef_class_kernel<AccT, false><<<grid, block, 0, st>>>(H, Ch, HQ, Cp, ld, N, rows, NR, NRp, t.d_cls_real, inv_r, inv_c,
+                                                                   d4, fmt, K_hi[0], K_lo[0], K_hi[1], K_lo[1], K_hi[2], K_lo[2],
+                                                                   K_hi[3], K_lo[3], ldk, BR);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template <typename T>
+int freq_vjp_reconstruct(const FreqTables &t, int N, int n, long long P, const T *VbarQ, const T *GQ, const T *YQ, T *Vbar,
+                         long long ldv, T *gbar, T *ypart, long long ldg, cudaStream_t st) {
+    vjp_recon_pairs_kernel<T><<<grid_rows(P, N), 256, 0, st>>>(N, P, t.Kq, VbarQ, t.pp_col0, t.pp_col1, t.pp_c0, t.pp_c1, t.pc_re,
+                                                               Vbar, ldv);
+    vjp_recon_modes_kernel<T><<<grid1((long long)N * n), 256, 0, st>>>(N, n, t.Kmq, GQ, YQ, t.mode_col, t.mc_sign, t.mc_re, gbar,
+                                                                         ypart, ldg);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+template int freq_vjp_coef<float>(const FreqTables &, int, const float *, const float *, const float *, const float *, long long,
+                                  int, int, int, int, bool, Format, void *const *, void *const *, long long, double *,
+                                  cudaStream_t);
+template int freq_vjp_coef<double>(const FreqTables &, int, const double *, const double *, const double *, const double *,
+                                   long long, int, int, int, int, bool, Format, void *const *, void *const *, long long, double *,
+                                   cudaStream_t);
+template int freq_vjp_reconstruct<float>(const FreqTables &, int, int, long long, const float *, const float *, const float *,
+                                         float *, long long, float *, float *, long long, cudaStream_t);
+template int freq_vjp_reconstruct<double>(const FreqTables &, int, int, long long, const double *, const double *, const double *,
+                                          double *, long long, double *, double *, long long, cudaStream_t);
 
 }  // namespace tdscha

@@ -37,6 +37,7 @@ struct FreqLayout {
     std::vector<int> cls_real;                        // class is a real character
     std::vector<int> pcol_off, pcol_cnt;              // pair columns of each class (padded)
     std::vector<int> mcol_off, mcol_cnt;              // mode columns of each class (padded; 0 when none)
+    std::vector<int> mcol_used;                       // the class's mode columns before padding
     // per pair column: own value = c0 M[mu0, nu0] + c1 M[mu1, nu1] of a symmetric matrix M
     std::vector<int> pc_mu0, pc_nu0, pc_mu1, pc_nu1;
     std::vector<double> pc_c0, pc_c1;
@@ -60,7 +61,8 @@ int build_freq_layout(int n, const std::vector<int> &dim, const std::vector<int>
 // Device copy of the layout tables.
 struct FreqTables {
     int n_class = 0, Kq = 0, Kmq = 0;
-    std::vector<int> cls_real, pcol_off, pcol_cnt, mcol_off, mcol_cnt;
+    std::vector<int> cls_real, pcol_off, pcol_cnt, mcol_off, mcol_cnt, mcol_used;
+    int *d_mcol_off = nullptr, *d_mcol_used = nullptr;   // per class (device)
     int *pc_mu0 = nullptr, *pc_nu0 = nullptr, *pc_mu1 = nullptr, *pc_nu1 = nullptr, *pc_partner = nullptr;
     double *pc_c0 = nullptr, *pc_c1 = nullptr, *pc_re = nullptr, *pc_im = nullptr, *pc_zc = nullptr;
     int *pp_col0 = nullptr, *pp_col1 = nullptr;
@@ -87,9 +89,11 @@ struct FreqOps {
 };
 size_t freq_operand_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo);
 // Operands of configurations [c0, c0 + Nc) into caller-provided storage `buf` (freq_operand_bytes).
-// X, G, Y, Xt: (N x n) rotated-basis ensemble (row c0 first).
-int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt, int n,
-                        long long Nc, Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st);
+// X, G, Y, Xt: (N x n) rotated-basis ensemble (row c0 first); XGT: [X^T; G^T] (2n x ldT, column c0
+// first) or nullptr (the split formats build from it when given).
+int freq_build_operands(const FreqTables &t, const double *X, const double *G, const double *Y, const double *Xt,
+                        const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
+                        cudaStream_t st);
 
 // Left operands from the representatives' transforms (InT float or double):
 //   Lab (2 NR x Kq) from U (NR x ldu, packed pairs), Lcd (2 NR x Kmq) from r1p (NR x ldr).
@@ -104,6 +108,44 @@ int freq_left(const FreqTables &t, int NR, int n, const InT *U, long long ldu, c
 template <typename AccT>
 int freq_weights(const FreqTables &t, const AccT *H, const AccT *Ch, long long ld, const double *rho, long long Nc, int NR,
                  long long N2pc, int d4, Format fmt, void *Cw_hi, void *Cw_lo, void *AB_hi, void *AB_lo, cudaStream_t st);
+
+// ---- the averages' VJP in the character basis -------------------------------------------------
+// With the hatted class-basis quantities (H = [a|b], Ch = [c|d] from U / r1; HQ = [A'|B'], Cp =
+// [C'|D'] from the cotangent transforms Q / phi) the VJP's per-row coefficients are linear:
+//   K1 = d4 A'/8 - D'/3,  K2 = -c/3 + d4 a/8,  K3 = -A'/6,  K4 = -a/6,
+// and the transposed contractions over the rows give the components of the configuration-side
+// cotangents: xi(Vbar_i) = sum_p conj(K1) xi(U_p) + conj(K2) xi(Q_p), z(gbar_i) += sum_p conj(K3)
+// z(r1_p), z(ypart_i) = sum_p conj(K4) z(phi_p), real GEMMs whose right operands are the left
+// operands L (their columns scaled by s_K m, undone in freq_vjp_reconstruct).  The weights'
+// pairing sum over the symmetry rows (rho's cotangent) is a sum over rows of products / s_K.
+
+// Row-major mode components of two (Nc x n) arrays, [A ; B] (2Nc x Kmq): [X; G] or [Y; X~].
+int freq_build_mode_rows(const FreqTables &t, const double *A, const double *B, int n, long long Nc, Format fmt, void *hi,
+                         void *lo, cudaStream_t st);
+// out (cols x 2 NRp) = L^T with the rows comp * NR + j moved to comp * NRp + j (zeros elsewhere).
+int freq_transpose_left(Format fmt, const void *L, int NR, int NRp, long long cols, void *out, cudaStream_t st);
+// Coefficients of the VJP from H, Ch, HQ, Cp (rows g * 2NR + comp * NR + j, ld, columns i and N + i):
+//   trans: K1..K4 transposed (N x nC * 2NRp, row g * 2NRp + comp * NRp + j), split into fmt
+//          (zeroed first by the caller: padding and the imaginary rows of real classes stay zero);
+//   else:  K1..K4 row-major like H (rows x ldk, FP64).
+//   BR (rows x N, FP64): the rho-pairing terms of every row, 1 / s_K included (0 for unused rows).
+template <typename AccT>
+int freq_vjp_coef(const FreqTables &t, int sub, const AccT *H, const AccT *Ch, const AccT *HQ, const AccT *Cp, long long ld,
+                  int N, int NR, int NRp, int d4, bool trans, Format fmt, void *const *K_hi, void *const *K_lo, long long ldk,
+                  double *BR, cudaStream_t st);
+// Vbar (N x ldv, packed entries), gbar / ypart (N x ldg, mode entries; gbar accumulated) from the
+// component outputs VbarQ (N x Kq), GQ and YQ (N x Kmq).
+template <typename T>
+int freq_vjp_reconstruct(const FreqTables &t, int N, int n, long long P, const T *VbarQ, const T *GQ, const T *YQ, T *Vbar,
+                         long long ldv, T *gbar, T *ypart, long long ldg, cudaStream_t st);
+
+// The weights with the thin [c|d] contraction folded in (split formats): c and d of row r and
+// configuration i are the dot products of the row's left operand Lcd (2NR x Kmq, hi + lo) with the
+// configuration's mode components XGq (2Nc x Kmq, hi + lo) over the row's class columns, formed in
+// fp32 next to [a|b] (H) instead of being stored by a contraction and read back.
+int freq_weights_cd(const FreqTables &t, const float *H, long long ld, const void *Lcd_hi, const void *Lcd_lo, const void *XG_hi,
+                    const void *XG_lo, const double *rho, long long Nc, int NR, long long N2pc, int d4, Format fmt, void *Cw_hi,
+                    void *Cw_lo, void *AB_hi, void *AB_lo, cudaStream_t st);
 
 // Back from the character basis: Zs (NR x ldz, packed c_p N~) from O (2 NR x Kq), Fs (NR x ldf)
 // from OF (2 NR x Kmq).

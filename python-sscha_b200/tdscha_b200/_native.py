@@ -172,7 +172,7 @@ class DeviceEnsemble:
                                                ctypes.byref(off)))
         return dict(rotated=bool(r.value), n_cosets=nc.value, coset_size=cs.value, offpattern=off.value)
 
-    STAGES = ("transform", "gemm_ab", "gemm_cd", "weights", "gemm_z", "gemm_f", "fold", "other")
+    STAGES = ("transform", "gemm_ab", "gemm_cd", "weights", "gemm_z", "gemm_f", "fold", "other", "operands")
 
     def set_profiling(self, enable=True):
         check(self._lib.tdscha_set_profiling(self.handle, int(enable)))

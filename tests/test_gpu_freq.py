@@ -131,3 +131,55 @@ def test_batched_classes_equal_single_vectors(cuda):
             fk, dk = ens.perturb_average(R1[k], Y1[k], 1, prec)
             tol = 1e-13 if prec == "fp64" else 1e-6
             assert _rel(f[k].cpu().numpy(), fk) < tol and _rel(d[k].cpu().numpy(), dk) < tol
+
+
+@pytest.mark.parametrize("prec,tol", [("fp64", 1e-11), ("bf16x3", 1e-4), ("tf32x3", 2e-5)])
+def test_vjp_classes_equal_the_symmetry_rows(cuda, monkeypatch, prec, tol):
+    """The averages' VJP (d<fbar, f_av> + <Dbar, D_av> / d(Y, rho)) on the character classes against
+    the same VJP over every symmetry row in FP64 (TDSCHA_VJP_FREQ=0)."""
+    import torch
+    from tdscha_b200 import _native
+    ens = _native.DeviceEnsemble(*_system(3, 24, seed=6))
+    N, n = 24, ens.n
+    rng = np.random.default_rng(17)
+    dev = torch.device("cuda")
+    t = lambda a: torch.as_tensor(np.ascontiguousarray(a), device=dev)   # noqa: E731
+    R1, Y1 = rng.standard_normal((3, n)), rng.standard_normal((3, n, n))
+    Ys = t(Y1 + Y1.transpose(0, 2, 1))
+    fb, Db = rng.standard_normal((3, n)), rng.standard_normal((3, n, n))
+    Db = t(Db + Db.transpose(0, 2, 1))
+
+    def vjp(precision, rows):
+        if rows:
+            monkeypatch.setenv("TDSCHA_VJP_FREQ", "0")
+        else:
+            monkeypatch.delenv("TDSCHA_VJP_FREQ", raising=False)
+        Yb = torch.zeros((N, n), dtype=torch.float64, device=dev)
+        rb = torch.zeros(N, dtype=torch.float64, device=dev)
+        ens.perturb_average_vjp(t(R1), Ys, t(fb), Db, Yb, rb, precision=precision)
+        torch.cuda.synchronize()
+        monkeypatch.delenv("TDSCHA_VJP_FREQ", raising=False)
+        return Yb.cpu().numpy(), rb.cpu().numpy()
+
+    Y0, r0 = vjp("fp64", True)
+    Yc, rc = vjp(prec, False)
+    print(f"{prec}: Ybar {_rel(Yc, Y0):.2e}  rhobar {_rel(rc, r0):.2e}")
+    assert _rel(Yc, Y0) < tol and _rel(rc, r0) < tol
+
+
+@pytest.mark.parametrize("prec", ["bf16x3", "tf32x3"])
+def test_fused_cd_weights_equal_the_contraction(cuda, monkeypatch, prec):
+    """The thin [c|d] contraction formed inside the weights kernel (TDSCHA_FREQ_FUSED_CD=1) against
+    the grouped contraction plus the separate weights kernel (the default), and both against FP64."""
+    from tdscha_b200 import _native
+    ens = _native.DeviceEnsemble(*_system(4, 4, seed=12))
+    n = ens.n
+    for R1, Y1, d4 in _perturbations(n, 2, 31):
+        fr, dr = ens.perturb_average(R1, Y1, d4, "fp64")
+        monkeypatch.setenv("TDSCHA_FREQ_FUSED_CD", "1")
+        ff, df = ens.perturb_average(R1, Y1, d4, prec)
+        monkeypatch.delenv("TDSCHA_FREQ_FUSED_CD")
+        fs, ds = ens.perturb_average(R1, Y1, d4, prec)
+        e_f, e_s = max(_rel(ff, fr), _rel(df, dr)), max(_rel(fs, fr), _rel(ds, dr))
+        print(f"{prec} d4={d4}: fused {e_f:.2e}  separate {e_s:.2e}")
+        assert e_f < max(1.5 * e_s, 2e-6)
