@@ -401,7 +401,7 @@ __global__ void __launch_bounds__(256) build_Vq_tiles_kernel(const double *__res
 // same 256 configurations (x fastest), whose XGT block (2n x 256) stays in L2 while every column
 // tile is built from it.  VqT rows go out directly (512 B per warp), Vq rows through shared memory.
 template <typename T>
-__global__ void __launch_bounds__(256) build_Vq_cols_kernel(const double *__restrict__ XGT, long long ldT, int n, long long Nc,
+__global__ void __launch_bounds__(256, 2) build_Vq_cols_kernel(const double *__restrict__ XGT, long long ldT, int n, long long Nc,
                                                             long long N2pc, int Kq, const int *__restrict__ mu0,
                                                             const int *__restrict__ nu0, const int *__restrict__ mu1,
                                                             const int *__restrict__ nu1, const double *__restrict__ c0,
@@ -420,30 +420,57 @@ __global__ void __launch_bounds__(256) build_Vq_cols_kernel(const double *__rest
     const bool second = k >= Nc && k < 2 * Nc;
     const bool live = k < 2 * Nc;
     const long long i = second ? k - Nc : k;
-    for (int cc = 0; cc < COLS; ++cc) {
-        const int c = cb + cc;
-        double v = 0.0;
+    // four columns per pass: every load of the pass is issued before the first is used, so the
+    // XGT reads of the four columns overlap instead of waiting one after the other
+    constexpr int U = 4;
+    const double *Xr = XGT + i;                              // column i of every mode row
+    const double *Gr = XGT + (long long)n * ldT + i;
+    for (int cc0 = 0; cc0 < COLS; cc0 += U) {
+        double v[U];
         if (live) {
-            const int a0 = __ldg(mu0 + c), b0 = __ldg(nu0 + c), a1 = __ldg(mu1 + c), b1 = __ldg(nu1 + c);
-            const double f0 = __ldg(c0 + c), f1 = __ldg(c1 + c);
-            const double xa0 = XGT[(long long)a0 * ldT + i], xb0 = XGT[(long long)b0 * ldT + i];
-            const double xa1 = XGT[(long long)a1 * ldT + i], xb1 = XGT[(long long)b1 * ldT + i];
-            if (!second) {
-                v = f0 * xa0 * xb0 + f1 * xa1 * xb1;
-            } else {
-                const double *G = XGT + (long long)n * ldT;
-                v = 0.5 * (f0 * (xa0 * G[(long long)b0 * ldT + i] + xb0 * G[(long long)a0 * ldT + i]) +
-                           f1 * (xa1 * G[(long long)b1 * ldT + i] + xb1 * G[(long long)a1 * ldT + i]));
+            int a0[U], b0[U], a1[U], b1[U];
+            double f0[U], f1[U], xa0[U], xb0[U], xa1[U], xb1[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = cb + cc0 + u;
+                a0[u] = __ldg(mu0 + c); b0[u] = __ldg(nu0 + c); a1[u] = __ldg(mu1 + c); b1[u] = __ldg(nu1 + c);
+                f0[u] = __ldg(c0 + c); f1[u] = __ldg(c1 + c);
             }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                xa0[u] = Xr[(long long)a0[u] * ldT]; xb0[u] = Xr[(long long)b0[u] * ldT];
+                xa1[u] = Xr[(long long)a1[u] * ldT]; xb1[u] = Xr[(long long)b1[u] * ldT];
+            }
+            if (!second) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) v[u] = f0[u] * xa0[u] * xb0[u] + f1[u] * xa1[u] * xb1[u];
+            } else {
+                double ga0[U], gb0[U], ga1[U], gb1[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    ga0[u] = Gr[(long long)a0[u] * ldT]; gb0[u] = Gr[(long long)b0[u] * ldT];
+                    ga1[u] = Gr[(long long)a1[u] * ldT]; gb1[u] = Gr[(long long)b1[u] * ldT];
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+                    v[u] = 0.5 * (f0[u] * (xa0[u] * gb0[u] + xb0[u] * ga0[u]) + f1[u] * (xa1[u] * gb1[u] + xb1[u] * ga1[u]));
+            }
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) v[u] = 0.0;
         }
-        T h, l;
-        split_to<T>(fmt, v, h, l);
-        if (k < N2pc) {
-            VT_hi[(long long)c * N2pc + k] = h;
-            if (lo) VT_lo[(long long)c * N2pc + k] = l;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int cc = cc0 + u, c = cb + cc;
+            T h, l;
+            split_to<T>(fmt, v[u], h, l);
+            if (k < N2pc) {
+                VT_hi[(long long)c * N2pc + k] = h;
+                if (lo) VT_lo[(long long)c * N2pc + k] = l;
+            }
+            th[cc * LDS + t] = h;
+            tl[cc * LDS + t] = l;
         }
-        th[cc * LDS + t] = h;
-        tl[cc * LDS + t] = l;
     }
     __syncthreads();
     // Vq rows k < 2Nc: one warp per row and pass, COLS columns as 32-bit words
