@@ -203,6 +203,9 @@ int tdscha_ensemble_device_bytes(const tdscha_ensemble *e, long long *bytes) {
     TD_CHECK(e != nullptr && bytes != nullptr, TDSCHA_EINVAL, "NULL argument");
     size_t b = e->base_bytes + e->ws.bytes;
     for (const auto &o : e->ops) b += o.bytes;
+    for (const auto &o : e->fops) b += o.bytes;
+    for (const auto &o : e->fhalf) b += o.bytes;
+    b += e->chunk_ops.bytes;
     *bytes = (long long)b;
     return 0;
 }

@@ -542,6 +542,8 @@ int ensemble_destroy(tdscha_ensemble *e) {
     freq_tables_destroy(e->freq);
     for (auto &fo : e->fops)
         if (fo.V_hi) cudaFree(fo.V_hi);   // one allocation per format, V_hi first
+    for (auto &fo : e->fhalf)
+        if (fo.V_hi) cudaFree(fo.V_hi);   // one allocation per format, V_hi first
     for (int f = 0; f < 3; ++f) {
         if (e->fyx_hi[f]) cudaFree(e->fyx_hi[f]);
         if (e->fyx_lo[f]) cudaFree(e->fyx_lo[f]);
@@ -859,6 +861,7 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
     TD_CUDA(cudaStreamIsCapturing(st, &cap));
     long long Nc = e->N;
     int ncj = 0;
+    bool half = false;   // chunks over resident row-major class operands
     FreqOps co;
     if (cap != cudaStreamCaptureStatusNone) {
         const AvgPlan &pl = e->plan;
@@ -866,9 +869,12 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
                  "graph capture of the averages needs an earlier call with the same batch (%d) and precision", nb);
         Nc = pl.Nc;
         ncj = pl.Jc / sub;
-        if (Nc < e->N)
-            TD_CHECK(e->chunk_ops.bytes >= freq_operand_bytes(ft, Nc, fmt, lo), TDSCHA_EINVAL, "chunk buffer changed since the plan");
-        else {
+        half = pl.half;
+        if (Nc < e->N) {
+            const size_t need = half ? freq_chunk_cols_bytes(ft, Nc, fmt, lo) : freq_operand_bytes(ft, Nc, fmt, lo);
+            TD_CHECK(e->chunk_ops.bytes >= need, TDSCHA_EINVAL, "chunk buffer changed since the plan");
+            TD_CHECK(!half || (e->fhalf[fmt].built && (e->fhalf[fmt].has_lo || !lo)), TDSCHA_EINVAL, "resident rows released since the plan");
+        } else {
             TD_CHECK(e->fops[fmt].built && (e->fops[fmt].has_lo || !lo), TDSCHA_EINVAL, "operands released since the plan");
             co = e->fops[fmt];
         }
@@ -877,15 +883,36 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
         TD_CUDA(cudaMemGetInfo(&free_b, &tot_b));
         const size_t avail = free_b + e->ws.bytes + e->chunk_ops.bytes;
         const char *env_chunk = getenv("TDSCHA_CONFIG_CHUNK");
+        // Configuration chunks: all configurations when their operands fit in half of the memory this
+        // call may use; else every class operand is rebuilt per chunk, or, with
+        // TDSCHA_CHUNK_RESIDENT_ROWS=1 and a split format, the row-major class operands of all
+        // configurations stay resident (when they fit in 55 % of that memory) and only the transposed
+        // ones are formed per chunk.  Off by default: on the 5x5x5 system the per-chunk transposes
+        // took 263 ms per 16-vector step against 143 ms for the full rebuilds.
+        const char *env_rows = getenv("TDSCHA_CHUNK_RESIDENT_ROWS");
+        const bool may_half = fmt != FMT_F64 && env_rows && atoi(env_rows) == 1;
+        const size_t resident = freq_resident_rows_bytes(ft, e->N, fmt, lo);
+        const bool rows_fit = may_half && (e->fhalf[fmt].built || resident < (size_t)(avail * 0.55));
         if (env_chunk && atoll(env_chunk) > 0 && atoll(env_chunk) < e->N) {
             Nc = atoll(env_chunk);
+            half = rows_fit;
         } else if (!e->fops[fmt].built && freq_operand_bytes(ft, e->N, fmt, lo) > avail / 2) {
-            const long long per_conf = 4LL * (ft.Kq + ft.Kmq) * (long long)es * (lo ? 2 : 1);
-            const long long fit = (long long)(avail * 0.4) / per_conf;
+            half = rows_fit;
+            const long long per_conf = (half ? 2LL : 4LL) * (ft.Kq + ft.Kmq) * (long long)es * (lo ? 2 : 1);
+            const size_t room = half ? (e->fhalf[fmt].built ? avail : avail - resident) : avail;
+            const long long fit = (long long)(room * 0.4) / per_conf;
             Nc = std::min<long long>(e->N, std::max<long long>(32, fit / 32 * 32));
         }
         if (Nc < e->N) {
-            const size_t need = freq_operand_bytes(ft, Nc, fmt, lo);
+            if (half && !(e->fhalf[fmt].built && (e->fhalf[fmt].has_lo || !lo))) {
+                if (e->fhalf[fmt].V_hi) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->fhalf[fmt].V_hi); e->fhalf[fmt] = FreqOps(); }
+                void *buf = nullptr;
+                TD_CUDA(cudaMalloc(&buf, resident));
+                TD_TRY(ensure_XGT(e, st));
+                const int rc = freq_build_rows(ft, e->X, e->G, e->XGT, e->N, e->n, e->N, fmt, lo, buf, e->fhalf[fmt], st);
+                if (rc) { cudaFree(buf); e->fhalf[fmt] = FreqOps(); return rc; }
+            }
+            const size_t need = half ? freq_chunk_cols_bytes(ft, Nc, fmt, lo) : freq_operand_bytes(ft, Nc, fmt, lo);
             if (e->chunk_ops.bytes < need) {
                 if (e->chunk_ops.base) { TD_CUDA(cudaDeviceSynchronize()); cudaFree(e->chunk_ops.base); e->chunk_ops = Workspace(); }
                 TD_CUDA(cudaMalloc(&e->chunk_ops.base, need));
@@ -908,6 +935,7 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
         e->plan.lo = lo;
         e->plan.cosets = true;
         e->plan.freq = true;
+        e->plan.half = half;
         e->plan.Nc = Nc;
         e->plan.Jc = ncj * sub;
     }
@@ -959,22 +987,41 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
             const long long Ncur = std::min(Nc, e->N - c0);
             const long long N2c = 2 * Ncur, N2pc = round_up(N2c, 64);   // the last chunk may be shorter
             const bool acc = c0 > 0;
-            if (chunked) {
+            if (chunked && half) {
+                StageScope sc(e, ST_OPERANDS, st, lo ? 3 : 2);
+                TD_TRY(freq_build_chunk_cols(ft, e->fhalf[fmt], e->N, c0, Ncur, e->Y, e->Xt, e->n, fmt, lo, e->chunk_ops.base, co, st));
+            } else if (chunked) {
                 StageScope sc(e, ST_OPERANDS, st, 3);
                 const int n = e->n;
                 TD_TRY(ensure_XGT(e, st));
                 TD_TRY(freq_build_operands(ft, e->X + c0 * n, e->G + c0 * n, e->Y + c0 * n, e->Xt + c0 * n, e->XGT + c0, e->N, n,
                                            Ncur, fmt, lo, e->chunk_ops.base, co, st));
             }
+            // rows of the row-major operands: the chunk's own (2 Ncur rows), or the resident operands'
+            // two ranges [c0, c0 + Ncur) and [N + c0, N + c0 + Ncur)
+            const bool two = chunked && half;
+            const long long brows = two ? e->N2 : N2c;
             // per class: [a|b] and [c|d] in the character basis, (rows (comp, v, c), 2Nc columns)
             std::vector<tc::GemmGroup> gab, gcd, gz, gf;
             for (int g = 0; g < nC; ++g) {
                 const int Mg = ft.cls_real[g] ? NR : 2 * NR;
                 const long long hrow = (long long)g * 2 * NR;
-                gab.push_back({Mg, (int)N2c, ft.pcol_cnt[g], 0, ft.pcol_off[g], 0, ft.pcol_off[g], hrow * L.ld1});
+                if (two) {
+                    gab.push_back({Mg, (int)Ncur, ft.pcol_cnt[g], 0, ft.pcol_off[g], (int)c0, ft.pcol_off[g], hrow * L.ld1});
+                    gab.push_back({Mg, (int)Ncur, ft.pcol_cnt[g], 0, ft.pcol_off[g], (int)(e->N + c0), ft.pcol_off[g],
+                                   hrow * L.ld1 + Ncur});
+                } else {
+                    gab.push_back({Mg, (int)N2c, ft.pcol_cnt[g], 0, ft.pcol_off[g], 0, ft.pcol_off[g], hrow * L.ld1});
+                }
                 gz.push_back({Mg, ft.pcol_cnt[g], (int)N2pc, (int)hrow, 0, ft.pcol_off[g], 0, (long long)ft.pcol_off[g]});
                 if (ft.mcol_cnt[g] > 0) {
-                    gcd.push_back({Mg, (int)N2c, ft.mcol_cnt[g], 0, ft.mcol_off[g], 0, ft.mcol_off[g], hrow * L.ld1});
+                    if (two) {
+                        gcd.push_back({Mg, (int)Ncur, ft.mcol_cnt[g], 0, ft.mcol_off[g], (int)c0, ft.mcol_off[g], hrow * L.ld1});
+                        gcd.push_back({Mg, (int)Ncur, ft.mcol_cnt[g], 0, ft.mcol_off[g], (int)(e->N + c0), ft.mcol_off[g],
+                                       hrow * L.ld1 + Ncur});
+                    } else {
+                        gcd.push_back({Mg, (int)N2c, ft.mcol_cnt[g], 0, ft.mcol_off[g], 0, ft.mcol_off[g], hrow * L.ld1});
+                    }
                     gf.push_back({Mg, ft.mcol_cnt[g], (int)N2pc, (int)hrow, 0, ft.mcol_off[g], 0, (long long)ft.mcol_off[g]});
                 } else if (!fused_cd) {
                     TD_CUDA(cudaMemsetAsync(static_cast<uint8_t *>(Ch) + hrow * L.ld1 * as, 0, (size_t)2 * NR * L.ld1 * as, st));
@@ -982,7 +1029,7 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
             }
             {
                 StageScope sc(e, ST_GEMM_AB, st);
-                TD_TRY(gemm_groups(e, fmt, nprod, Lab_hi, Lab_lo, 2LL * NR, ft.Kq, co.V_hi, co.V_lo, N2c, ft.Kq, gab, H, L.ld1, false,
+                TD_TRY(gemm_groups(e, fmt, nprod, Lab_hi, Lab_lo, 2LL * NR, ft.Kq, co.V_hi, co.V_lo, brows, ft.Kq, gab, H, L.ld1, false,
                                    st, freq_ab_drain()));
             }
             if (fused_cd) {
@@ -993,7 +1040,7 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
             } else {
                 {
                     StageScope sc(e, ST_GEMM_CD, st);
-                    TD_TRY(gemm_groups(e, fmt, nprod, Lcd_hi, Lcd_lo, 2LL * NR, Kmq1, co.XG_hi, co.XG_lo, N2c, Kmq1, gcd, Ch, L.ld1,
+                    TD_TRY(gemm_groups(e, fmt, nprod, Lcd_hi, Lcd_lo, 2LL * NR, Kmq1, co.XG_hi, co.XG_lo, brows, Kmq1, gcd, Ch, L.ld1,
                                        false, st));
                 }
                 StageScope sc(e, ST_WEIGHTS, st);

@@ -54,6 +54,7 @@ struct AvgPlan {
     bool lo = false;
     bool cosets = false;
     bool freq = false;
+    bool half = false;   // configuration chunks over resident row-major class operands
     long long Nc = 0;
     int Jc = 0;
 };
@@ -116,6 +117,7 @@ struct tdscha_ensemble {
     tdscha::SymCosets *cosets = nullptr;           // factorised symmetry transform / fold (mixed formats)
     tdscha::FreqTables *freq = nullptr;            // character classes of the subgroup (freq.cuh)
     tdscha::FreqOps fops[3];                       // character-basis operands per storage format (resident)
+    tdscha::FreqOps fhalf[3];                      // resident row-major class operands of chunked ensembles
     void *fyx_hi[3] = {nullptr, nullptr, nullptr};  // [Y; X~] mode components (2N x Kmq) per format (class VJP)
     void *fyx_lo[3] = {nullptr, nullptr, nullptr};
     tdscha::Workspace rot_ws;                      // rotated inputs / outputs of the VJP

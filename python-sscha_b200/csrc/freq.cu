@@ -377,6 +377,7 @@ __global__ void __launch_bounds__(256) build_Vq_tiles_kernel(const double *__res
         }
     }
     // transposed: rows c (64), columns k0 .. k0 + 63 (< N2pc)
+    if (VT_hi == nullptr) return;
     for (int w = tid; w < 64 * WPR; w += 256) {
         const int cr = w / WPR, j = (w % WPR) * EPW;
         const int c = cb + cr;
@@ -464,7 +465,7 @@ __global__ void __launch_bounds__(256, 2) build_Vq_cols_kernel(const double *__r
             const int cc = cc0 + u, c = cb + cc;
             T h, l;
             split_to<T>(fmt, v[u], h, l);
-            if (k < N2pc) {
+            if (VT_hi && k < N2pc) {
                 VT_hi[(long long)c * N2pc + k] = h;
                 if (lo) VT_lo[(long long)c * N2pc + k] = l;
             }
@@ -1167,5 +1168,116 @@ template int freq_vjp_reconstruct<float>(const FreqTables &, int, int, long long
                                          float *, long long, float *, float *, long long, cudaStream_t);
 template int freq_vjp_reconstruct<double>(const FreqTables &, int, int, long long, const double *, const double *, const double *,
                                           double *, long long, double *, double *, long long, cudaStream_t);
+
+}  // namespace tdscha
+
+// ================================================================================================
+// Configuration chunks over a resident row-major class operand
+// ================================================================================================
+namespace tdscha {
+namespace {
+
+// out (cols x ldo) column q = in row (q < Nc ? ra + q : rb + q - Nc) for q < 2Nc, zero after; 32 x 32
+// tiles through shared memory
+template <typename T>
+__global__ void transpose_two_ranges_kernel(const T *__restrict__ in, long long cols, long long ra, long long rb, long long Nc,
+                                            T *__restrict__ out, long long ldo) {
+    __shared__ T tile[32][33];
+    const long long c0 = (long long)blockIdx.x * 32, q0 = (long long)blockIdx.y * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long q = q0 + j, c = c0 + threadIdx.x;
+        T v = T(0);
+        if (q < 2 * Nc && c < cols) v = in[(q < Nc ? ra + q : rb + q - Nc) * cols + c];
+        tile[j][threadIdx.x] = v;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const long long c = c0 + j, q = q0 + threadIdx.x;
+        if (c < cols && q < ldo) out[c * ldo + q] = tile[threadIdx.x][j];
+    }
+}
+
+template <typename T>
+int transpose_two_ranges(const void *in, long long cols, long long ra, long long rb, long long Nc, void *out, long long ldo,
+                         cudaStream_t st) {
+    TD_CHECK(ldo % 32 == 0 && ldo / 32 <= 65535, TDSCHA_EINVAL, "chunk transpose: %lld columns", ldo);
+    const dim3 grid((unsigned)ceil_div(cols, 32), (unsigned)(ldo / 32)), block(32, 8);
+    transpose_two_ranges_kernel<T><<<grid, block, 0, st>>>(static_cast<const T *>(in), cols, ra, rb, Nc, static_cast<T *>(out), ldo);
+    TD_CUDA(cudaGetLastError());
+    return 0;
+}
+
+}  // namespace
+
+size_t freq_resident_rows_bytes(const FreqTables &t, long long N, Format fmt, bool lo) {
+    return (size_t)2 * N * (t.Kq + t.Kmq) * format_bytes(fmt) * (lo ? 2 : 1) + 8 * 256;
+}
+
+size_t freq_chunk_cols_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo) {
+    const long long N2pc = round_up(2 * Nc, 64);
+    return (size_t)N2pc * (t.Kq + t.Kmq) * format_bytes(fmt) * (lo ? 2 : 1) + 8 * 256;
+}
+
+int freq_build_rows(const FreqTables &t, const double *X, const double *G, const double *XGT, long long ldT, int n, long long N,
+                    Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st) {
+    TD_CHECK(fmt == FMT_BF16 || fmt == FMT_TF32, TDSCHA_EINVAL, "resident class rows need a split format");
+    const size_t es = format_bytes(fmt);
+    const long long N2p = round_up(2 * N, 64);
+    uint8_t *b = static_cast<uint8_t *>(buf);
+    size_t off = 0;
+    auto take = [&](long long count) { void *p = b + off; off += ((size_t)count * es + 255) / 256 * 256; return p; };
+    o = FreqOps();
+    o.V_hi = take(2 * N * t.Kq);
+    o.XG_hi = take(2 * N * t.Kmq);
+    if (lo) {
+        o.V_lo = take(2 * N * t.Kq);
+        o.XG_lo = take(2 * N * t.Kmq);
+    }
+    if (fmt == FMT_BF16)
+        TD_TRY(build_Vq_cols<uint16_t>(t, XGT, ldT, n, N, N2p, fmt, o.V_hi, o.V_lo, nullptr, nullptr, st));
+    else
+        TD_TRY(build_Vq_cols<float>(t, XGT, ldT, n, N, N2p, fmt, o.V_hi, o.V_lo, nullptr, nullptr, st));
+    if (t.Kmq > 0)
+        build_XGq_kernel<<<grid1(2 * N * t.Kmq), 256, 0, st>>>(X, G, n, N, t.Kmq, t.mc_mode, t.mc_sign, fmt, o.XG_hi, o.XG_lo);
+    TD_CUDA(cudaGetLastError());
+    o.built = true;
+    o.has_lo = lo;
+    o.bytes = off;
+    return 0;
+}
+
+int freq_build_chunk_cols(const FreqTables &t, const FreqOps &rows, long long N, long long c0, long long Nc, const double *Y,
+                          const double *Xt, int n, Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st) {
+    const size_t es = format_bytes(fmt);
+    const long long N2pc = round_up(2 * Nc, 64);
+    uint8_t *b = static_cast<uint8_t *>(buf);
+    size_t off = 0;
+    auto take = [&](long long count) { void *p = b + off; off += ((size_t)count * es + 255) / 256 * 256; return p; };
+    o = FreqOps();
+    o.V_hi = rows.V_hi;
+    o.V_lo = rows.V_lo;
+    o.XG_hi = rows.XG_hi;
+    o.XG_lo = rows.XG_lo;
+    o.VT_hi = take((long long)t.Kq * N2pc);
+    o.YX_hi = take((long long)t.Kmq * N2pc);
+    if (lo) {
+        o.VT_lo = take((long long)t.Kq * N2pc);
+        o.YX_lo = take((long long)t.Kmq * N2pc);
+    }
+    for (int part = 0; part < (lo ? 2 : 1); ++part) {
+        const void *src = part ? rows.V_lo : rows.V_hi;
+        void *dst = part ? o.VT_lo : o.VT_hi;
+        if (fmt == FMT_BF16) TD_TRY(transpose_two_ranges<uint16_t>(src, t.Kq, c0, N + c0, Nc, dst, N2pc, st));
+        else TD_TRY(transpose_two_ranges<float>(src, t.Kq, c0, N + c0, Nc, dst, N2pc, st));
+    }
+    if (t.Kmq > 0)
+        build_YXq_kernel<<<grid1((long long)t.Kmq * N2pc), 256, 0, st>>>(Y + c0 * n, Xt + c0 * n, n, Nc, N2pc, t.Kmq, t.mc_mode,
+                                                                           t.mc_sign, fmt, o.YX_hi, o.YX_lo);
+    TD_CUDA(cudaGetLastError());
+    o.built = true;
+    o.has_lo = lo;
+    o.bytes = off;
+    return 0;
+}
 
 }  // namespace tdscha

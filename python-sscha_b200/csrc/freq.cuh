@@ -95,6 +95,19 @@ int freq_build_operands(const FreqTables &t, const double *X, const double *G, c
                         const double *XGT, long long ldT, int n, long long Nc, Format fmt, bool lo, void *buf, FreqOps &o,
                         cudaStream_t st);
 
+// Configuration chunks over a resident row-major operand (split formats): Vq and XGq of all N
+// configurations stay resident (freq_build_rows, freq_resident_rows_bytes), and per chunk only the
+// transposed operands are formed: VqT by a tiled transpose of the chunk's two row ranges of Vq
+// (rows c0.. and N + c0..), YXq from Y, X~ (freq_build_chunk_cols, freq_chunk_cols_bytes).  The
+// chunk's FreqOps then points at the resident Vq / XGq, whose chunk rows the [a|b] and [c|d]
+// contractions address as two row ranges.
+size_t freq_resident_rows_bytes(const FreqTables &t, long long N, Format fmt, bool lo);
+size_t freq_chunk_cols_bytes(const FreqTables &t, long long Nc, Format fmt, bool lo);
+int freq_build_rows(const FreqTables &t, const double *X, const double *G, const double *XGT, long long ldT, int n, long long N,
+                    Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st);
+int freq_build_chunk_cols(const FreqTables &t, const FreqOps &rows, long long N, long long c0, long long Nc, const double *Y,
+                          const double *Xt, int n, Format fmt, bool lo, void *buf, FreqOps &o, cudaStream_t st);
+
 // Left operands from the representatives' transforms (InT float or double):
 //   Lab (2 NR x Kq) from U (NR x ldu, packed pairs), Lcd (2 NR x Kmq) from r1p (NR x ldr).
 template <typename InT>

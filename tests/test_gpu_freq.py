@@ -96,8 +96,12 @@ def test_classes_against_the_reference_fixture(cuda, c1):
         assert _rel(f, fr) < 1e-12 and _rel(d, dr) < 1e-12
 
 
-@pytest.mark.parametrize("prec", ["fp64", "bf16x3"])
-def test_classes_in_configuration_and_coset_chunks(cuda, monkeypatch, prec):
+@pytest.mark.parametrize("prec,resident_rows", [("fp64", "0"), ("bf16x3", "0"), ("bf16x3", "1"), ("tf32x3", "1")])
+def test_classes_in_configuration_and_coset_chunks(cuda, monkeypatch, prec, resident_rows):
+    """Configuration chunks (32 + 18) and coset chunks (5) against the resident single pass: every
+    class operand rebuilt per chunk (the default), or, with TDSCHA_CHUNK_RESIDENT_ROWS=1 and a split
+    format, the row-major class operands of all configurations resident and the transposed ones
+    formed per chunk."""
     from tdscha_b200 import _native
     ens = _native.DeviceEnsemble(*_system(3, 50, seed=2))
     n = ens.n
@@ -105,9 +109,11 @@ def test_classes_in_configuration_and_coset_chunks(cuda, monkeypatch, prec):
     f1, d1 = ens.perturb_average(R1, Y1, 1, prec)
     monkeypatch.setenv("TDSCHA_CONFIG_CHUNK", "32")    # chunks of 32 + 18 configurations
     monkeypatch.setenv("TDSCHA_SYM_CHUNK", "270")      # 10 cosets of 27 per chunk (5 chunks)
+    monkeypatch.setenv("TDSCHA_CHUNK_RESIDENT_ROWS", resident_rows)
     f2, d2 = ens.perturb_average(R1, Y1, 1, prec)
     monkeypatch.delenv("TDSCHA_CONFIG_CHUNK")
     monkeypatch.delenv("TDSCHA_SYM_CHUNK")
+    monkeypatch.delenv("TDSCHA_CHUNK_RESIDENT_ROWS")
     tol = 1e-12 if prec == "fp64" else 1e-6
     assert _rel(f2, f1) < tol and _rel(d2, d1) < tol
 
