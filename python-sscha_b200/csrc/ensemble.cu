@@ -854,7 +854,9 @@ static int perturb_average_freq(tdscha_ensemble *e, int nb, const double *R1, co
     const FreqTables &ft = *e->freq;
     const SymCosets *cs = e->cosets;
     const int n_cos = cs->n_cos, sub = cs->sub, nC = ft.n_class;
-    const int Jf = ceil_div(n_cos, 64);
+    // fold partials: Jf representatives per fold CTA (eight partials of 6 at 48 representatives), so
+    // that each CTA reuses its W block over several representatives
+    const int Jf = std::max(1, ceil_div(n_cos, 8));
     const int nf_total = ceil_div(n_cos, Jf);
     const size_t es = format_bytes(fmt);
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
