@@ -296,6 +296,13 @@ __device__ __forceinline__ long long packed_of(int a, int b, int n) {
 
 unsigned grid1(long long work) { return (unsigned)std::max<long long>(1, std::min<long long>((work + 255) / 256, 148LL * 32)); }
 
+// columns one per thread, rows in groups of rb (grid.y capped; the kernels stride over row groups)
+dim3 grid_cols_rows(long long cols, long long rows, int rb) {
+    const long long gx = std::max<long long>(1, ceil_div(cols, 256));
+    const long long gy = std::max<long long>(1, std::min<long long>(ceil_div(rows, rb), 65535));
+    return dim3((unsigned)gx, (unsigned)gy);
+}
+
 dim3 grid_rows(long long cols, long long rows) {
     const long long gx = std::max<long long>(1, std::min<long long>(ceil_div(cols, 256), 64));
     const long long gy = std::max<long long>(1, std::min<long long>(rows, 65535));
@@ -550,22 +557,42 @@ __global__ void build_YXq_kernel(const double *__restrict__ Y, const double *__r
     }
 }
 
-// Lab rows r (real parts) and NR + r (imaginary parts) from the representatives' U rows
+// Lab rows r (real parts) and NR + r (imaginary parts) from the representatives' U rows.  One thread
+// per component column c and LEFT_RB consecutive rows: the column's tables (packed indices, weights,
+// partner) are read once and its LEFT_RB rows' gathers are independent, in flight together.
+constexpr int LEFT_RB = 8;
+
 template <typename InT>
-__global__ void left_ab_kernel(int NR, int n, int Kq, const InT *__restrict__ U, long long ldu, const int *__restrict__ mu0,
-                               const int *__restrict__ nu0, const int *__restrict__ mu1, const int *__restrict__ nu1,
-                               const double *__restrict__ c0, const double *__restrict__ c1, const int *__restrict__ partner,
-                               const double *__restrict__ re, const double *__restrict__ im, Format fmt, void *hi, void *lo) {
-    for (long long r = blockIdx.y; r < NR; r += gridDim.y) {
-        const InT *u = U + r * ldu;
-        for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < Kq; c += gridDim.x * blockDim.x) {
-            const double own = c0[c] * (double)u[packed_of(mu0[c], nu0[c], n)] + c1[c] * (double)u[packed_of(mu1[c], nu1[c], n)];
-            const int pc = partner[c];
-            double oth = 0.0;
-            if (pc >= 0 && im[c] != 0.0)
-                oth = c0[pc] * (double)u[packed_of(mu0[pc], nu0[pc], n)] + c1[pc] * (double)u[packed_of(mu1[pc], nu1[pc], n)];
-            store_split(fmt, hi, lo, r * Kq + c, re[c] * own);
-            store_split(fmt, hi, lo, (NR + r) * Kq + c, im[c] * oth);
+__global__ void __launch_bounds__(256) left_ab_kernel(int NR, int n, int Kq, const InT *__restrict__ U, long long ldu,
+                                                      const int *__restrict__ mu0, const int *__restrict__ nu0,
+                                                      const int *__restrict__ mu1, const int *__restrict__ nu1,
+                                                      const double *__restrict__ c0, const double *__restrict__ c1,
+                                                      const int *__restrict__ partner, const double *__restrict__ re,
+                                                      const double *__restrict__ im, Format fmt, void *hi, void *lo) {
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= Kq) return;
+    const long long p0 = packed_of(mu0[c], nu0[c], n), p1 = packed_of(mu1[c], nu1[c], n);
+    const double a0 = c0[c], a1 = c1[c], rc = re[c], ic = im[c];
+    const int pc = partner[c];
+    const bool has = pc >= 0 && ic != 0.0;
+    long long q0 = 0, q1 = 0;
+    double b0 = 0.0, b1 = 0.0;
+    if (has) {
+        q0 = packed_of(mu0[pc], nu0[pc], n);
+        q1 = packed_of(mu1[pc], nu1[pc], n);
+        b0 = c0[pc];
+        b1 = c1[pc];
+    }
+    for (long long r0 = (long long)blockIdx.y * LEFT_RB; r0 < NR; r0 += (long long)gridDim.y * LEFT_RB) {
+#pragma unroll
+        for (int i = 0; i < LEFT_RB; ++i) {
+            const long long r = r0 + i;
+            if (r >= NR) break;
+            const InT *u = U + r * ldu;
+            const double own = a0 * (double)u[p0] + a1 * (double)u[p1];
+            const double oth = has ? b0 * (double)u[q0] + b1 * (double)u[q1] : 0.0;
+            store_split(fmt, hi, lo, r * Kq + c, rc * own);
+            store_split(fmt, hi, lo, (NR + r) * Kq + c, ic * oth);
         }
     }
 }
@@ -595,18 +622,36 @@ __device__ __forceinline__ double own_out(const AccT *o1, const AccT *o2, int c,
     return v;
 }
 
+// Zs rows from the class outputs: one thread per pair p and LEFT_RB consecutive rows, the pair's
+// tables (columns, weights, partners) read once
 template <typename AccT>
-__global__ void recon_z_kernel(int NR, long long P, int Kq, const AccT *__restrict__ O, const int *__restrict__ pmu,
-                               const int *__restrict__ pnu, const int *__restrict__ col0, const int *__restrict__ col1,
-                               const double *__restrict__ pc0, const double *__restrict__ pc1, const int *__restrict__ partner,
-                               const double *__restrict__ zc, AccT *__restrict__ Zs, long long ldz) {
-    for (long long r = blockIdx.y; r < NR; r += gridDim.y) {
-        const AccT *o1 = O + r * Kq, *o2 = O + (NR + r) * Kq;
-        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x) {
-            double v = pc0[p] * own_out(o1, o2, col0[p], partner, zc);
-            const double k1 = pc1[p];
-            if (k1 != 0.0) v += k1 * own_out(o1, o2, col1[p], partner, zc);
-            Zs[r * ldz + p] = (AccT)((pmu[p] == pnu[p] ? 1.0 : 2.0) * v);
+__global__ void __launch_bounds__(256) recon_z_kernel(int NR, long long P, int Kq, const AccT *__restrict__ O,
+                                                      const int *__restrict__ pmu, const int *__restrict__ pnu,
+                                                      const int *__restrict__ col0, const int *__restrict__ col1,
+                                                      const double *__restrict__ pc0, const double *__restrict__ pc1,
+                                                      const int *__restrict__ partner, const double *__restrict__ zc,
+                                                      AccT *__restrict__ Zs, long long ldz) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= P) return;
+    const int ca = col0[p], cb = col1[p];
+    const double k0 = pc0[p], k1 = pc1[p], fac = pmu[p] == pnu[p] ? 1.0 : 2.0;
+    const double za = zc[ca], zb = k1 != 0.0 ? zc[cb] : 0.0;
+    const int qa = za != 0.0 ? partner[ca] : 0, qb = zb != 0.0 ? partner[cb] : 0;
+    for (long long r0 = (long long)blockIdx.y * LEFT_RB; r0 < NR; r0 += (long long)gridDim.y * LEFT_RB) {
+#pragma unroll
+        for (int i = 0; i < LEFT_RB; ++i) {
+            const long long r = r0 + i;
+            if (r >= NR) break;
+            const AccT *o1 = O + r * Kq, *o2 = O + (NR + r) * Kq;
+            double va = (double)o1[ca];
+            if (za != 0.0) va += za * (double)o2[qa];
+            double v = k0 * va;
+            if (k1 != 0.0) {
+                double vb = (double)o1[cb];
+                if (zb != 0.0) vb += zb * (double)o2[qb];
+                v += k1 * vb;
+            }
+            Zs[r * ldz + p] = (AccT)(fac * v);
         }
     }
 }
@@ -939,7 +984,7 @@ int freq_build_operands(const FreqTables &t, const double *X, const double *G, c
 template <typename InT>
 int freq_left(const FreqTables &t, int NR, int n, const InT *U, long long ldu, const InT *r1p, long long ldr, Format fmt,
               void *Lab_hi, void *Lab_lo, void *Lcd_hi, void *Lcd_lo, cudaStream_t st) {
-    left_ab_kernel<InT><<<grid_rows(t.Kq, NR), 256, 0, st>>>(NR, n, t.Kq, U, ldu, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0,
+    left_ab_kernel<InT><<<grid_cols_rows(t.Kq, NR, LEFT_RB), 256, 0, st>>>(NR, n, t.Kq, U, ldu, t.pc_mu0, t.pc_nu0, t.pc_mu1, t.pc_nu1, t.pc_c0,
                                                              t.pc_c1, t.pc_partner, t.pc_re, t.pc_im, fmt, Lab_hi, Lab_lo);
     if (t.Kmq > 0)
         left_cd_kernel<InT><<<grid1((long long)NR * t.Kmq), 256, 0, st>>>(NR, t.Kmq, r1p, ldr, t.mc_mode, t.mc_sign, t.mc_partner,
@@ -951,7 +996,7 @@ int freq_left(const FreqTables &t, int NR, int n, const InT *U, long long ldu, c
 template <typename AccT>
 int freq_reconstruct(const FreqTables &t, int NR, int n, long long P, const int *pmu, const int *pnu, const AccT *O,
                      const AccT *OF, AccT *Zs, long long ldz, AccT *Fs, long long ldf, cudaStream_t st) {
-    recon_z_kernel<AccT><<<grid_rows(P, NR), 256, 0, st>>>(NR, P, t.Kq, O, pmu, pnu, t.pp_col0, t.pp_col1, t.pp_c0, t.pp_c1,
+    recon_z_kernel<AccT><<<grid_cols_rows(P, NR, LEFT_RB), 256, 0, st>>>(NR, P, t.Kq, O, pmu, pnu, t.pp_col0, t.pp_col1, t.pp_c0, t.pp_c1,
                                                            t.pc_partner, t.pc_zc, Zs, ldz);
     recon_f_kernel<AccT><<<grid1((long long)NR * n), 256, 0, st>>>(NR, n, t.Kmq, OF, t.mode_col, t.mc_sign, t.mc_partner,
                                                                     t.mc_zc, Fs, ldf);
