@@ -207,10 +207,13 @@ struct Cfg {
     static constexpr int STAGE_BYTES = NOPS * (A_BYTES + B_BYTES);
     static constexpr int K_ELEMS = TF32 ? 32 : 64;            // K per stage (128 B of K)
     static constexpr int UMMA_K = TF32 ? 8 : 16;              // K per instruction (32 B)
-    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
     static constexpr uint32_t TMEM_COLS = 2 * BN;             // two accumulator buffers
     static constexpr int EPI_WARPS = 8;                       // 2 warps per TMEM lane quadrant
     static constexpr int EPI_COLS = BN / 2;                   // columns owned by one epilogue thread
+    static constexpr int EPI_BUF_FLOATS = 32 * 32;            // one epilogue warp's 32 x 32 staging block
+    static constexpr int SMEM_BYTES = STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/ +
+                                      EPI_WARPS * EPI_BUF_FLOATS * 4 /*epilogue staging*/;
+    static_assert(SMEM_BYTES <= 227 * 1024, "shared memory of the contraction kernel");
 };
 
 // Persistent: CTA c processes tiles c, c + gridDim.x, ... (m fastest).  Each tile's K loop is split
@@ -233,6 +236,7 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
     volatile int *abort_flag = reinterpret_cast<volatile int *>(bars + 2 * STAGES + 4);
     uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(bars + 2 * STAGES + 5);
     uint64_t *done_bar = bars + 2 * STAGES + 6;   // abort path: completion of every MMA issued
+    float *epi_buf = reinterpret_cast<float *>(smem + STAGES * C::STAGE_BYTES + 256);   // epilogue staging blocks
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
@@ -340,7 +344,6 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
         const int ew = warp - 2;
         const int q = warp & 3;              // TMEM lane quadrant this warp may access
         const int half = ew >> 2;            // which half of the BN columns this warp owns
-        const int row = q * 32 + lane;
         long long ch = 0;
         bool ok = true;
         for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
@@ -371,26 +374,45 @@ tc_gemm_kernel(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant
                 if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[X])) : "memory");
             }
             if (!ok) break;
-            const long long grow = (long long)m0 + row;
-            if (grow < M) {
-                float *drow = D + G.d_off + grow * ldd;
-                const int cb0 = n0 + half * C::EPI_COLS;
+            // Store through this warp's 32 x 32 staging block: each lane writes its row's 32 columns, then
+            // lanes 8i..8i+7 store 128 contiguous bytes of one row each, so one store instruction covers
+            // four full 128-byte lines instead of 16 bytes of 32 rows.  16-byte chunks are XOR-swizzled by
+            // row (chunk j of row r at j ^ (r & 7)), which keeps both phases free of bank conflicts.
+            float *wbuf = epi_buf + ew * C::EPI_BUF_FLOATS;
+            const int cb0 = n0 + half * C::EPI_COLS;
+            const bool vec = ((ldd & 3) == 0) && ((G.d_off & 3) == 0);
+            const int rsub = lane >> 3, chk = lane & 7;
 #pragma unroll
-                for (int v = 0; v < C::EPI_COLS / 4; ++v) {
-                    const int cb = cb0 + 4 * v;
-                    if (cb + 4 <= N && ((ldd & 3) == 0) && ((G.d_off & 3) == 0)) {
-                        float4 o = make_float4(acc[4 * v], acc[4 * v + 1], acc[4 * v + 2], acc[4 * v + 3]);
+            for (int sub = 0; sub < C::EPI_COLS / 32; ++sub) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    *reinterpret_cast<float4 *>(wbuf + lane * 32 + 4 * (j ^ (lane & 7))) =
+                        make_float4(acc[sub * 32 + 4 * j], acc[sub * 32 + 4 * j + 1], acc[sub * 32 + 4 * j + 2],
+                                    acc[sub * 32 + 4 * j + 3]);
+                __syncwarp();
+                const int cb = cb0 + sub * 32 + 4 * chk;
+#pragma unroll 1
+                for (int i0 = 0; i0 < 32; i0 += 4) {
+                    const int i = i0 + rsub;
+                    const float4 v = *reinterpret_cast<const float4 *>(wbuf + i * 32 + 4 * (chk ^ (i & 7)));
+                    const long long grow = (long long)m0 + q * 32 + i;
+                    if (grow >= M) continue;
+                    float *drow = D + G.d_off + grow * ldd;
+                    if (vec && cb + 4 <= N) {
+                        float4 o = v;
                         if (accumulate) {
                             const float4 old = *reinterpret_cast<const float4 *>(drow + cb);
                             o.x += old.x; o.y += old.y; o.z += old.z; o.w += old.w;
                         }
                         *reinterpret_cast<float4 *>(drow + cb) = o;
                     } else {
+                        const float vv[4] = {v.x, v.y, v.z, v.w};
 #pragma unroll
                         for (int e = 0; e < 4; ++e)
-                            if (cb + e < N) drow[cb + e] = accumulate ? drow[cb + e] + acc[4 * v + e] : acc[4 * v + e];
+                            if (cb + e < N) drow[cb + e] = accumulate ? drow[cb + e] + vv[e] : vv[e];
                     }
                 }
+                __syncwarp();   // the block is rewritten by the next 32 columns
             }
         }
         if (!ok) *abort_flag = 1;
