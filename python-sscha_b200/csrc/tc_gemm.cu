@@ -688,7 +688,7 @@ static int choose(int tf32, int nprod, int M, int N, int K, unsigned long long s
 
 template <bool TF32, int NPROD>
 static int launch_tuned(const GemmOperands &op, const Problem &pb, float *D, long long ldd, cudaStream_t st, unsigned *err) {
-    constexpr int S_WIDE = NPROD == 3 ? 2 : 4, S_NARROW = NPROD == 3 ? 3 : 6;
+    constexpr int S_WIDE = NPROD == 3 ? 2 : 4, S_NARROW = NPROD == 3 ? 3 : 6, S_THIN = NPROD == 3 ? 4 : 8;
     int dev = 0;
     TD_CUDA(cudaGetDevice(&dev));
     cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -699,9 +699,16 @@ static int launch_tuned(const GemmOperands &op, const Problem &pb, float *D, lon
     const int stall = g_stall_next.exchange(0);
     for (size_t g0 = 0; g0 < pb.groups.size(); g0 += MAX_GROUPS) {
         const size_t g1 = std::min(pb.groups.size(), g0 + MAX_GROUPS);
-        Prepared cfgs[2];
+        Prepared cfgs[3];
         TD_TRY((prepare_cfg<256, S_WIDE, TF32, NPROD>(op, pb, g0, g1, D, ldd, st, err, counter, stall, &cfgs[0])));
         TD_TRY((prepare_cfg<128, S_NARROW, TF32, NPROD>(op, pb, g0, g1, D, ldd, st, err, counter, stall, &cfgs[1])));
+        // outputs at most 64 columns wide in every group (the per-class mode-column contractions): the
+        // 128 x 64 tile, whose shorter B rows leave room for a deeper A stream, and no wasted MMA columns
+        bool thin = true;
+        for (size_t i = g0; i < g1; ++i) thin = thin && pb.groups[i].N <= 64;
+        const char *env_tn = getenv("TDSCHA_TILE_N");
+        if (env_tn) thin = thin && atoi(env_tn) == 64;
+        if (thin) TD_TRY((prepare_cfg<64, S_THIN, TF32, NPROD>(op, pb, g0, g1, D, ldd, st, err, counter, stall, &cfgs[2])));
         // tuning key: the one problem's shape, or the groups' shapes hashed (FNV-1a)
         int kM = pb.groups[g0].M, kN = pb.groups[g0].N, kK = pb.groups[g0].K;
         unsigned long long shape = 0;
@@ -715,7 +722,10 @@ static int launch_tuned(const GemmOperands &op, const Problem &pb, float *D, lon
             kM = (int)(g1 - g0);
         }
         int c = 0, gm = cfgs[0].num_m;
-        if (!stall) {   // abort-path test: one launch of the wide tile, no tuning trials
+        if (thin && !stall) {
+            c = 2;
+            gm = cfgs[2].num_m;
+        } else if (!stall) {   // abort-path test: one launch of the wide tile, no tuning trials
             // trial runs write D, so an accumulating launch only reuses a choice tuned earlier (and a
             // launch being captured into a CUDA graph runs nothing, so it cannot time trials)
             TD_TRY(choose(TF32 ? 1 : 0, NPROD, kM, kN, kK, shape, cfgs, 2, st, !op.accumulate && !capturing, &c, &gm));
