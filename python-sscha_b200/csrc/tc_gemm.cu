@@ -5,14 +5,15 @@
 //   hi.hi + hi.lo + lo.hi recover ~16 (bf16) / ~21 (tf32) significant bits.
 //   D (M x N): fp32, row-major, written with edge masking.
 //
-// Pipeline (one CTA per 128 x BN output tile, 6 warps):
+// Pipeline (persistent: one CTA per SM walks 128 x BN output tiles; BN = 256, 128 or 64; 10 warps):
 //   warp 0      : TMA producer -- cp.async.bulk.tensor.2d into a STAGES-deep ring of 128B-swizzled
 //                 tiles, completion tracked by mbarrier transaction counts;
-//   warp 1      : allocates BN TMEM columns; one elected thread issues tcgen05.mma (kind::f16 for
-//                 bf16, kind::tf32) from shared-memory descriptors, accumulating in TMEM, and frees
-//                 each ring slot with tcgen05.commit -> mbarrier;
-//   warps 2..5  : epilogue -- tcgen05.ld 32x32b from TMEM (warp w reads lanes 32*(w%4)..+31), fp32
-//                 stores to global memory.
+//   warp 1      : allocates 2 x BN TMEM columns (two accumulator buffers); one elected thread issues
+//                 tcgen05.mma (kind::f16 for bf16, kind::tf32) from shared-memory descriptors,
+//                 accumulating in TMEM, and frees each ring slot with tcgen05.commit -> mbarrier;
+//   warps 2..9  : epilogue -- tcgen05.ld 32x32b from TMEM (warp w reads lanes 32*(w%4)..+31, half of
+//                 the columns), fp32 sums in registers, stores to global memory through a per-warp
+//                 shared-memory block (full 128-byte lines per store instruction).
 // Every mbarrier wait is bounded by a %globaltimer budget; on expiry the CTA raises ERR_TIMEOUT in
 // the caller's error word, drains its own TMA copies (bounded), frees TMEM and returns.
 #include <cuda.h>
