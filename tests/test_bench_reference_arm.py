@@ -22,6 +22,10 @@ def test_reference_arm_prints_the_contract_line():
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["e2e"]["d2h_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port") and line["cpu_baseline"]["cores"] >= 1
     assert line["reference_kind"] == line["cpu_baseline"]["kind"]     # which CPU code ran, at the top level
+    # the same step as the repo arm: one batched apply of 2 x chains vectors
+    assert line["applies_per_step"] == 16
+    assert abs(line["ms_per_step"] - 16 * line["ms_per_apply"]) <= 1e-9 * line["ms_per_step"]
+    assert abs(line["ms_per_apply"] * line["value"] - 1e3) <= 1e-9 * 1e3
 
 
 def test_cpu_timing_with_the_port_backend():
