@@ -101,7 +101,7 @@ def _emulate(ens, R1, Y1, d4):
     return Rf @ (fr * norm), Rf @ (Dr * norm) @ Rf.T, cl
 
 
-@pytest.mark.parametrize("L,N,n_class", [(2, 6, 8), (3, 3, 14)])
+@pytest.mark.parametrize("L,N,n_class", [(2, 6, 8), (3, 3, 14), (4, 2, 36)])   # 4x4x4: the benchmark's group
 def test_class_tables_reproduce_the_averages(L, N, n_class):
     ens = RS.make_ensemble(L, N, seed=5)
     n = ens.X.shape[1]
