@@ -197,15 +197,24 @@ def build_system(L, T=300.0, a_ang=5.6, masses_amu=(23.0, 35.45), k2=2.0, k3=-3.
         from . import _native
         sym_blocks = _native.symmetries_on_modes(vec, perms, rmats, sys_.deg_space)
     else:
-        # P_j acting on (3 nat) mass-weighted displacement: (P v)[pi(a)] = R v[a]
+        # P_j acting on (3 nat) mass-weighted displacement: (P v)[pi(a)] = R v[a].  The symmetries
+        # are ordered rotation-major, so R E is formed once per rotation; the images of a chunk of
+        # translations are stacked and their block products run as one batched matmul (the same
+        # per-matrix product as one symmetry at a time, so the tables are identical)
         sym_blocks = [np.zeros((N_sym, len(blk), len(blk))) for blk in blocks]
         E3 = vec.reshape(nat, 3, -1)
-        for j in range(N_sym):
-            PE = np.zeros_like(E3)
-            PE[perms[j]] = np.einsum("ab,nbm->nam", rmats[j], E3)
-            PE = PE.reshape(3 * nat, -1)
-            for b, blk in enumerate(blocks):
-                sym_blocks[b][j] = vec[:, blk].T @ PE[:, blk]
+        n_tr = len(trans)
+        chunk = 32
+        for r in range(len(rots)):
+            RE = np.einsum("ab,nbm->nam", rmats[r * n_tr], E3)
+            for t0 in range(0, n_tr, chunk):
+                t1 = min(n_tr, t0 + chunk)
+                j0, j1 = r * n_tr + t0, r * n_tr + t1
+                PE = np.empty((t1 - t0,) + E3.shape)
+                PE[np.arange(t1 - t0)[:, None], perms[j0:j1]] = RE[None]
+                PE = PE.reshape(t1 - t0, 3 * nat, -1)
+                for b, blk in enumerate(blocks):
+                    sym_blocks[b][j0:j1] = np.matmul(vec[:, blk].T[None], PE[:, :, blk])
     sys_.symmetries = sym_blocks
     sys_.n_syms = N_sym
     sys_.perm = perms

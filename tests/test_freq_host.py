@@ -120,6 +120,22 @@ def test_class_tables_reproduce_the_averages(L, N, n_class):
     assert cl["flops_ratio"] < 2.0 / sub * 1.3
 
 
+def test_class_tables_reproduce_the_averages_at_5x5x5():
+    """The largest group of the benchmark configurations: O_h x 125 = 6000 operations, 63 classes."""
+    ens = RS.make_ensemble(5, 2, seed=5)
+    n = ens.X.shape[1]
+    rng = np.random.default_rng(5)
+    R1, Y1 = rng.standard_normal(n), rng.standard_normal((n, n))
+    n_deg = np.array([len(b) for b in ens.deg_space], dtype=np.intc)
+    f_ref, d_ref = LO.perturb_average_sym(ens.X, ens.Y, ens.w, ens.rho, R1, Y1, ens.T, 1, ens.symmetries, n_deg,
+                                          ens.deg_space, ens.blocks_ids)
+    f, d, cl = _emulate(ens, R1, Y1, 1)
+    assert np.abs(f - f_ref).max() <= 1e-12 * np.abs(f_ref).max()
+    assert np.abs(d - d_ref).max() <= 1e-12 * np.abs(d_ref).max()
+    assert cl["n_class"] == 63
+    assert cl["flops_ratio"] < 2.0 / 125 * 1.3
+
+
 def test_classes_of_the_benchmark_system():
     system = RS.build_system(4)
     cl = _native.symmetry_classes(system.symmetries)
